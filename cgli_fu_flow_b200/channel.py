@@ -1,0 +1,182 @@
+"""Seeded turbulent-channel workloads: physical constants, grid spacings and the
+initial field, in the array layout of the reference solver.
+
+The reference hard-wires its case in compile-time headers (Resolution.h,
+prm.h, Viscous_terms.h) and starts from a quiescent heated channel
+(Initial_condition.cpp:64-97).  The workloads here are the periodic channel
+at bulk Mach 0.2 and Re_b = 5600 (Re_b = rho0 * U_b * 2h / mu0, the
+Kim-Moin-Moser convention), in the reference's dimensional SI units:
+
+* domain 2*pi*h x 2h x pi*h, uniform in x and z, tanh wall clustering in y
+  with the mapping of Jacobian.cpp:76-90 (stretching parameter 2.0);
+* air: gamma 1.4, R 287, Cv 717.5, Sutherland viscosity written as in
+  Viscous_terms.cpp:527 with mu0 = 1.85e-5 at 298.0592 K, Pr 0.72;
+* isothermal walls at T0 on both sides (Y_boundary_condition.cpp:139,166
+  with equal temperatures);
+* initial field: laminar Poiseuille profile plus uniform-random velocity
+  perturbations of +-10 % of U_b from a counter-based generator
+  (splitmix64 of seed + 3*cell + component), each component's x-z plane
+  mean removed; uniform density and temperature.  Q^n = Q^(n-1).
+
+A workload is named by its cell counts; nothing here depends on a GPU.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field, asdict
+
+import numpy as np
+
+GAMMA = 1.4
+R_GAS = 287.0
+CV = 717.5
+T0 = 298.0592
+P0 = 101300.0
+MU0 = 1.85e-5
+PR = 0.72
+MACH_B = 0.2
+RE_B = 5600.0
+STRETCH = 2.0
+# e of main.cpp:57, the low-Mach preconditioning floor beta >= e.  The
+# reference uses 1e-4 for its near-incompressible heated cavity; on the Mach
+# 0.2 channel at CFL 1 that value makes its own pseudo-time iteration diverge
+# within the first physical step, 1e-3 converges.
+PRECOND_EPS = 1e-3
+SEED = 20261203
+
+
+def splitmix64(x: np.ndarray) -> np.ndarray:
+    """splitmix64 finaliser (Steele, Lea, Flood 2014) on uint64 arrays."""
+    with np.errstate(over="ignore"):
+        z = (x + np.uint64(0x9E3779B97F4A7C15)).astype(np.uint64)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return z ^ (z >> np.uint64(31))
+
+
+@dataclass
+class Channel:
+    """One channel workload: cell counts plus every derived constant the
+    solver, the oracle and the reference build need."""
+    nx: int
+    ny: int
+    nz: int
+    cfl: float = 1.0
+    seed: int = SEED
+    # derived (filled in __post_init__)
+    rho0: float = field(init=False)
+    c0: float = field(init=False)
+    u_b: float = field(init=False)
+    h: float = field(init=False)
+    high: float = field(init=False)
+    lx: float = field(init=False)
+    lz: float = field(init=False)
+    dxi: float = field(init=False)
+    det: float = field(init=False)
+    dzt: float = field(init=False)
+    dt: float = field(init=False)
+    force_lam: float = field(init=False)
+
+    def __post_init__(self):
+        self.rho0 = P0 / T0 / R_GAS                       # Initial_condition.cpp:75 order
+        self.c0 = math.sqrt(GAMMA * R_GAS * T0)
+        self.u_b = MACH_B * self.c0
+        self.h = 0.5 * RE_B * MU0 / (self.rho0 * self.u_b)
+        self.high = 2.0 * self.h                          # prm.h:16 (channel height)
+        self.lx = 2.0 * math.pi * self.h
+        self.lz = math.pi * self.h
+        self.dxi = self.lx / self.nx                      # deltaXI, metres (xidx = 1)
+        self.det = 1.0 / self.ny                          # deltaET, normalised eta
+        self.dzt = self.lz / self.nz                      # deltaZT, metres (ztdz = 1)
+        self.dt = self.cfl * self.dxi / self.u_b
+        self.force_lam = 3.0 * MU0 * self.u_b / (self.h * self.h)
+
+    @property
+    def name(self) -> str:
+        return f"channel_{self.nx}x{self.ny}x{self.nz}"
+
+    @property
+    def cells(self) -> int:
+        return self.nx * self.ny * self.nz
+
+    @property
+    def shape(self) -> tuple[int, int, int]:
+        """(X_np, Y_m, Z_m): the reference's per-array shape for one x-slab."""
+        return (self.nx + 6, self.ny + 4, self.nz + 4)
+
+    @property
+    def target_flux(self) -> float:
+        return self.rho0 * self.u_b
+
+    def as_dict(self) -> dict:
+        return asdict(self)
+
+    # ------------------------------------------------------------------ IC
+    def cell_y(self) -> np.ndarray:
+        """Wall-normal cell-centre coordinates, the mapping of Jacobian.cpp:77
+        evaluated at eta = (j - 1.5) * deltaET for interior j = 2..Ny+1."""
+        j = np.arange(2, self.ny + 2, dtype=np.float64)
+        g = STRETCH
+        eta = (j - 1.5) * self.det
+        return (0.5 * self.high) * (1 - 1. / math.tanh(g) * np.tanh(g * (1 - 2 * eta)))
+
+    def initial_primitives(self) -> tuple[np.ndarray, ...]:
+        """rho, u, v, w, p on the interior cells, shape (Nx, Ny, Nz)."""
+        nx, ny, nz = self.nx, self.ny, self.nz
+        y = self.cell_y()
+        u_lam = 1.5 * self.u_b * (1.0 - (y / self.h - 1.0) ** 2)
+        idx = np.arange(nx * ny * nz, dtype=np.uint64).reshape(nx, ny, nz)
+        comps = []
+        for c in range(3):
+            ctr = np.uint64(self.seed) + np.uint64(3) * idx + np.uint64(c)
+            r = (splitmix64(ctr) >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+            pert = 0.1 * self.u_b * (2.0 * r - 1.0)
+            pert -= pert.mean(axis=(0, 2), keepdims=True)
+            comps.append(pert)
+        u = u_lam[None, :, None] + comps[0]
+        v = comps[1]
+        w = comps[2]
+        rho = np.full((nx, ny, nz), self.rho0)
+        p = np.full((nx, ny, nz), P0)
+        return rho, u, v, w, p
+
+    def initial_conserved(self) -> np.ndarray:
+        """(5, Nx, Ny, Nz) physical conserved variables rho, rho u, rho v,
+        rho w, E (not divided by J) -- the content of one time level of the
+        reference restart file (Initial_condition.cpp:136-221)."""
+        rho, u, v, w, p = self.initial_primitives()
+        vv = u * u + v * v + w * w
+        return np.stack([rho, rho * u, rho * v, rho * w, p / (GAMMA - 1) + 0.5 * rho * vv])
+
+    def write_restart(self, path: str, q_n: np.ndarray, q_nm1: np.ndarray, ranks: int = 3) -> None:
+        """Writes the reference restart layout for a run presented as rank 1
+        of `ranks` equal x-slabs: 10 fields [U1..U5 at n, U1..U5 at n-1],
+        each of ranks*Nx x Ny x Nz doubles, this slab at x-offset Nx."""
+        nx, ny, nz = self.nx, self.ny, self.nz
+        out = np.zeros((10, ranks * nx, ny, nz))
+        out[0:5, nx:2 * nx] = q_n
+        out[5:10, nx:2 * nx] = q_nm1
+        out.tofile(path)
+
+
+def force_update(state: dict, bulk_flux: float, ch: Channel, kp: float = 0.5, ki: float = 0.05) -> float:
+    """Mass-flux controller that holds the bulk flux at rho0*U_b.
+
+    The reference only monitors the bulk flux (Driven_force.cpp:38-71) and
+    applies buoyancy (Dual_time_stepping.cpp:831); the workloads replace that
+    body force by a uniform x-force F that is updated once per physical step
+    from the converged state:  e = Q_t - Q_b,  I += e,
+    F = F_lam + (kp*e + ki*I) / dt,  F_lam = 3 mu0 U_b / h^2 (laminar wall
+    shear).  `state` carries I between calls; returns the new F."""
+    e = ch.target_flux - bulk_flux
+    state["I"] = state.get("I", 0.0) + e
+    return ch.force_lam + (kp * e + ki * state["I"]) / ch.dt
+
+
+WORKLOADS = {
+    "small": (8, 12, 8),
+    "c1": (64, 64, 64),
+    "c2": (256, 192, 192),
+    "c3": (384, 256, 256),
+    "c4": (256, 256, 128),
+}

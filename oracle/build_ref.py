@@ -1,0 +1,200 @@
+"""Build recipe for the reference oracle library  oracle/_ref/<name>/libref.so.
+
+Test infrastructure only.  It compiles the reference's own hot-path sources,
+read from the reference tree, together with oracle/ref_harness.cpp and the
+single-process MPI stub.  Nothing is copied into the repository: each source
+is read, the recorded patch list is applied in memory, and the text is piped
+to g++ on standard input; only objects and the shared library are written,
+and only under oracle/_ref/.
+
+The reference fixes its grid and physics at compile time, so one library is
+built per workload from generated stand-ins for Resolution.h, prm.h,
+Viscous_terms.h and MPI_prm.h (placed first on the include path; ijk.h and
+Mpi_division.h are used as shipped).  The process is presented to the
+reference as rank 1 of 3 equal x-slabs (X_out = 3*Nx, np = 3).
+
+Patch list (each replacement must match the stated number of times):
+  P4  Jacobian*.cpp:49-50  wall-clustering parameter 2.8 -> workload value
+  P5  Y_boundary_condition.cpp:139,166  wall temperatures -> workload values
+  P6  Dual_time_stepping.cpp:831  buoyancy -> uniform driving force read
+      from the harness (mass-flux controller value)
+  P9  Flux_Y.cpp:383-385, Flux_Z.cpp:339-341  the Roe pressure-jump term
+      multiplies the never-initialised locals XIx, XIy, XIz; use the face
+      unit normal of the routine's own direction (ETx.., ZTx..) instead
+  P1-P3 (grid, channel height, viscosity, Pr) come from the generated headers;
+  P10 (value-initialised arrays) is the harness's calloc.
+
+Usage:  python oracle/build_ref.py --nx 8 --ny 12 --nz 8 [--name NAME]
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import json
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
+REF_SRC = os.environ.get("CGLI_REFERENCE_DIR", "/root/reference")
+
+SOURCES = [
+    "Jacobian.cpp", "Jacobian_u.cpp", "Jacobian_v.cpp", "Jacobian_w.cpp",
+    "Initial_condition.cpp", "X_boundary_condition.cpp", "Y_boundary_condition.cpp",
+    "Z_boundary_condition.cpp", "Flux_X.cpp", "Flux_Y.cpp", "Flux_Z.cpp",
+    "Viscous_terms.cpp", "Dual_time_stepping.cpp", "Driven_force.cpp", "Hyperplane.cpp",
+    "Filter.cpp",
+]
+
+PATCHES = {
+    "Jacobian.cpp": [("double gamma1 = 2.8;", "double gamma1 = CGLI_STRETCH;", 1)],
+    "Jacobian_u.cpp": [("double gamma1 = 2.8;", "double gamma1 = CGLI_STRETCH;", 1)],
+    "Jacobian_v.cpp": [("double gamma1 = 2.8;", "double gamma1 = CGLI_STRETCH;", 1)],
+    "Jacobian_w.cpp": [("double gamma1 = 2.8;", "double gamma1 = CGLI_STRETCH;", 1)],
+    "Y_boundary_condition.cpp": [("T = 343.0592;", "T = CGLI_TWALL_LO;", 1),
+                                 ("T = 298.0592;", "T = CGLI_TWALL_HI;", 1)],
+    "Dual_time_stepping.cpp": [("f = -(rho-1.1842)*9.81;", "f = cgli_ref_force;", 1),
+                               ("void Dual_time_stepping", "extern double cgli_ref_force;\nvoid Dual_time_stepping", 1)],
+    "Flux_Y.cpp": [("deltaP*XIx;", "deltaP*ETx;", 1), ("deltaP*XIy;", "deltaP*ETy;", 1),
+                   ("deltaP*XIz;", "deltaP*ETz;", 1)],
+    "Flux_Z.cpp": [("deltaP*XIx;", "deltaP*ZTx;", 1), ("deltaP*XIy;", "deltaP*ZTy;", 1),
+                   ("deltaP*XIz;", "deltaP*ZTz;", 1)],
+}
+
+CXXFLAGS = ["-O2", "-fopenmp", "-fPIC", "-w", "-std=gnu++14", "-ffp-contract=off"]
+
+
+def r17(x: float) -> str:
+    return repr(float(x))
+
+
+def gen_headers(cfgdir: str, p: dict) -> None:
+    nx3 = 3 * p["nx"]
+    res = f"""/* generated stand-in for Resolution.h: rank 1 of 3 x-slabs */
+#define nx_inlet  0
+#define nx_outlet 0
+#define X_out {nx3}
+#define Y_out {p['ny']}
+#define Z_out {p['nz']}
+#define X_m {nx3 + 4}
+#define Y_m {p['ny'] + 4}
+#define Z_m {p['nz'] + 4}
+#define nx X_out+1
+#define ny Y_out+1
+#define nz Z_out+1
+#define deltaXI {r17(p['dxi'])}
+#define deltaET {r17(p['det'])}
+#define deltaZT {r17(p['dzt'])}
+#define nxx nx+1
+#define nyy ny+1
+#define nzz nz+1
+#define nxxx nxx+1
+#define nyyy nyy+1
+#define nzzz nzz+1
+#define CGLI_STRETCH {r17(p['stretch'])}
+#define CGLI_TWALL_LO {r17(p['twall_lo'])}
+#define CGLI_TWALL_HI {r17(p['twall_hi'])}
+"""
+    prm = f"""/* generated stand-in for prm.h */
+#define K 1.4
+#define R 287
+#define minimum 0.0000001
+double f = 0.5993;
+double Q0 = 2.07;
+double Qold = Q0;
+double high = {r17(p['high'])};
+double psi = 0.001;
+"""
+    vis = f"""/* generated stand-in for Viscous_terms.h */
+#include "prm.h"
+#define Cv 717.5
+#define mu_L {r17(p['mu'])}
+#define Pr_L {r17(p['pr'])}
+#define R 287
+double Cp = Cv*K;
+double lambda_L = mu_L*Cv*K/Pr_L;
+"""
+    mpi = """/* generated stand-in for MPI_prm.h: three x-slabs */
+#define np 3
+int nproc = np;
+int istart, iend, icount, r_nbr, l_nbr, lastp, iroot;
+int itag, isrc, idest, istart1, icount1,icount2, istart2, iend1, iend2;
+int gstart0[np], gend0[np],gstart[np], gend[np], gcount[np];
+double tstart,tend;
+MPI_Request l_reqs1,l_reqs2,l_reqs3,l_reqs4,l_reqs5,
+            r_reqs1,r_reqs2,r_reqs3,r_reqs4,r_reqs5;
+MPI_Request r1,r2,r3,r4,r5,r6,r7,r8,r9,r10;
+"""
+    os.makedirs(cfgdir, exist_ok=True)
+    for name, text in (("Resolution.h", res), ("prm.h", prm), ("Viscous_terms.h", vis), ("MPI_prm.h", mpi)):
+        with open(os.path.join(cfgdir, name), "w") as fh:
+            fh.write(text)
+
+
+def patched_source(fname: str) -> str:
+    with open(os.path.join(REF_SRC, fname)) as fh:
+        text = fh.read()
+    for old, new, count in PATCHES.get(fname, []):
+        n = text.count(old)
+        if n != count:
+            raise RuntimeError(f"patch for {fname}: '{old}' found {n} times, expected {count}")
+        text = text.replace(old, new)
+    return text
+
+
+def compile_one(fname: str, outdir: str, cfgdir: str) -> str:
+    obj = os.path.join(outdir, fname.replace(".cpp", ".o"))
+    incs = ["-I", cfgdir, "-I", os.path.join(HERE, "mpi_stub"), "-I", REF_SRC]
+    if fname == "ref_harness.cpp":
+        cmd = ["g++", *CXXFLAGS, *incs, "-c", os.path.join(HERE, fname), "-o", obj]
+        subprocess.run(cmd, check=True)
+    else:
+        cmd = ["g++", *CXXFLAGS, *incs, "-x", "c++", "-c", "-", "-o", obj]
+        subprocess.run(cmd, input=patched_source(fname).encode(), check=True)
+    return obj
+
+
+def build(params: dict, name: str | None = None, jobs: int = 8) -> str:
+    """Builds (if needed) and returns the path of libref.so for `params`
+    (keys nx, ny, nz, dxi, det, dzt, high, mu, pr, stretch, twall_lo, twall_hi)."""
+    if not os.path.isdir(REF_SRC):
+        raise FileNotFoundError(f"reference sources not found at {REF_SRC}")
+    name = name or f"channel_{params['nx']}x{params['ny']}x{params['nz']}"
+    outdir = os.path.join(HERE, "_ref", name)
+    lib = os.path.join(outdir, "libref.so")
+    stamp = os.path.join(outdir, "params.json")
+    want = json.dumps(params, sort_keys=True)
+    deps = [os.path.join(HERE, "ref_harness.cpp"), os.path.join(HERE, "mpi_stub", "mpi.h"),
+            os.path.abspath(__file__)]
+    if os.path.exists(lib) and os.path.exists(stamp):
+        with open(stamp) as fh:
+            same = fh.read() == want
+        if same and all(os.path.getmtime(d) <= os.path.getmtime(lib) for d in deps):
+            return lib
+    cfgdir = os.path.join(outdir, "cfg")
+    gen_headers(cfgdir, params)
+    with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
+        objs = list(ex.map(lambda f: compile_one(f, outdir, cfgdir), SOURCES + ["ref_harness.cpp"]))
+    subprocess.run(["g++", "-shared", "-fopenmp", "-o", lib, *objs, "-Wl,--no-undefined", "-lm"], check=True)
+    with open(stamp, "w") as fh:
+        fh.write(want)
+    return lib
+
+
+def channel_params(nx: int, ny: int, nz: int) -> dict:
+    sys.path.insert(0, REPO)
+    from cgli_fu_flow_b200.channel import Channel, MU0, PR, STRETCH, T0
+    ch = Channel(nx, ny, nz)
+    return dict(nx=nx, ny=ny, nz=nz, dxi=ch.dxi, det=ch.det, dzt=ch.dzt, high=ch.high,
+                mu=MU0, pr=PR, stretch=STRETCH, twall_lo=T0, twall_hi=T0)
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--nx", type=int, required=True)
+    ap.add_argument("--ny", type=int, required=True)
+    ap.add_argument("--nz", type=int, required=True)
+    ap.add_argument("--name", default=None)
+    a = ap.parse_args()
+    print(build(channel_params(a.nx, a.ny, a.nz), a.name))

@@ -1,0 +1,141 @@
+"""ctypes wrapper for the C restatement oracle (oracle/cgli_oracle.c).
+
+Test infrastructure only (tests/, __graft_entry__.smoke(), bench.py's
+CPU-baseline leg).  `build()` compiles the C file into oracle/_build/.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "liboracle.so")
+SRC = os.path.join(HERE, "cgli_oracle.c")
+
+
+def build() -> str:
+    if not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(SRC):
+        os.makedirs(os.path.dirname(LIB), exist_ok=True)
+        subprocess.run(["gcc", "-O2", "-fPIC", "-shared", "-ffp-contract=off", "-o", LIB, SRC, "-lm"],
+                       check=True)
+    return LIB
+
+
+class _Params(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("dxi", ctypes.c_double), ("det", ctypes.c_double), ("dzt", ctypes.c_double),
+                ("dt", ctypes.c_double), ("e", ctypes.c_double),
+                ("mu", ctypes.c_double), ("pr", ctypes.c_double),
+                ("twall_lo", ctypes.c_double), ("twall_hi", ctypes.c_double),
+                ("force", ctypes.c_double)]
+
+
+_lib = None
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        L = ctypes.CDLL(build())
+        L.or_create.restype = ctypes.c_void_p
+        L.or_create.argtypes = [ctypes.POINTER(_Params)]
+        L.or_destroy.argtypes = [ctypes.c_void_p]
+        L.or_array.restype = ctypes.POINTER(ctypes.c_double)
+        L.or_array.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+        L.or_metrics.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
+        L.or_initial.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.or_set_force.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        L.or_bulk_flux.restype = ctypes.c_double
+        L.or_bulk_flux.argtypes = [ctypes.c_void_p]
+        for name in ("or_halo_x", "or_bc_y", "or_bc_z", "or_flux_x", "or_flux_y", "or_flux_z",
+                     "or_viscous", "or_dts_residual", "or_sweeps", "or_end_step"):
+            getattr(L, name).argtypes = [ctypes.c_void_p]
+        L.or_update.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.or_inner_iteration.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        _lib = L
+    return _lib
+
+
+class Oracle:
+    """CPU restatement of one slab of the reference solver for one workload."""
+
+    def __init__(self, ch, e: float | None = None):
+        from cgli_fu_flow_b200 import channel as C
+        self.C = C
+        self.ch = ch
+        self.L = _load()
+        p = _Params(ch.nx, ch.ny, ch.nz, ch.dxi, ch.det, ch.dzt, ch.dt,
+                    C.PRECOND_EPS if e is None else e, C.MU0, C.PR, C.T0, C.T0, ch.force_lam)
+        self.s = self.L.or_create(ctypes.byref(p))
+        self.shape = ch.shape
+        self.force = ch.force_lam
+        self.ctrl = {}
+        self.L.or_metrics(self.s, ch.high, C.STRETCH)
+
+    def __del__(self):
+        if getattr(self, "s", None):
+            self.L.or_destroy(self.s)
+            self.s = None
+
+    def array(self, name: str) -> np.ndarray:
+        p = self.L.or_array(self.s, name.encode())
+        if not p:
+            raise KeyError(name)
+        n = int(np.prod(self.shape))
+        return np.ctypeslib.as_array(p, shape=(n,)).reshape(self.shape)
+
+    def q(self, which: str = "_") -> np.ndarray:
+        suffix = {"_": "_", "n": "", "nm1": "q"}[which]
+        return np.stack([self.array(f"U{v}{suffix}").copy() for v in range(1, 6)])
+
+    def init(self, q_n: np.ndarray | None = None, q_nm1: np.ndarray | None = None) -> None:
+        if q_n is None:
+            q_n = self.ch.initial_conserved()
+        if q_nm1 is None:
+            q_nm1 = q_n
+        a = np.ascontiguousarray(q_n, dtype=np.float64)
+        b = np.ascontiguousarray(q_nm1, dtype=np.float64)
+        self.L.or_initial(self.s, a.ctypes.data, b.ctypes.data)
+        self.L.or_set_force(self.s, self.force)
+
+    def call(self, name: str) -> None:
+        getattr(self.L, "or_" + name)(self.s)
+
+    def update(self) -> np.ndarray:
+        er = np.zeros(5)
+        self.L.or_update(self.s, er.ctypes.data)
+        return er
+
+    def inner_iteration(self) -> np.ndarray:
+        er = np.zeros(5)
+        self.L.or_inner_iteration(self.s, er.ctypes.data)
+        return er
+
+    def bulk_flux(self) -> float:
+        return self.L.or_bulk_flux(self.s)
+
+    def end_step(self, update_force: bool = True) -> None:
+        qb = self.bulk_flux()
+        self.L.or_end_step(self.s)
+        if update_force:
+            self.force = self.C.force_update(self.ctrl, qb, self.ch)
+            self.L.or_set_force(self.s, self.force)
+
+    def step(self, fixed_iters: int | None = 10, drop: float = 1e-3, cap: int = 30):
+        first = None
+        it = 0
+        while True:
+            it += 1
+            er = self.inner_iteration()
+            if first is None:
+                first = np.where(er > 0, er, 1.0)
+            if fixed_iters is not None:
+                if it >= fixed_iters:
+                    break
+            elif np.all(er / first < drop) or it >= cap:
+                break
+        self.end_step()
+        return it, er

@@ -1,0 +1,110 @@
+"""ctypes driver for the reference oracle library (oracle/_ref/<name>/libref.so).
+
+Test infrastructure only: used by tests/, by the CPU-baseline leg of bench.py
+and by tests/golden/make_golden.py.  It reproduces the reference driver loop
+of main.cpp:152-420 on top of the harness entry points: inner iterations
+until the workload's stopping rule, then the end-of-step block.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import tempfile
+
+import numpy as np
+
+from . import build_ref
+
+
+class RefSolver:
+    """One reference process (rank 1 of 3, periodic x) for one workload."""
+
+    def __init__(self, ch, threads: int = 0, build: bool = True):
+        params = dict(nx=ch.nx, ny=ch.ny, nz=ch.nz, dxi=ch.dxi, det=ch.det, dzt=ch.dzt,
+                      high=ch.high, mu=_c().MU0, pr=_c().PR, stretch=_c().STRETCH,
+                      twall_lo=_c().T0, twall_hi=_c().T0)
+        if build:
+            path = build_ref.build(params, ch.name)
+        else:
+            path = os.path.join(os.path.dirname(__file__), "_ref", ch.name, "libref.so")
+        self.lib = ctypes.CDLL(path)
+        L = self.lib
+        L.ref_array.restype = ctypes.POINTER(ctypes.c_double)
+        L.ref_array.argtypes = [ctypes.c_char_p]
+        L.ref_init.argtypes = [ctypes.c_char_p, ctypes.c_double, ctypes.c_double]
+        L.ref_set_force.argtypes = [ctypes.c_double]
+        L.ref_bulk_flux.restype = ctypes.c_double
+        L.ref_check_hyperplanes.restype = ctypes.c_long
+        L.ref_filter.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        self.ch = ch
+        dims = (ctypes.c_int * 6)()
+        L.ref_dims(dims)
+        self.shape = (dims[3], dims[4], dims[5])
+        assert self.shape == ch.shape, (self.shape, ch.shape)
+        if threads:
+            L.ref_set_threads(threads)
+        self.force = ch.force_lam
+        self.ctrl = {}
+
+    def init(self, q_n: np.ndarray | None = None, q_nm1: np.ndarray | None = None) -> None:
+        """Loads the seeded initial field through the reference's own restart
+        reader (Initial_condition.cpp:111-236)."""
+        ch = self.ch
+        if q_n is None:
+            q_n = ch.initial_conserved()
+        if q_nm1 is None:
+            q_nm1 = q_n
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "initial.bin")
+            ch.write_restart(path, q_n, q_nm1)
+            self.lib.ref_init(path.encode(), ch.dt, _c().PRECOND_EPS)
+        self.lib.ref_set_force(self.force)
+
+    def array(self, name: str) -> np.ndarray:
+        """A live view of one reference array, shape (X_np, Y_m, Z_m)."""
+        p = self.lib.ref_array(name.encode())
+        if not p:
+            raise KeyError(name)
+        n = int(np.prod(self.shape))
+        return np.ctypeslib.as_array(p, shape=(n,)).reshape(self.shape)
+
+    def q(self, which: str = "_") -> np.ndarray:
+        suffix = {"_": "_", "n": "", "nm1": "q"}[which]
+        return np.stack([self.array(f"U{v}{suffix}").copy() for v in range(1, 6)])
+
+    def inner_iteration(self) -> np.ndarray:
+        er = (ctypes.c_double * 5)()
+        self.lib.ref_inner_iteration(er)
+        return np.array(er[:])
+
+    def end_step(self, update_force: bool = True) -> None:
+        qb = self.lib.ref_bulk_flux()
+        self.lib.ref_end_step()
+        if update_force:
+            self.force = _c().force_update(self.ctrl, qb, self.ch)
+            self.lib.ref_set_force(self.force)
+
+    def step(self, fixed_iters: int | None = 10, drop: float = 1e-3, cap: int = 30) -> tuple[int, np.ndarray]:
+        """One physical step.  fixed_iters=N runs exactly N inner iterations;
+        fixed_iters=None iterates until every one of the five update norms has
+        dropped by `drop` relative to the step's first iteration, or `cap`."""
+        first = None
+        it = 0
+        while True:
+            it += 1
+            er = self.inner_iteration()
+            if first is None:
+                first = np.where(er > 0, er, 1.0)
+            rel = er / first
+            if fixed_iters is not None:
+                if it >= fixed_iters:
+                    break
+            elif np.all(rel < drop) or it >= cap:
+                break
+        self.end_step()
+        return it, er
+
+
+def _c():
+    from cgli_fu_flow_b200 import channel
+    return channel
