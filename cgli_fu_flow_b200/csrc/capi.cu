@@ -1,0 +1,414 @@
+// extern "C" entry points of include/cgli_fu_flow.h: context lifetime,
+// device memory, array transfer, the reference-routine entry points and the
+// physical-step driver (the loop of main.cpp:152-420).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cgli_fu_flow.h"
+#include "cgli_dev.cuh"
+#include "cgli_launch.h"
+
+#include "host_setup.h"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CUDA_TRY(call)                                                                    \
+  do {                                                                                    \
+    cudaError_t _e = (call);                                                              \
+    if (_e != cudaSuccess)                                                                \
+      return fail(CGLI_ECUDA, std::string(#call) + ": " + cudaGetErrorString(_e));       \
+  } while (0)
+
+const char *kMetricNames[9] = {"xidx", "xidy", "xidz", "etdx", "etdy", "etdz", "ztdx", "ztdy", "ztdz"};
+
+}  // namespace
+
+struct cgli_ctx {
+  cgli_params p;
+  cgli::Dev d;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<void *> allocs;
+  long long bytes = 0;
+  bool have_metrics = false, have_state = false;
+  double *h_norms = nullptr;   // pinned, 8 doubles
+  double *d_out = nullptr;     // device scratch for norms / bulk flux
+  int update_blocks = 0;
+  cudaGraphExec_t iter_graph = nullptr;
+  cudaGraphExec_t dts_graph = nullptr;
+};
+
+namespace {
+
+int alloc(cgli_ctx *c, size_t bytes, void **out) {
+  void *p = nullptr;
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) return fail(CGLI_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  e = cudaMemset(p, 0, bytes);
+  if (e != cudaSuccess) return fail(CGLI_ECUDA, std::string("cudaMemset: ") + cudaGetErrorString(e));
+  c->allocs.push_back(p);
+  c->bytes += (long long)bytes;
+  *out = p;
+  return CGLI_OK;
+}
+
+int field(cgli_ctx *c, double **out) {
+  size_t n = (size_t)c->d.X * c->d.Y * c->d.Z;
+  return alloc(c, n * sizeof(double), (void **)out);
+}
+
+// device array of a reference name; *is_metric tells whether it is one of
+// the 40 metric arrays
+double *lookup(cgli_ctx *c, const char *name, bool *is_metric = nullptr) {
+  if (is_metric) *is_metric = false;
+  cgli::Dev &d = c->d;
+  char buf[32];
+  for (int v = 0; v < 5; v++) {
+    snprintf(buf, sizeof buf, "U%d_", v + 1); if (!strcmp(name, buf)) return d.U_[v];
+    snprintf(buf, sizeof buf, "U%d", v + 1); if (!strcmp(name, buf)) return d.U[v];
+    snprintf(buf, sizeof buf, "U%dq", v + 1); if (!strcmp(name, buf)) return d.Uq[v];
+    snprintf(buf, sizeof buf, "MR%d", v + 1); if (!strcmp(name, buf)) return d.MR[v];
+    snprintf(buf, sizeof buf, "NR%d", v + 1); if (!strcmp(name, buf)) return d.NR[v];
+    snprintf(buf, sizeof buf, "NL%d", v + 1); if (!strcmp(name, buf)) return d.NL[v];
+    snprintf(buf, sizeof buf, "inFx%d", v + 1); if (!strcmp(name, buf)) return d.inF[0][v];
+    snprintf(buf, sizeof buf, "inFy%d", v + 1); if (!strcmp(name, buf)) return d.inF[1][v];
+    snprintf(buf, sizeof buf, "inFz%d", v + 1); if (!strcmp(name, buf)) return d.inF[2][v];
+  }
+  for (int v = 0; v < 4; v++) {
+    snprintf(buf, sizeof buf, "vF%d", v + 2); if (!strcmp(name, buf)) return d.vF[v];
+  }
+  if (is_metric) *is_metric = true;
+  if (!strcmp(name, "J")) return d.J;
+  const char *fs[3] = {"_u", "_v", "_w"};
+  for (int f = 0; f < 3; f++) {
+    snprintf(buf, sizeof buf, "J%s", fs[f]); if (!strcmp(name, buf)) return d.Jf[f];
+  }
+  for (int v = 0; v < 9; v++) {
+    if (!strcmp(name, kMetricNames[v])) return d.m[v];
+    for (int f = 0; f < 3; f++) {
+      snprintf(buf, sizeof buf, "%s%s", kMetricNames[v], fs[f]); if (!strcmp(name, buf)) return d.mf[f][v];
+    }
+  }
+  return nullptr;
+}
+
+int check(cgli_ctx *c) {
+  if (!c) return fail(CGLI_EINVAL, "null context");
+  cudaError_t e = cudaSetDevice(c->device);
+  if (e != cudaSuccess) return fail(CGLI_ECUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+  return CGLI_OK;
+}
+
+int need_ready(cgli_ctx *c) {
+  if (!c->have_metrics) return fail(CGLI_ESTATE, "metrics not set (cgli_channel_metrics / cgli_set_array)");
+  if (!c->have_state) return fail(CGLI_ESTATE, "state not set (cgli_set_state)");
+  return CGLI_OK;
+}
+
+int last_launch(const char *what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(CGLI_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  return CGLI_OK;
+}
+
+int read_norms(cgli_ctx *c, double er[5]) {
+  double scale = 1.0 / ((double)c->p.nx * c->p.ny * c->p.nz);
+  cgli::launch_norms(c->d, c->stream, c->update_blocks, scale, c->d_out);
+  CUDA_TRY(cudaMemcpyAsync(c->h_norms, c->d_out, 5 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  for (int v = 0; v < 5; v++) er[v] = c->h_norms[v];
+  for (int v = 0; v < 5; v++)
+    if (!std::isfinite(er[v])) return fail(CGLI_EDIVERGED, "update norm is not finite");
+  return CGLI_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *cgli_last_error(void) { return g_err.c_str(); }
+
+long long cgli_device_bytes(const cgli_ctx *ctx) { return ctx ? ctx->bytes : 0; }
+
+int cgli_create(const cgli_params *p, cgli_ctx **out) {
+  if (!p || !out) return fail(CGLI_EINVAL, "null argument");
+  *out = nullptr;
+  if (p->nx < 3 || p->ny < 6 || p->nz < 4)
+    return fail(CGLI_EINVAL, "grid too small: need Nx >= 3, Ny >= 6, Nz >= 4 (reduced wall stencils)");
+  if (p->precision != CGLI_FP64 && p->precision != CGLI_MIXED)
+    return fail(CGLI_EINVAL, "precision must be CGLI_FP64 or CGLI_MIXED");
+  if (!(p->dxi > 0 && p->det > 0 && p->dzt > 0 && p->dt > 0 && p->e > 0 && p->mu > 0 && p->pr > 0))
+    return fail(CGLI_EINVAL, "spacings, time step, e, mu and Pr must be positive");
+  cgli_ctx *c = new cgli_ctx();
+  c->p = *p;
+  cudaError_t e = cudaGetDevice(&c->device);
+  if (e != cudaSuccess) { delete c; return fail(CGLI_ECUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e)); }
+  cgli::Dev &d = c->d;
+  memset(&d, 0, sizeof d);
+  d.nx = p->nx; d.ny = p->ny; d.nz = p->nz;
+  d.X = p->nx + 6; d.Y = p->ny + 4; d.Z = p->nz + 4;
+  d.dj = d.Z; d.di = (long long)d.Y * d.Z;
+  d.dxi = p->dxi; d.det = p->det; d.dzt = p->dzt; d.dt = p->dt; d.e = p->e;
+  d.mu = p->mu; d.pr = p->pr; d.twl = p->twall_lo; d.twh = p->twall_hi;
+  int rc = CGLI_OK;
+#define F(x) if (rc == CGLI_OK) rc = field(c, &(x))
+  for (int v = 0; v < 5; v++) {
+    F(d.U_[v]); F(d.U[v]); F(d.Uq[v]); F(d.MR[v]); F(d.NL[v]); F(d.NR[v]);
+    for (int f = 0; f < 3; f++) F(d.inF[f][v]);
+  }
+  for (int v = 0; v < 4; v++) {
+    F(d.vF[v]); F(d.vprim[v]);
+    for (int f = 0; f < 3; f++) F(d.vflux[f][v]);
+  }
+  F(d.J);
+  for (int v = 0; v < 9; v++) F(d.m[v]);
+  for (int f = 0; f < 3; f++) {
+    F(d.Jf[f]);
+    for (int v = 0; v < 9; v++) F(d.mf[f][v]);
+  }
+#undef F
+  if (rc == CGLI_OK) rc = alloc(c, 16 * sizeof(double), (void **)&d.scal);
+  if (rc == CGLI_OK) rc = alloc(c, 16 * sizeof(double), (void **)&c->d_out);
+  if (rc == CGLI_OK) rc = alloc(c, 16 * sizeof(int), (void **)&d.status);
+  c->update_blocks = p->nx * p->ny;
+  if (rc == CGLI_OK) rc = alloc(c, 5 * sizeof(double) * (size_t)c->update_blocks, (void **)&d.partial);
+  if (rc == CGLI_OK && cudaMallocHost(&c->h_norms, 16 * sizeof(double)) != cudaSuccess)
+    rc = fail(CGLI_ENOMEM, "cudaMallocHost");
+  if (rc == CGLI_OK && cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+    rc = fail(CGLI_ECUDA, "cudaStreamCreate");
+  if (rc != CGLI_OK) {
+    std::string keep = g_err;
+    cgli_destroy(c);
+    g_err = keep;
+    return rc;
+  }
+  double f = p->force;
+  cudaMemcpy(d.scal, &f, sizeof f, cudaMemcpyHostToDevice);
+  *out = c;
+  return CGLI_OK;
+}
+
+int cgli_destroy(cgli_ctx *c) {
+  if (!c) return CGLI_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->iter_graph) cudaGraphExecDestroy(c->iter_graph);
+  if (c->dts_graph) cudaGraphExecDestroy(c->dts_graph);
+  for (void *p : c->allocs) cudaFree(p);
+  if (c->h_norms) cudaFreeHost(c->h_norms);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return CGLI_OK;
+}
+
+int cgli_set_array(cgli_ctx *c, const char *name, const double *host) {
+  int rc = check(c); if (rc) return rc;
+  if (!name || !host) return fail(CGLI_EINVAL, "null argument");
+  bool is_metric = false;
+  double *dst = lookup(c, name, &is_metric);
+  if (!dst) return fail(CGLI_EINVAL, std::string("unknown array ") + name);
+  size_t n = (size_t)c->d.X * c->d.Y * c->d.Z;
+  CUDA_TRY(cudaMemcpyAsync(dst, host, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (is_metric) c->have_metrics = true;
+  return CGLI_OK;
+}
+
+int cgli_get_array(cgli_ctx *c, const char *name, double *host) {
+  int rc = check(c); if (rc) return rc;
+  if (!name || !host) return fail(CGLI_EINVAL, "null argument");
+  double *src = lookup(c, name);
+  if (!src) return fail(CGLI_EINVAL, std::string("unknown array ") + name);
+  size_t n = (size_t)c->d.X * c->d.Y * c->d.Z;
+  CUDA_TRY(cudaMemcpyAsync(host, src, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return CGLI_OK;
+}
+
+int cgli_channel_metrics(cgli_ctx *c, double high, double stretch) {
+  int rc = check(c); if (rc) return rc;
+  if (!(high > 0 && stretch > 0)) return fail(CGLI_EINVAL, "high and stretch must be positive");
+  cgli::MetricSet M;
+  cgli::channel_metrics(c->p.nx, c->p.ny, c->p.nz, c->p.det, high, stretch, M);
+  size_t n = (size_t)c->d.X * c->d.Y * c->d.Z;
+  CUDA_TRY(cudaMemcpyAsync(c->d.J, M.J.data(), n * 8, cudaMemcpyHostToDevice, c->stream));
+  for (int v = 0; v < 9; v++) CUDA_TRY(cudaMemcpyAsync(c->d.m[v], M.m[v].data(), n * 8, cudaMemcpyHostToDevice, c->stream));
+  for (int f = 0; f < 3; f++) {
+    CUDA_TRY(cudaMemcpyAsync(c->d.Jf[f], M.Jf[f].data(), n * 8, cudaMemcpyHostToDevice, c->stream));
+    for (int v = 0; v < 9; v++)
+      CUDA_TRY(cudaMemcpyAsync(c->d.mf[f][v], M.mf[f][v].data(), n * 8, cudaMemcpyHostToDevice, c->stream));
+  }
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->have_metrics = true;
+  return CGLI_OK;
+}
+
+int cgli_set_state(cgli_ctx *c, const double *const U_[5], const double *const U[5], const double *const Uq[5]) {
+  int rc = check(c); if (rc) return rc;
+  if (!U_ || !U || !Uq) return fail(CGLI_EINVAL, "null argument");
+  size_t n = (size_t)c->d.X * c->d.Y * c->d.Z * sizeof(double);
+  for (int v = 0; v < 5; v++) {
+    if (!U_[v] || !U[v] || !Uq[v]) return fail(CGLI_EINVAL, "null state array");
+    CUDA_TRY(cudaMemcpyAsync(c->d.U_[v], U_[v], n, cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(c->d.U[v], U[v], n, cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(c->d.Uq[v], Uq[v], n, cudaMemcpyHostToDevice, c->stream));
+  }
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->have_state = true;
+  return CGLI_OK;
+}
+
+int cgli_get_state(cgli_ctx *c, double *const U_[5]) {
+  int rc = check(c); if (rc) return rc;
+  if (!U_) return fail(CGLI_EINVAL, "null argument");
+  size_t n = (size_t)c->d.X * c->d.Y * c->d.Z * sizeof(double);
+  for (int v = 0; v < 5; v++) {
+    if (!U_[v]) return fail(CGLI_EINVAL, "null state array");
+    CUDA_TRY(cudaMemcpyAsync(U_[v], c->d.U_[v], n, cudaMemcpyDeviceToHost, c->stream));
+  }
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return CGLI_OK;
+}
+
+#define SIMPLE_ENTRY(name, launcher, what)                  \
+  int name(cgli_ctx *c) {                                   \
+    int rc = check(c); if (rc) return rc;                   \
+    rc = need_ready(c); if (rc) return rc;                  \
+    cgli::launcher(c->d, c->stream);                        \
+    rc = last_launch(what); if (rc) return rc;              \
+    CUDA_TRY(cudaStreamSynchronize(c->stream));             \
+    return CGLI_OK;                                         \
+  }
+
+SIMPLE_ENTRY(cgli_halo_x, launch_halo_x, "halo_x")
+SIMPLE_ENTRY(cgli_y_boundary_condition, launch_bc_y, "y_boundary_condition")
+SIMPLE_ENTRY(cgli_z_boundary_condition, launch_bc_z, "z_boundary_condition")
+SIMPLE_ENTRY(cgli_flux_x, launch_flux_x, "flux_x")
+SIMPLE_ENTRY(cgli_flux_y, launch_flux_y, "flux_y")
+SIMPLE_ENTRY(cgli_flux_z, launch_flux_z, "flux_z")
+SIMPLE_ENTRY(cgli_viscous_terms, launch_viscous, "viscous_terms")
+
+int cgli_dual_time_stepping(cgli_ctx *c, double er[5]) {
+  int rc = check(c); if (rc) return rc;
+  rc = need_ready(c); if (rc) return rc;
+  if (!er) return fail(CGLI_EINVAL, "null er");
+  cgli::launch_dts(c->d, c->stream, c->update_blocks);
+  rc = last_launch("dual_time_stepping"); if (rc) return rc;
+  return read_norms(c, er);
+}
+
+int cgli_inner_iteration(cgli_ctx *c, double er[5]) {
+  int rc = check(c); if (rc) return rc;
+  rc = need_ready(c); if (rc) return rc;
+  if (!er) return fail(CGLI_EINVAL, "null er");
+  if (!c->iter_graph) {
+    cudaGraph_t g;
+    CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    cgli::launch_fused_iteration(c->d, c->stream, c->p.precision, c->update_blocks);
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (e != cudaSuccess) return fail(CGLI_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&c->iter_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(CGLI_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  }
+  CUDA_TRY(cudaGraphLaunch(c->iter_graph, c->stream));
+  return read_norms(c, er);
+}
+
+int cgli_driven_force(cgli_ctx *c, double *bulk_flux) {
+  int rc = check(c); if (rc) return rc;
+  rc = need_ready(c); if (rc) return rc;
+  if (!bulk_flux) return fail(CGLI_EINVAL, "null argument");
+  cgli::launch_bulk_flux(c->d, c->stream, c->d_out);
+  rc = last_launch("driven_force"); if (rc) return rc;
+  CUDA_TRY(cudaMemcpyAsync(c->h_norms, c->d_out, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  *bulk_flux = c->h_norms[0];
+  return CGLI_OK;
+}
+
+int cgli_end_step(cgli_ctx *c) {
+  int rc = check(c); if (rc) return rc;
+  rc = need_ready(c); if (rc) return rc;
+  cgli::launch_end_step(c->d, c->stream);
+  rc = last_launch("end_step"); if (rc) return rc;
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return CGLI_OK;
+}
+
+int cgli_set_force(cgli_ctx *c, double force) {
+  int rc = check(c); if (rc) return rc;
+  c->p.force = force;
+  CUDA_TRY(cudaMemcpyAsync(c->d.scal, &c->p.force, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return CGLI_OK;
+}
+
+int cgli_step(cgli_ctx *c, int fixed_iters, double drop, int cap, int *iters, double er[5]) {
+  int rc = check(c); if (rc) return rc;
+  if (!iters || !er) return fail(CGLI_EINVAL, "null argument");
+  if (fixed_iters <= 0 && (cap <= 0 || !(drop > 0))) return fail(CGLI_EINVAL, "need fixed_iters > 0 or cap > 0 and drop > 0");
+  double first[5] = {1, 1, 1, 1, 1};
+  int it = 0;
+  while (true) {
+    it++;
+    rc = cgli_inner_iteration(c, er);
+    if (rc) return rc;
+    if (it == 1)
+      for (int v = 0; v < 5; v++) first[v] = er[v] > 0 ? er[v] : 1.0;
+    if (fixed_iters > 0) {
+      if (it >= fixed_iters) break;
+    } else {
+      bool done = true;
+      for (int v = 0; v < 5; v++) done = done && (er[v] / first[v] < drop);
+      if (done || it >= cap) break;
+    }
+  }
+  *iters = it;
+  return cgli_end_step(c);
+}
+
+int cgli_channel_metrics_host(int nx, int ny, int nz, double det, double high, double stretch,
+                              const char *name, double *out) {
+  if (!name || !out || nx < 1 || ny < 1 || nz < 1 || !(det > 0 && high > 0 && stretch > 0))
+    return fail(CGLI_EINVAL, "bad argument");
+  cgli::MetricSet M;
+  cgli::channel_metrics(nx, ny, nz, det, high, stretch, M);
+  const std::vector<double> *src = nullptr;
+  if (!strcmp(name, "J")) src = &M.J;
+  const char *fs[3] = {"J_u", "J_v", "J_w"};
+  const char *sfx[3] = {"_u", "_v", "_w"};
+  char buf[32];
+  for (int f = 0; f < 3 && !src; f++)
+    if (!strcmp(name, fs[f])) src = &M.Jf[f];
+  for (int v = 0; v < 9 && !src; v++) {
+    if (!strcmp(name, kMetricNames[v])) src = &M.m[v];
+    for (int f = 0; f < 3 && !src; f++) {
+      snprintf(buf, sizeof buf, "%s%s", kMetricNames[v], sfx[f]);
+      if (!strcmp(name, buf)) src = &M.mf[f][v];
+    }
+  }
+  if (!src) return fail(CGLI_EINVAL, std::string("unknown metric ") + name);
+  memcpy(out, src->data(), src->size() * sizeof(double));
+  return CGLI_OK;
+}
+
+int cgli_hyperplane(int nx, int ny, int nz, int *Nijk, long nijk_len, int *ijk, long ijk_len) {
+  if (!Nijk || !ijk || nx < 1 || ny < 1 || nz < 1) return fail(CGLI_EINVAL, "bad argument");
+  if (!cgli::hyperplane(nx, ny, nz, Nijk, nijk_len, ijk, ijk_len)) return fail(CGLI_EINVAL, "buffers too small");
+  return CGLI_OK;
+}
+
+}  // extern "C"

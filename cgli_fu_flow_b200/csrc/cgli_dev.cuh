@@ -1,0 +1,269 @@
+// Device-side state description and the per-cell / per-face arithmetic of
+// the hot path, shared by every kernel translation unit.
+//
+// All arrays use the reference layout [X_np][Y_m][Z_m], k fastest (see
+// include/cgli_fu_flow.h).  The arithmetic helpers restate the reference's
+// expressions in the same evaluation order (file:line cited at each); the
+// compiler may contract a*b+c into fused multiply-adds, so results agree
+// with the CPU reference to rounding, not bit for bit.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace cgli {
+
+constexpr double KG = 1.4;    // gamma, prm.h:7
+constexpr double RG = 287.0;  // gas constant, prm.h:8
+constexpr double CV = 717.5;  // Viscous_terms.h:3
+
+// Pointers and sizes of one context's device state; passed by value.
+struct Dev {
+  int nx, ny, nz;         // interior cells
+  int X, Y, Z;            // X_np, Y_m, Z_m
+  long long di, dj;       // strides of i and j (k stride is 1)
+  double dxi, det, dzt, dt, e, mu, pr, twl, twh;
+  double *U_[5], *U[5], *Uq[5];
+  double *J, *m[9];
+  double *Jf[3], *mf[3][9];
+  double *inF[3][5], *vF[4];
+  double *MR[5], *NL[5], *NR[5];
+  double *vflux[3][4];
+  double *vprim[4];
+  double *scal;           // [0] = driving force
+  double *partial;        // per-block partial sums of the update norms
+  int *status;            // device status word (0 ok)
+  // mixed-precision sweep state
+  float *MRf[5], *NLf[5], *NRf[5];
+};
+
+__host__ __device__ __forceinline__ long long ix(const Dev &d, int i, int j, int k) {
+  return (long long)i * d.di + (long long)j * d.dj + k;
+}
+
+// ---------------------------------------------------------------- MUSCL
+// 1/J-weighted upwind-biased interpolation of Q/J (Flux_X.cpp:112-126 and
+// the reduced stencils of Flux_X.cpp:138-216, Flux_Y.cpp:135-250,
+// Flux_Z.cpp:135-216).
+__device__ __forceinline__ double m5L(const double *u, const double *J, long long a, long long b,
+                                      long long c, long long dd, long long e) {
+  double t = 1. / (2 / J[a] - 13 / J[b] + 47 / J[c] + 27 / J[dd] - 3 / J[e]);
+  return t * (2 * u[a] - 13 * u[b] + 47 * u[c] + 27 * u[dd] - 3 * u[e]);
+}
+__device__ __forceinline__ double m5R(const double *u, const double *J, long long a, long long b,
+                                      long long c, long long dd, long long e) {
+  double t = 1. / (-3 / J[a] + 27 / J[b] + 47 / J[c] - 13 / J[dd] + 2 / J[e]);
+  return t * (-3 * u[a] + 27 * u[b] + 47 * u[c] - 13 * u[dd] + 2 * u[e]);
+}
+__device__ __forceinline__ double m3L(const double *u, const double *J, long long a, long long b, long long c) {
+  double t = 1. / (-1 / J[a] + 5 / J[b] + 2 / J[c]);
+  return t * (-u[a] + 5 * u[b] + 2 * u[c]);
+}
+__device__ __forceinline__ double m3R(const double *u, const double *J, long long a, long long b, long long c) {
+  double t = 1. / (2 / J[a] + 5 / J[b] - 1 / J[c]);
+  return t * (2 * u[a] + 5 * u[b] - u[c]);
+}
+__device__ __forceinline__ double m2(const double *u, const double *J, long long a, long long b) {
+  double t = 1. / (1 / J[a] + 1 / J[b]);
+  return t * (u[a] + u[b]);
+}
+
+// ------------------------------------------------------------- Roe flux
+// Preconditioned Roe flux through one face, Flux_X.cpp:229-350 (same
+// statements in Flux_Y.cpp:291-396 and Flux_Z.cpp:250-354; the pressure-jump
+// term uses the face's own unit normal).  L, R: MUSCL states; (mx,my,mz)
+// face metric; Jf face Jacobian.  Also returns Fav3 and iP+P_ for the wall
+// faces of Flux_Y.cpp:400-408.
+__device__ __forceinline__ void roe_face(const double L[5], const double R[5], double mx, double my,
+                                         double mz, double Jf, double e, double F[5], double &Fav3o,
+                                         double &ppo) {
+  double insqr = 1.0 / sqrt(mx * mx + my * my + mz * mz);
+  double NX = mx * insqr, NY = my * insqr, NZ = mz * insqr;
+  double _rho = L[0], _u = L[1] / _rho, _v = L[2] / _rho, _w = L[3] / _rho;
+  double iU = mx * _u + my * _v + mz * _w;
+  double _VV = _u * _u + _v * _v + _w * _w;
+  double iP = (L[4] - 0.5 * _rho * _VV) * (KG - 1);
+  double iC = KG * iP / _rho;
+  double _H = 0.5 * _VV + iC / (KG - 1);
+  double rho_ = R[0], u_ = R[1] / rho_, v_ = R[2] / rho_, w_ = R[3] / rho_;
+  double U_ = mx * u_ + my * v_ + mz * w_;
+  double VV_ = u_ * u_ + v_ * v_ + w_ * w_;
+  double P_ = (R[4] - 0.5 * rho_ * VV_) * (KG - 1);
+  double C_ = KG * P_ / rho_;
+  double H_ = 0.5 * VV_ + C_ / (KG - 1);
+  double temp5 = sqrt(_rho), temp6 = sqrt(rho_);
+  double temp4 = temp5 + temp6;
+  double rho = sqrt(_rho * rho_);
+  double u = (temp5 * _u + temp6 * u_) / temp4;
+  double v = (temp5 * _v + temp6 * v_) / temp4;
+  double w = (temp5 * _w + temp6 * w_) / temp4;
+  double U = (temp5 * iU + temp6 * U_) / temp4;
+  double VV = u * u + v * v + w * w;
+  double H = (temp5 * _H + temp6 * H_) / temp4;
+  double C = (H - 0.5 * VV) * (KG - 1);
+  double dU1 = rho_ - _rho;
+  double dU2 = rho_ * u_ - _rho * _u;
+  double dU3 = rho_ * v_ - _rho * _v;
+  double dU4 = rho_ * w_ - _rho * _w;
+  double dU5 = (P_ / (KG - 1) + 0.5 * rho_ * VV_) - (iP / (KG - 1) + 0.5 * _rho * _VV);
+  double beta = VV / C > e ? VV / C : e;   // max() macro semantics
+  double temp = 0.5 * (1 + beta) * U * insqr;
+  double S = 0.5 * sqrt(4 * beta * C + U * insqr * U * insqr * (1 - beta) * (1 - beta));
+  double theda_p = VV / C;
+  double U_p = 0.5 * (1 + theda_p) * U * insqr;
+  double C_p = 0.5 * sqrt(4 * C * theda_p + U * insqr * U * insqr * (1 - theda_p) * (1 - theda_p));
+  double temp1 = (P_ - iP) / rho / beta / C;
+  double temp2 = U_p / S * (U_ - iU) * insqr;
+  double temp3 = 0.5 * (1 - beta) * U * insqr * temp / S;
+  temp4 = 0.5 * (1 - theda_p) * U * insqr * U_p / S;
+  double deltaU = (S - temp3 - beta * fabs(U) * insqr) * temp1 + temp2;
+  double deltaP = U_p / S * (P_ - iP) + (C_p - fabs(U) * insqr + temp4) * rho * (U_ - iU) * insqr;
+  double aU = fabs(U * insqr);
+  double Fav1 = aU * dU1 + deltaU * rho;
+  double Fav2 = aU * dU2 + deltaU * rho * u + deltaP * NX;
+  double Fav3 = aU * dU3 + deltaU * rho * v + deltaP * NY;
+  double Fav4 = aU * dU4 + deltaU * rho * w + deltaP * NZ;
+  double Fav5 = aU * dU5 + deltaU * rho * H + deltaP * U * insqr;
+  F[0] = 0.5 * ((_rho * iU + rho_ * U_) - Fav1 / insqr) / Jf;
+  F[1] = 0.5 * ((_rho * _u * iU + rho_ * u_ * U_ + mx * (iP + P_)) - Fav2 / insqr) / Jf;
+  F[2] = 0.5 * ((_rho * _v * iU + rho_ * v_ * U_ + my * (iP + P_)) - Fav3 / insqr) / Jf;
+  F[3] = 0.5 * ((_rho * _w * iU + rho_ * w_ * U_ + mz * (iP + P_)) - Fav4 / insqr) / Jf;
+  F[4] = 0.5 * ((iU * (3.5 * iP + 0.5 * _rho * _VV) + U_ * (3.5 * P_ + 0.5 * rho_ * VV_)) - Fav5 / insqr) / Jf;
+  Fav3o = Fav3;
+  ppo = iP + P_;
+}
+
+// ------------------------------------------------ dual-time primitives
+// Primitive state of one cell as Dual_time_stepping.cpp:759-769 forms it.
+template <typename T>
+struct CPrim {
+  T rho, u, v, w, VV, P, C, Tt, H, beta;
+};
+
+template <typename T>
+__device__ __forceinline__ CPrim<T> cprim(T q1, T q2, T q3, T q4, T q5, T J, T e) {
+  CPrim<T> r;
+  const T K = (T)KG;
+  r.rho = q1 * J;
+  r.u = q2 / q1;
+  r.v = q3 / q1;
+  r.w = q4 / q1;
+  r.VV = r.u * r.u + r.v * r.v + r.w * r.w;
+  r.P = (q5 * J - (T)0.5 * r.rho * r.VV) * (K - 1);
+  r.C = K * r.P / r.rho;
+  r.Tt = r.P / r.rho;
+  r.H = (T)0.5 * r.VV + r.C / (K - 1);
+  r.beta = r.VV / r.C > e ? r.VV / r.C : e;
+  return r;
+}
+
+// Own LU-SGS diagonal of one cell, Dual_time_stepping.cpp:853-895.
+template <typename T>
+struct Diag {
+  T d11, d22, d51;
+};
+
+template <typename T>
+__device__ __forceinline__ Diag<T> diag(const CPrim<T> &q, const T mm[9], T dxi, T det, T dzt, T deltaT) {
+  const T K = (T)KG;
+  T beta = q.beta, C = q.C;
+  T U = mm[0] * q.u + mm[1] * q.v + mm[2] * q.w;
+  T V = mm[3] * q.u + mm[4] * q.v + mm[5] * q.w;
+  T W = mm[6] * q.u + mm[7] * q.v + mm[8] * q.w;
+  T Sx = sqrt(U * U * (beta - 1) * (beta - 1) + 4 * beta * C * (mm[0] * mm[0] + mm[1] * mm[1] + mm[2] * mm[2]));
+  T Sy = sqrt(V * V * (beta - 1) * (beta - 1) + 4 * beta * C * (mm[3] * mm[3] + mm[4] * mm[4] + mm[5] * mm[5]));
+  T Sz = sqrt(W * W * (beta - 1) * (beta - 1) + 4 * beta * C * (mm[6] * mm[6] + mm[7] * mm[7] + mm[8] * mm[8]));
+  T lambdaX = ((beta + 1) * fabs(U) + Sx) / 2;
+  T lambdaY = ((beta + 1) * fabs(V) + Sy) / 2;
+  T lambdaZ = ((beta + 1) * fabs(W) + Sz) / 2;
+  T lambda = lambdaX / dxi + lambdaY / det + lambdaZ / dzt;
+  Diag<T> d;
+  d.d11 = 2 * deltaT / (3 * beta + 2 * lambda * deltaT);
+  d.d22 = 2 * deltaT / (3 + 2 * lambda * deltaT);
+  T temp1 = 6 * (K - 1) * (beta - 1) * deltaT;
+  T temp2 = K * (3 + 2 * lambda * deltaT) * (3 * beta + 2 * lambda * deltaT) * q.rho;
+  d.d51 = -temp1 / temp2;
+  return d;
+}
+
+// Split Jacobian of a neighbour in one direction: A+ entries of
+// Dual_time_stepping.cpp:1054-1072 (B+ :1103-1121, C+ :1152-1170) and the
+// A- diagonals of :1405-1409.  `xdir` selects the x product order of row 5.
+template <typename T>
+struct Split {
+  T p11, p12, p13, p14, p21, p22, p31, p41, p51, p52, p53, p54, m11, m22;
+};
+
+template <typename T>
+__device__ __forceinline__ Split<T> split(const CPrim<T> &q, T mx, T my, T mz, bool xdir) {
+  const T K = (T)KG;
+  T beta = q.beta, U = mx * q.u + my * q.v + mz * q.w;
+  T Sx = sqrt(U * U * (beta - 1) * (beta - 1) + 4 * beta * q.C * (mx * mx + my * my + mz * mz));
+  T lambdaX = ((beta + 1) * fabs(U) + Sx) / 2;
+  T dd = fabs(lambdaX);
+  Split<T> a;
+  a.p11 = (T)0.5 * (beta * U + dd);
+  a.p12 = (T)0.5 * q.P * K * beta * mx;
+  a.p13 = (T)0.5 * q.P * K * beta * my;
+  a.p14 = (T)0.5 * q.P * K * beta * mz;
+  a.p21 = (T)0.5 * mx / q.rho;
+  a.p22 = (T)0.5 * (U + dd);
+  a.p31 = (T)0.5 * my / q.rho;
+  a.p41 = (T)0.5 * mz / q.rho;
+  a.p51 = (T)0.5 * U * (K - 1) * (beta - 1) / q.rho / K;
+  if (xdir) {
+    a.p52 = (T)0.5 * mx * beta * q.Tt * (K - 1);
+    a.p53 = (T)0.5 * my * beta * q.Tt * (K - 1);
+    a.p54 = (T)0.5 * mz * beta * q.Tt * (K - 1);
+  } else {
+    a.p52 = (T)0.5 * beta * q.Tt * (K - 1) * mx;
+    a.p53 = (T)0.5 * beta * q.Tt * (K - 1) * my;
+    a.p54 = (T)0.5 * beta * q.Tt * (K - 1) * mz;
+  }
+  a.m11 = (T)0.5 * (beta * U - dd);
+  a.m22 = (T)0.5 * (U - dd);
+  return a;
+}
+
+// Lower-triangular contribution of one upwind neighbour to LL1..LL5,
+// the parenthesised terms of Dual_time_stepping.cpp:1172-1232.
+template <typename T>
+__device__ __forceinline__ void lower_terms(const Split<T> &A, const T n[5], T o[5]) {
+  o[0] = -A.p11 * n[0] - A.p12 * n[1] - A.p13 * n[2] - A.p14 * n[3];
+  o[1] = -A.p21 * n[0] - A.p22 * n[1];
+  o[2] = -A.p31 * n[0] - A.p22 * n[2];
+  o[3] = -A.p41 * n[0] - A.p22 * n[3];
+  o[4] = -A.p51 * n[0] - A.p52 * n[1] - A.p53 * n[2] - A.p54 * n[3] - A.p22 * n[4];
+}
+// Upper-triangular contribution, Dual_time_stepping.cpp:1529-1590.
+template <typename T>
+__device__ __forceinline__ void upper_terms(const Split<T> &A, const T n[5], T o[5]) {
+  o[0] = +A.m11 * n[0] + A.p12 * n[1] + A.p13 * n[2] + A.p14 * n[3];
+  o[1] = +A.p21 * n[0] + A.m22 * n[1];
+  o[2] = +A.p31 * n[0] + A.m22 * n[2];
+  o[3] = +A.p41 * n[0] + A.m22 * n[3];
+  o[4] = +A.p51 * n[0] + A.p52 * n[1] + A.p53 * n[2] + A.p54 * n[3] + A.m22 * n[4];
+}
+
+// Deterministic block reduction of five partial sums (warp shuffles, then
+// one warp over the per-warp results); thread 0 writes out[0..4].  Requires
+// blockDim.x a multiple of 32 and at most 1024.
+__device__ __forceinline__ void block_sum5(double acc[5], double *out) {
+  __shared__ double red[32][5];
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int v = 0; v < 5; v++)
+    for (int o = 16; o > 0; o >>= 1) acc[v] += __shfl_down_sync(0xffffffffu, acc[v], o);
+  if (lane == 0)
+    for (int v = 0; v < 5; v++) red[warp][v] = acc[v];
+  __syncthreads();
+  if (warp == 0) {
+    double a[5];
+    for (int v = 0; v < 5; v++) a[v] = lane < nw ? red[lane][v] : 0.0;
+    for (int v = 0; v < 5; v++)
+      for (int o = 16; o > 0; o >>= 1) a[v] += __shfl_down_sync(0xffffffffu, a[v], o);
+    if (lane == 0)
+      for (int v = 0; v < 5; v++) out[v] = a[v];
+  }
+}
+
+}  // namespace cgli

@@ -1,0 +1,14 @@
+// Host-side set-up helpers (analytic metrics, hyperplane enumeration).
+#pragma once
+#include <vector>
+
+namespace cgli {
+
+struct MetricSet {
+  std::vector<double> J, m[9], Jf[3], mf[3][9];
+};
+
+void channel_metrics(int nx, int ny, int nz, double det, double high, double g, MetricSet &M);
+bool hyperplane(int nx, int ny, int nz, int *Nijk, long nijk_len, int *ijk, long ijk_len);
+
+}  // namespace cgli

@@ -1,0 +1,513 @@
+// Reference-granularity kernels: one kernel (or a short sequence) per
+// reference routine, reading and writing the same arrays in the same layout
+// as the reference, so every entry point of include/cgli_fu_flow.h can be
+// checked against its counterpart on its own.  The fused fast path of
+// cgli_inner_iteration lives in kernels_fused.cu.
+#include "cgli_dev.cuh"
+#include "cgli_launch.h"
+#include "viscous_face.cuh"
+
+namespace cgli {
+
+// ---------------------------------------------------------------- halos
+// main.cpp:167-200: U_[ie+1..ie+3] <- U_[3..5], U_[0..2] <- U_[ie-2..ie]
+__global__ void k_halo_x(Dev d) {
+  long long plane = d.di;
+  long long n = 3 * plane;
+  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  int v = blockIdx.y;
+  int ie = d.nx + 2;
+  double *q = d.U_[v];
+  q[(long long)(ie + 1) * plane + t] = q[3 * plane + t];
+  q[t] = q[(long long)(ie - 2) * plane + t];
+}
+
+// Y_boundary_condition.cpp:94-182 for interior planes i = 3..ie
+__global__ void k_bc_y(Dev d) {
+  int k = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  int i = 3 + blockIdx.y;
+  int side = blockIdx.z;
+  int jn = d.ny + 1, kn = d.nz + 1;
+  if (k > kn) return;
+  int js = side ? jn : 2, jg = side ? jn + 1 : 1;
+  long long c = ix(d, i, js, k), g = ix(d, i, jg, k);
+  double q1 = d.U_[0][c], q2 = d.U_[1][c], q3 = d.U_[2][c], q4 = d.U_[3][c], q5 = d.U_[4][c];
+  double Jc = d.J[c], Jg = d.J[g];
+  double rho = q1 * Jc;
+  double U = q2 / q1, V = q3 / q1, W = q4 / q1;
+  double VV = U * U + V * V + W * W;
+  double P = (q5 * Jc - 0.5 * rho * VV) * (KG - 1);
+  double T = side ? d.twh : d.twl;
+  rho = P / RG / T;
+  d.U_[0][g] = rho / Jg;
+  d.U_[1][g] = -rho * U / Jg;
+  d.U_[2][g] = -rho * V / Jg;
+  d.U_[3][g] = -rho * W / Jg;
+  d.U_[4][g] = (P / (KG - 1) + 0.5 * rho * VV) / Jg;
+}
+
+// Z_boundary_condition.cpp:39-66: all planes 0..ie+3, all rows 0..nyyy
+__global__ void k_bc_z(Dev d) {
+  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long n = (long long)d.X * d.Y;
+  if (t >= n) return;
+  int v = blockIdx.y;
+  long long row = t * d.dj;
+  int kn = d.nz + 1;
+  double *q = d.U_[v];
+  q[row + 1] = q[row + kn];
+  q[row + kn + 1] = q[row + 2];
+}
+
+// ---------------------------------------------------------------- fluxes
+// x faces i = 2..ie, tangential j = 1..jn-1, k = 1..kn-1 (Flux_X.cpp:96-357)
+__global__ void k_flux_x(Dev d) {
+  int k = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  int j = 1 + blockIdx.y;
+  int i = 2 + blockIdx.z;
+  if (k > d.nz) return;
+  long long f = ix(d, i, j, k);
+  // left state ML[i] from cells i-2..i+2, right state MR[i] from i-1..i+3
+  long long c = ix(d, i, j + 1, k + 1);
+  double L[5], R[5], F[5], fav3, pp;
+  for (int v = 0; v < 5; v++) {
+    L[v] = m5L(d.U_[v], d.J, c - 2 * d.di, c - d.di, c, c + d.di, c + 2 * d.di);
+    R[v] = m5R(d.U_[v], d.J, c - d.di, c, c + d.di, c + 2 * d.di, c + 3 * d.di);
+  }
+  roe_face(L, R, d.mf[0][0][f], d.mf[0][1][f], d.mf[0][2][f], d.Jf[0][f], d.e, F, fav3, pp);
+  for (int v = 0; v < 5; v++) d.inF[0][v][f] = F[v];
+}
+
+// left / right MUSCL states at y face j+1/2 of column (i,k), with the
+// reduced stencils of Flux_Y.cpp:135-250 (valid for Ny >= 6)
+__device__ __forceinline__ void muscl_y(const Dev &d, int v, int i, int j, int k, double &L, double &R) {
+  int jn = d.ny + 1;
+  const double *u = d.U_[v], *J = d.J;
+  long long dj = d.dj;
+  long long c = ix(d, i, j, k);
+  if (j == 1) L = m2(u, J, c, c + dj);
+  else if (j == 2) L = m2(u, J, c, c + dj);
+  else if (j == 3) L = m3L(u, J, c - dj, c, c + dj);
+  else if (j == jn - 1) L = m3L(u, J, c - dj, c, c + dj);
+  else if (j == jn) L = m2(u, J, c, c - dj);
+  else L = m5L(u, J, c - 2 * dj, c - dj, c, c + dj, c + 2 * dj);
+  long long r = c + dj;  // cell j+1
+  if (j == 1) R = m2(u, J, r, r + dj);
+  else if (j == 2) R = m3R(u, J, r - dj, r, r + dj);
+  else if (j == jn - 2) R = m3R(u, J, r - dj, r, r + dj);
+  else if (j == jn - 1) R = m2(u, J, r, r - dj);
+  else if (j == jn) R = m2(u, J, c, c + dj);
+  else R = m5R(u, J, r - 2 * dj, r - dj, r, r + dj, r + 2 * dj);
+}
+
+// y faces j = 1..jn, i = 2..ie-1, k = 1..kn-1 (Flux_Y.cpp:94-413)
+__global__ void k_flux_y(Dev d) {
+  int k = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  int j = 1 + blockIdx.y;
+  int i = 2 + blockIdx.z;
+  if (k > d.nz) return;
+  int jn = d.ny + 1;
+  long long f = ix(d, i, j, k);
+  double L[5], R[5], F[5], fav3, pp;
+  for (int v = 0; v < 5; v++) muscl_y(d, v, i + 1, j, k + 1, L[v], R[v]);
+  double ety = d.mf[1][4][f], Jf = d.Jf[1][f];
+  roe_face(L, R, d.mf[1][3][f], ety, d.mf[1][5][f], Jf, d.e, F, fav3, pp);
+  if (j == 1 || j == jn) {
+    F[0] = 0; F[1] = 0; F[3] = 0; F[4] = 0;
+    F[2] = 0.5 * (ety * pp - 1. * fav3) / Jf;
+  }
+  for (int v = 0; v < 5; v++) d.inF[1][v][f] = F[v];
+}
+
+// left / right states at z face k+1/2 (Flux_Z.cpp:105-216, valid for Nz >= 4)
+__device__ __forceinline__ void muscl_z(const Dev &d, int v, int i, int j, int k, double &L, double &R) {
+  int kn = d.nz + 1;
+  const double *u = d.U_[v], *J = d.J;
+  long long c = ix(d, i, j, k);
+  if (k == 1) L = m2(u, J, c, c + 1);
+  else if (k == 2) L = m3L(u, J, c - 1, c, c + 1);
+  else if (k == kn) L = m3L(u, J, c - 1, c, c + 1);
+  else L = m5L(u, J, c - 2, c - 1, c, c + 1, c + 2);
+  long long r = c + 1;
+  if (k == 1) R = m3R(u, J, r - 1, r, r + 1);
+  else if (k == kn - 1) R = m3R(u, J, r - 1, r, r + 1);
+  else if (k == kn) R = m2(u, J, c, c + 1);
+  else R = m5R(u, J, r - 2, r - 1, r, r + 1, r + 2);
+}
+
+// z faces k = 1..kn, i = 2..ie-1, j = 1..jn-1 (Flux_Z.cpp:91-359)
+__global__ void k_flux_z(Dev d) {
+  int k = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  int j = 1 + blockIdx.y;
+  int i = 2 + blockIdx.z;
+  if (k > d.nz + 1) return;
+  long long f = ix(d, i, j, k);
+  double L[5], R[5], F[5], fav3, pp;
+  for (int v = 0; v < 5; v++) muscl_z(d, v, i + 1, j + 1, k, L[v], R[v]);
+  roe_face(L, R, d.mf[2][6][f], d.mf[2][7][f], d.mf[2][8][f], d.Jf[2][f], d.e, F, fav3, pp);
+  for (int v = 0; v < 5; v++) d.inF[2][v][f] = F[v];
+}
+
+// ---------------------------------------------------------------- viscous
+// velocity and temperature of every cell the viscous face fluxes read
+// (Viscous_terms.cpp:260-394): planes 2..ie+1, rows 1..nyy, k 1..nzz
+__global__ void k_vprim(Dev d) {
+  int k = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  int j = 1 + blockIdx.y;
+  int i = 2 + blockIdx.z;
+  if (k > d.nz + 2) return;
+  long long c = ix(d, i, j, k);
+  double rho = d.U_[0][c];
+  double U = d.U_[1][c] / rho, V = d.U_[2][c] / rho, W = d.U_[3][c] / rho;
+  double P = (d.U_[4][c] - 0.5 * rho * (U * U + V * V + W * W)) * (KG - 1) * d.J[c];
+  double T = P / (rho * RG) / d.J[c];
+  d.vprim[0][c] = U; d.vprim[1][c] = V; d.vprim[2][c] = W; d.vprim[3][c] = T;
+}
+
+struct VP { double U, V, W, T; };
+__device__ __forceinline__ VP vp(const Dev &d, long long c) {
+  VP r; r.U = d.vprim[0][c]; r.V = d.vprim[1][c]; r.W = d.vprim[2][c]; r.T = d.vprim[3][c]; return r;
+}
+
+// face viscous fluxes of cell (i,j,k): x face i-1/2 for j<=jn, k<=kn; y face
+// j-1/2 for i<=ie, k<=kn; z face k-1/2 for i<=ie, j<=jn (the faces the
+// divergence of Viscous_terms.cpp:875-904 reads)
+__global__ void k_viscous_faces(Dev d) {
+  int k = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  int j = 2 + blockIdx.y;
+  int i = 3 + blockIdx.z;
+  int ie = d.nx + 2, jn = d.ny + 1, kn = d.nz + 1;
+  if (k > kn + 1) return;
+  long long c = ix(d, i, j, k);
+  long long f = ix(d, i - 1, j - 1, k - 1);
+  const long long di = d.di, dj = d.dj;
+  VP o = vp(d, c);
+  if (j <= jn && k <= kn) {
+    double out[4];
+    double mm[9];
+    for (int v = 0; v < 9; v++) mm[v] = d.mf[0][v][f];
+    visc_face_x(d.dxi, d.det, d.dzt, d.mu, d.pr, o, vp(d, c - di), vp(d, c + dj), vp(d, c - di + dj), vp(d, c - dj), vp(d, c - di - dj),
+                vp(d, c + 1), vp(d, c - di + 1), vp(d, c - 1), vp(d, c - di - 1), mm, d.Jf[0][f], out);
+    for (int v = 0; v < 4; v++) d.vflux[0][v][c] = out[v];
+  }
+  if (i <= ie && k <= kn) {
+    double out[4];
+    double mm[9];
+    for (int v = 0; v < 9; v++) mm[v] = d.mf[1][v][f];
+    visc_face_y(d.dxi, d.det, d.dzt, d.mu, d.pr, o, vp(d, c - dj), vp(d, c + di), vp(d, c + di - dj), vp(d, c - di), vp(d, c - di - dj),
+                vp(d, c + 1), vp(d, c - dj + 1), vp(d, c - 1), vp(d, c - dj - 1), mm, d.Jf[1][f], out);
+    for (int v = 0; v < 4; v++) d.vflux[1][v][c] = out[v];
+  }
+  if (i <= ie && j <= jn) {
+    double out[4];
+    double mm[9];
+    for (int v = 0; v < 9; v++) mm[v] = d.mf[2][v][f];
+    visc_face_z(d.dxi, d.det, d.dzt, d.mu, d.pr, o, vp(d, c - 1), vp(d, c + di), vp(d, c + di - 1), vp(d, c - di), vp(d, c - di - 1),
+                vp(d, c + dj), vp(d, c + dj - 1), vp(d, c - dj), vp(d, c - dj - 1), vp(d, c - di + dj),
+                mm, d.Jf[2][f], out);
+    for (int v = 0; v < 4; v++) d.vflux[2][v][c] = out[v];
+  }
+}
+
+// Viscous_terms.cpp:875-904
+__global__ void k_viscous_div(Dev d) {
+  int k = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  int j = 2 + blockIdx.y;
+  int i = 3 + blockIdx.z;
+  if (k > d.nz + 1) return;
+  long long c = ix(d, i, j, k);
+  const double invXI = 1. / (d.dxi), invET = 1. / (d.det), invZT = 1. / (d.dzt);
+  for (int v = 0; v < 4; v++)
+    d.vF[v][c] = (d.vflux[0][v][c + d.di] - d.vflux[0][v][c]) * invXI +
+                 (d.vflux[1][v][c + d.dj] - d.vflux[1][v][c]) * invET +
+                 (d.vflux[2][v][c + 1] - d.vflux[2][v][c]) * invZT;
+}
+
+// ---------------------------------------------------- dual-time residual
+// Dual_time_stepping.cpp:737-922 (the sponge Residual terms are zero for a
+// domain without inlet / outlet layers and are left out)
+__global__ void k_dts_residual(Dev d) {
+  int k = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  int j = 2 + blockIdx.y;
+  int i = 3 + blockIdx.z;
+  if (k > d.nz + 1) return;
+  long long c = ix(d, i, j, k);
+  const double J = d.J[c], deltaT = d.dt;
+  CPrim<double> q = cprim<double>(d.U_[0][c], d.U_[1][c], d.U_[2][c], d.U_[3][c], d.U_[4][c], J, d.e);
+  double rho = q.rho, u = q.u, v = q.v, w = q.w, VV = q.VV, T = q.Tt, H = q.H, beta = q.beta;
+  double temp = rho * KG;
+  double d11 = -(H * (KG - 1) + VV - KG * (T + VV)) * beta;
+  double d12 = -(KG - 1) * u * beta, d13 = -(KG - 1) * v * beta, d14 = -(KG - 1) * w * beta;
+  double d15 = (KG - 1) * beta;
+  double d21 = -u / rho, d22 = 1 / rho;
+  double d31 = -v / rho;
+  double d41 = -w / rho;
+  double d51 = (KG - 1) * (VV + KG * T * beta + (KG - 1) * VV * beta + H * (-1 + beta - KG * beta)) / temp;
+  double d52 = -(KG - 1) * u * (1 + (KG - 1) * beta) / temp;
+  double d53 = -(KG - 1) * v * (1 + (KG - 1) * beta) / temp;
+  double d54 = -(KG - 1) * w * (1 + (KG - 1) * beta) / temp;
+  double d55 = (KG - 1) * (1 + (KG - 1) * beta) / temp;
+  long long fx1 = ix(d, i, j - 1, k - 1), fx0 = ix(d, i - 1, j - 1, k - 1);
+  long long fy1 = ix(d, i - 1, j, k - 1), fz1 = ix(d, i - 1, j - 1, k);
+  double Rk[5];
+  double f = d.scal[0];
+  for (int n = 0; n < 5; n++) {
+    double Rp = -(3 * d.U_[n][c] - 4 * d.U[n][c] + d.Uq[n][c]) / (2 * deltaT);
+    double Rf = -((d.inF[0][n][fx1] - d.inF[0][n][fx0]) / d.dxi + (d.inF[1][n][fy1] - d.inF[1][n][fx0]) / d.det +
+                  (d.inF[2][n][fz1] - d.inF[2][n][fx0]) / d.dzt);
+    Rk[n] = Rp + Rf;
+  }
+  Rk[1] = Rk[1] + d.vF[0][c] + f / J;
+  Rk[2] = Rk[2] + d.vF[1][c];
+  Rk[3] = Rk[3] + d.vF[2][c];
+  Rk[4] = Rk[4] + d.vF[3][c] + f * u / J;
+  double MR1 = (d11 * Rk[0] + d12 * Rk[1] + d13 * Rk[2] + d14 * Rk[3] + d15 * Rk[4]);
+  double MR2 = (d21 * Rk[0] + d22 * Rk[1]);
+  double MR3 = (d31 * Rk[0] + d22 * Rk[2]);
+  double MR4 = (d41 * Rk[0] + d22 * Rk[3]);
+  double MR5 = (d51 * Rk[0] + d52 * Rk[1] + d53 * Rk[2] + d54 * Rk[3] + d55 * Rk[4]);
+  d.MR[0][c] = MR1; d.MR[1][c] = MR2; d.MR[2][c] = MR3; d.MR[3][c] = MR4; d.MR[4][c] = MR5;
+  double mm[9];
+  for (int v2 = 0; v2 < 9; v2++) mm[v2] = d.m[v2][c];
+  Diag<double> dd = diag<double>(q, mm, d.dxi, d.det, d.dzt, deltaT);
+  double n1 = dd.d11 * MR1, n2 = dd.d22 * MR2, n3 = dd.d22 * MR3, n4 = dd.d22 * MR4;
+  double n5 = dd.d51 * MR1 + dd.d22 * MR5;
+  d.NL[0][c] = n1; d.NL[1][c] = n2; d.NL[2][c] = n3; d.NL[3][c] = n4; d.NL[4][c] = n5;
+  d.NR[0][c] = n1; d.NR[1][c] = n2; d.NR[2][c] = n3; d.NR[3][c] = n4; d.NR[4][c] = n5;
+}
+
+// ------------------------------------------------------------- sweeps
+// lagged periodic halo planes of the sweep, Dual_time_stepping.cpp:942-976:
+// NL[2] <- NL[ie], NR[ie+1] <- NR[3]
+__global__ void k_sweep_halo(Dev d) {
+  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= d.di) return;
+  int v = blockIdx.y;
+  int ie = d.nx + 2;
+  d.NL[v][2 * d.di + t] = d.NL[v][(long long)ie * d.di + t];
+  d.NR[v][(long long)(ie + 1) * d.di + t] = d.NR[v][3 * d.di + t];
+}
+
+__device__ __forceinline__ CPrim<double> cp_at(const Dev &d, long long c) {
+  return cprim<double>(d.U_[0][c], d.U_[1][c], d.U_[2][c], d.U_[3][c], d.U_[4][c], d.J[c], d.e);
+}
+__device__ __forceinline__ Split<double> split_at(const Dev &d, long long c, int dir) {
+  CPrim<double> q = cp_at(d, c);
+  return split<double>(q, d.m[3 * dir][c], d.m[3 * dir + 1][c], d.m[3 * dir + 2][c], dir == 0);
+}
+
+// forward sweep on hyperplane m = i+j+k, Dual_time_stepping.cpp:983-1300
+__global__ void k_forward_plane(Dev d, int m, int ilo, int jcount) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int i = ilo + t / jcount, j = 2 + t % jcount;
+  int k = m - i - j;
+  int ie = d.nx + 2, kn = d.nz + 1;
+  if (i > ie || k < 2 || k > kn) return;
+  long long c = ix(d, i, j, k), ci = c - d.di, cj = c - d.dj, ck = c - 1;
+  double a[5], b[5], e3[5], n[5];
+  for (int v = 0; v < 5; v++) n[v] = d.NL[v][ci];
+  lower_terms<double>(split_at(d, ci, 0), n, a);
+  for (int v = 0; v < 5; v++) n[v] = d.NL[v][cj];
+  lower_terms<double>(split_at(d, cj, 1), n, b);
+  for (int v = 0; v < 5; v++) n[v] = d.NL[v][ck];
+  lower_terms<double>(split_at(d, ck, 2), n, e3);
+  double LL[5];
+  for (int v = 0; v < 5; v++) LL[v] = a[v] / d.dxi + b[v] / d.det + e3[v] / d.dzt;
+  CPrim<double> q = cp_at(d, c);
+  double mm[9];
+  for (int v = 0; v < 9; v++) mm[v] = d.m[v][c];
+  Diag<double> dg = diag<double>(q, mm, d.dxi, d.det, d.dzt, d.dt);
+  double r1 = d.MR[0][c] - LL[0];
+  d.NL[0][c] = dg.d11 * r1;
+  d.NL[1][c] = dg.d22 * (d.MR[1][c] - LL[1]);
+  d.NL[2][c] = dg.d22 * (d.MR[2][c] - LL[2]);
+  d.NL[3][c] = dg.d22 * (d.MR[3][c] - LL[3]);
+  d.NL[4][c] = dg.d51 * r1 + dg.d22 * (d.MR[4][c] - LL[4]);
+}
+
+// backward sweep on hyperplane m, Dual_time_stepping.cpp:1312-1664
+__global__ void k_backward_plane(Dev d, int m, int ilo, int jcount) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int i = ilo + t / jcount, j = 2 + t % jcount;
+  int k = m - i - j;
+  int ie = d.nx + 2, kn = d.nz + 1;
+  if (i > ie || k < 2 || k > kn) return;
+  long long c = ix(d, i, j, k), ci = c + d.di, cj = c + d.dj, ck = c + 1;
+  double a[5], b[5], e3[5], n[5];
+  for (int v = 0; v < 5; v++) n[v] = d.NR[v][ci];
+  upper_terms<double>(split_at(d, ci, 0), n, a);
+  for (int v = 0; v < 5; v++) n[v] = d.NR[v][cj];
+  upper_terms<double>(split_at(d, cj, 1), n, b);
+  for (int v = 0; v < 5; v++) n[v] = d.NR[v][ck];
+  upper_terms<double>(split_at(d, ck, 2), n, e3);
+  double UU[5];
+  for (int v = 0; v < 5; v++) UU[v] = a[v] / d.dxi + b[v] / d.det + e3[v] / d.dzt;
+  CPrim<double> q = cp_at(d, c);
+  double mm[9];
+  for (int v = 0; v < 9; v++) mm[v] = d.m[v][c];
+  Diag<double> dg = diag<double>(q, mm, d.dxi, d.det, d.dzt, d.dt);
+  d.NR[0][c] = d.NL[0][c] - dg.d11 * UU[0];
+  d.NR[1][c] = d.NL[1][c] - dg.d22 * UU[1];
+  d.NR[2][c] = d.NL[2][c] - dg.d22 * UU[2];
+  d.NR[3][c] = d.NL[3][c] - dg.d22 * UU[3];
+  d.NR[4][c] = d.NL[4][c] - (dg.d51 * UU[0] + dg.d22 * UU[4]);
+}
+
+// NL <- NR on interior cells, Dual_time_stepping.cpp:1675-1689
+__global__ void k_copy_nr_nl(Dev d) {
+  int k = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  int j = 2 + blockIdx.y;
+  int i = 3 + blockIdx.z;
+  if (k > d.nz + 1) return;
+  long long c = ix(d, i, j, k);
+  for (int v = 0; v < 5; v++) d.NL[v][c] = d.NR[v][c];
+}
+
+// --------------------------------------------------------------- update
+// Dual_time_stepping.cpp:1702-1743 plus per-block partial sums of the
+// squared increments (:1761-1776); one block per (j,i) row pair of k
+__global__ void k_update(Dev d) {
+  int k = 2 + threadIdx.x;
+  int j = 2 + blockIdx.x;
+  int i = 3 + blockIdx.y;
+  double acc[5] = {0, 0, 0, 0, 0};
+  for (int kk = k; kk <= d.nz + 1; kk += blockDim.x) {
+    long long c = ix(d, i, j, kk);
+    const double J = d.J[c];
+    double q1 = d.U_[0][c];
+    double rhoold = q1 * J;
+    double Uold = d.U_[1][c] / q1, Vold = d.U_[2][c] / q1, Wold = d.U_[3][c] / q1;
+    double VVold = Uold * Uold + Vold * Vold + Wold * Wold;
+    double Pold = (d.U_[4][c] * J - 0.5 * rhoold * VVold) * (KG - 1);
+    double Told = Pold / rhoold;
+    double P = Pold + d.NR[0][c] * J;
+    double U = Uold + d.NR[1][c] * J;
+    double V = Vold + d.NR[2][c] * J;
+    double W = Wold + d.NR[3][c] * J;
+    double T = Told + d.NR[4][c] * J;
+    double rho = P / T;
+    d.U_[0][c] = rho / J;
+    d.U_[1][c] = rho * U / J;
+    d.U_[2][c] = rho * V / J;
+    d.U_[3][c] = rho * W / J;
+    d.U_[4][c] = (P / (KG - 1) + 0.5 * rho * (U * U + V * V + W * W)) / J;
+    acc[0] += (rho - rhoold) * (rho - rhoold);
+    acc[1] += (U - Uold) * (U - Uold);
+    acc[2] += (V - Vold) * (V - Vold);
+    acc[3] += (W - Wold) * (W - Wold);
+    acc[4] += (T - Told) * (T - Told);
+  }
+  block_sum5(acc, d.partial + 5 * ((long long)blockIdx.y * gridDim.x + blockIdx.x));
+}
+
+// ------------------------------------------------------------ launchers
+static dim3 cellgrid(int nk, int nj, int ni, int bx) { return dim3((nk + bx - 1) / bx, nj, ni); }
+
+void launch_halo_bc(const Dev &d, cudaStream_t s) {
+  long long n = 3 * d.di;
+  k_halo_x<<<dim3((unsigned)((n + 255) / 256), 5), 256, 0, s>>>(d);
+  k_bc_y<<<dim3((d.nz + 127) / 128, d.nx, 2), 128, 0, s>>>(d);
+  long long rows = (long long)d.X * d.Y;
+  k_bc_z<<<dim3((unsigned)((rows + 255) / 256), 5), 256, 0, s>>>(d);
+}
+void launch_halo_x(const Dev &d, cudaStream_t s) {
+  long long n = 3 * d.di;
+  k_halo_x<<<dim3((unsigned)((n + 255) / 256), 5), 256, 0, s>>>(d);
+}
+void launch_bc_y(const Dev &d, cudaStream_t s) {
+  k_bc_y<<<dim3((d.nz + 127) / 128, d.nx, 2), 128, 0, s>>>(d);
+}
+void launch_bc_z(const Dev &d, cudaStream_t s) {
+  long long rows = (long long)d.X * d.Y;
+  k_bc_z<<<dim3((unsigned)((rows + 255) / 256), 5), 256, 0, s>>>(d);
+}
+void launch_flux_x(const Dev &d, cudaStream_t s) {
+  k_flux_x<<<cellgrid(d.nz, d.ny, d.nx + 1, 64), 64, 0, s>>>(d);
+}
+void launch_flux_y(const Dev &d, cudaStream_t s) {
+  k_flux_y<<<cellgrid(d.nz, d.ny + 1, d.nx, 64), 64, 0, s>>>(d);
+}
+void launch_flux_z(const Dev &d, cudaStream_t s) {
+  k_flux_z<<<cellgrid(d.nz + 1, d.ny, d.nx, 64), 64, 0, s>>>(d);
+}
+void launch_viscous(const Dev &d, cudaStream_t s) {
+  k_vprim<<<cellgrid(d.nz + 2, d.ny + 2, d.nx + 2, 64), 64, 0, s>>>(d);
+  k_viscous_faces<<<cellgrid(d.nz + 1, d.ny + 1, d.nx + 1, 64), 64, 0, s>>>(d);
+  k_viscous_div<<<cellgrid(d.nz, d.ny, d.nx, 64), 64, 0, s>>>(d);
+}
+void launch_dts(const Dev &d, cudaStream_t s, int update_blocks_x) {
+  k_dts_residual<<<cellgrid(d.nz, d.ny, d.nx, 64), 64, 0, s>>>(d);
+  int ie = d.nx + 2, jn = d.ny + 1, kn = d.nz + 1;
+  for (int sweep = 1; sweep <= 2; sweep++) {
+    k_sweep_halo<<<dim3((unsigned)((d.di + 255) / 256), 5), 256, 0, s>>>(d);
+    for (int m = 7; m <= ie + jn + kn; m++) {
+      int ilo = m - jn - kn > 3 ? m - jn - kn : 3;
+      int ihi = m - 4 < ie ? m - 4 : ie;
+      int n = (ihi - ilo + 1) * d.ny;
+      k_forward_plane<<<(n + 127) / 128, 128, 0, s>>>(d, m, ilo, d.ny);
+    }
+    for (int m = ie + jn + kn; m >= 7; m--) {
+      int ilo = m - jn - kn > 3 ? m - jn - kn : 3;
+      int ihi = m - 4 < ie ? m - 4 : ie;
+      int n = (ihi - ilo + 1) * d.ny;
+      k_backward_plane<<<(n + 127) / 128, 128, 0, s>>>(d, m, ilo, d.ny);
+    }
+    k_copy_nr_nl<<<cellgrid(d.nz, d.ny, d.nx, 64), 64, 0, s>>>(d);
+  }
+  (void)update_blocks_x;
+  k_update<<<dim3(d.ny, d.nx), 128, 0, s>>>(d);
+}
+
+// five norms from the per-block partial sums, in a fixed order
+__global__ void k_norms(const double *partial, int nblocks, double scale, double *out) {
+  double acc[5] = {0, 0, 0, 0, 0};
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+    for (int v = 0; v < 5; v++) acc[v] += partial[5 * (long long)b + v];
+  __shared__ double tot[5];
+  block_sum5(acc, tot);
+  __syncthreads();
+  if (threadIdx.x < 5) out[threadIdx.x] = sqrt(tot[threadIdx.x]) * scale;
+}
+
+// bulk mass flux, Driven_force.cpp:38-62: sum over interior cells of
+// (U2_*J)/J / Jsum with Jsum the column volume sum at (i,k) = (3,3)
+__global__ void k_bulk_flux(Dev d, double *out) {
+  double acc[5] = {0, 0, 0, 0, 0};
+  double Jsum = 0;
+  for (int j = 2; j <= d.ny + 1; j++) Jsum = Jsum + 1. / d.J[ix(d, 3, j, 3)];
+  long long n = (long long)d.nx * d.ny * d.nz;
+  for (long long t = threadIdx.x; t < n; t += blockDim.x) {
+    int k = (int)(t % d.nz), j = (int)((t / d.nz) % d.ny), i = (int)(t / ((long long)d.nz * d.ny));
+    long long c = ix(d, i + 3, j + 2, k + 2);
+    acc[0] += (d.U_[1][c] * d.J[c]) * 1. / d.J[c] / Jsum;
+  }
+  __shared__ double tot[5];
+  block_sum5(acc, tot);
+  __syncthreads();
+  if (threadIdx.x == 0) out[0] = tot[0] / d.nx / d.nz;
+}
+
+// main.cpp:364-386 over planes 2..ie+1, all rows
+__global__ void k_end_step(Dev d) {
+  long long n = (long long)(d.nx + 2) * d.di;
+  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  int v = blockIdx.y;
+  long long c = 2 * d.di + t;
+  d.Uq[v][c] = d.U[v][c];
+  d.U[v][c] = d.U_[v][c];
+}
+
+void launch_norms(const Dev &d, cudaStream_t s, int nblocks, double scale, double *out) {
+  k_norms<<<1, 1024, 0, s>>>(d.partial, nblocks, scale, out);
+}
+void launch_bulk_flux(const Dev &d, cudaStream_t s, double *out) {
+  k_bulk_flux<<<1, 1024, 0, s>>>(d, out);
+}
+void launch_end_step(const Dev &d, cudaStream_t s) {
+  long long n = (long long)(d.nx + 2) * d.di;
+  k_end_step<<<dim3((unsigned)((n + 255) / 256), 5), 256, 0, s>>>(d);
+}
+
+}  // namespace cgli

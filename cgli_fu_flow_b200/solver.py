@@ -1,0 +1,265 @@
+"""Python mirror of the reference solver's per-step interface over the C ABI
+of include/cgli_fu_flow.h (libcgli_fu_flow.so, built in this directory).
+
+The method names follow the reference routines (Flux_X, Viscous_terms,
+Dual_time_stepping, ...); arrays cross the boundary in the reference layout
+[X_np][Y_m][Z_m] as numpy float64.  There is no CPU fallback: constructing a
+Solver without the CUDA library or without a GPU raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import channel as C
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcgli_fu_flow.so")
+
+FP64 = 0
+MIXED = 1
+
+_ERRORS = {-1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "ESTATE", -5: "EDIVERGED", -6: "ETIMEOUT"}
+
+
+class CgliError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{_ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("dxi", ctypes.c_double), ("det", ctypes.c_double), ("dzt", ctypes.c_double),
+                ("dt", ctypes.c_double), ("e", ctypes.c_double),
+                ("mu", ctypes.c_double), ("pr", ctypes.c_double),
+                ("twall_lo", ctypes.c_double), ("twall_hi", ctypes.c_double),
+                ("force", ctypes.c_double), ("precision", ctypes.c_int)]
+
+
+EXPORTS = [
+    "cgli_create", "cgli_destroy", "cgli_last_error", "cgli_device_bytes", "cgli_set_array",
+    "cgli_get_array", "cgli_channel_metrics", "cgli_set_state", "cgli_get_state", "cgli_halo_x",
+    "cgli_y_boundary_condition", "cgli_z_boundary_condition", "cgli_flux_x", "cgli_flux_y",
+    "cgli_flux_z", "cgli_viscous_terms", "cgli_dual_time_stepping", "cgli_inner_iteration",
+    "cgli_driven_force", "cgli_end_step", "cgli_set_force", "cgli_step", "cgli_hyperplane",
+    "cgli_channel_metrics_host",
+]
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Loads libcgli_fu_flow.so and declares every exported signature."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} missing: build it with python -m cgli_fu_flow_b200.build")
+    L = ctypes.CDLL(path)
+    P = ctypes.c_void_p
+    D = ctypes.c_double
+    DP = ctypes.POINTER(ctypes.c_double)
+    L.cgli_create.argtypes = [ctypes.POINTER(Params), ctypes.POINTER(P)]
+    L.cgli_destroy.argtypes = [P]
+    L.cgli_last_error.restype = ctypes.c_char_p
+    L.cgli_device_bytes.restype = ctypes.c_longlong
+    L.cgli_device_bytes.argtypes = [P]
+    L.cgli_set_array.argtypes = [P, ctypes.c_char_p, P]
+    L.cgli_get_array.argtypes = [P, ctypes.c_char_p, P]
+    L.cgli_channel_metrics.argtypes = [P, D, D]
+    L.cgli_set_state.argtypes = [P, P, P, P]
+    L.cgli_get_state.argtypes = [P, P]
+    for n in ("cgli_halo_x", "cgli_y_boundary_condition", "cgli_z_boundary_condition", "cgli_flux_x",
+              "cgli_flux_y", "cgli_flux_z", "cgli_viscous_terms", "cgli_end_step"):
+        getattr(L, n).argtypes = [P]
+    L.cgli_dual_time_stepping.argtypes = [P, DP]
+    L.cgli_inner_iteration.argtypes = [P, DP]
+    L.cgli_driven_force.argtypes = [P, DP]
+    L.cgli_set_force.argtypes = [P, D]
+    L.cgli_step.argtypes = [P, ctypes.c_int, D, ctypes.c_int, ctypes.POINTER(ctypes.c_int), DP]
+    L.cgli_hyperplane.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, P, ctypes.c_long, P, ctypes.c_long]
+    L.cgli_channel_metrics_host.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, D, D, D, ctypes.c_char_p, P]
+    _lib = L
+    return L
+
+
+def _ptrs(arrs) -> ctypes.Array:
+    return (ctypes.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+
+
+def reference_state(ch: C.Channel, J: np.ndarray, q_n: np.ndarray, q_nm1: np.ndarray):
+    """U_, U, Uq in the reference layout as Initial_condition.cpp:56-221 and
+    main.cpp:127-141 leave them for an interior slab read from a restart file:
+    interior planes filled with the quiescent state over all rows (divided by
+    the cell's J, which is zero -- hence inf/nan -- on the outermost ring,
+    exactly as in the reference with value-initialised arrays), interior
+    cells from the restart data divided by J, x ghost planes zero."""
+    X, Y, Z = ch.shape
+    nx, ny, nz = ch.nx, ch.ny, ch.nz
+    U = np.zeros((5, X, Y, Z))
+    Uq = np.zeros((5, X, Y, Z))
+    T = 298.0592
+    P = 101300.0
+    rho = P / T / C.R_GAS
+    quiet = [rho, rho * 0.0, rho * 0.0, rho * 0.0, P / (C.GAMMA - 1) + 0.5 * rho * 0.0]
+    Js = J[3:nx + 3]
+    with np.errstate(divide="ignore", invalid="ignore"):
+        for v in range(5):
+            U[v, 3:nx + 3] = quiet[v] / Js
+            Uq[v, 3:nx + 3] = quiet[v] / Js
+            Jint = Js[:, 2:ny + 2, 2:nz + 2]
+            U[v, 3:nx + 3, 2:ny + 2, 2:nz + 2] = q_n[v] / Jint
+            Uq[v, 3:nx + 3, 2:ny + 2, 2:nz + 2] = q_nm1[v] / Jint
+    U_ = U.copy()
+    return U_, U, Uq
+
+
+class Solver:
+    """One device context for one channel workload."""
+
+    def __init__(self, ch: C.Channel, precision: int = FP64, e: float | None = None):
+        self.L = load_library()
+        self.ch = ch
+        self.shape = ch.shape
+        self.n = int(np.prod(self.shape))
+        p = Params(ch.nx, ch.ny, ch.nz, ch.dxi, ch.det, ch.dzt, ch.dt,
+                   C.PRECOND_EPS if e is None else e, C.MU0, C.PR, C.T0, C.T0, ch.force_lam, precision)
+        h = ctypes.c_void_p()
+        self._rc(self.L.cgli_create(ctypes.byref(p), ctypes.byref(h)))
+        self.h = h
+        self.force = ch.force_lam
+        self.ctrl: dict = {}
+        self._rc(self.L.cgli_channel_metrics(self.h, ch.high, C.STRETCH))
+
+    def _rc(self, rc: int) -> None:
+        if rc != 0:
+            raise CgliError(rc, self.L.cgli_last_error().decode())
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.L.cgli_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def device_bytes(self) -> int:
+        return self.L.cgli_device_bytes(self.h)
+
+    # ----------------------------------------------------------- arrays
+    def get(self, name: str) -> np.ndarray:
+        out = np.empty(self.shape)
+        self._rc(self.L.cgli_get_array(self.h, name.encode(), out.ctypes.data))
+        return out
+
+    def set(self, name: str, a: np.ndarray) -> None:
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        assert a.shape == self.shape, (a.shape, self.shape)
+        self._rc(self.L.cgli_set_array(self.h, name.encode(), a.ctypes.data))
+
+    def set_state(self, U_: np.ndarray, U: np.ndarray, Uq: np.ndarray) -> None:
+        arrs = [np.ascontiguousarray(x[v], dtype=np.float64) for x in (U_, U, Uq) for v in range(5)]
+        self._keep = arrs
+        self._rc(self.L.cgli_set_state(self.h, _ptrs(arrs[0:5]), _ptrs(arrs[5:10]), _ptrs(arrs[10:15])))
+
+    def init(self, q_n: np.ndarray | None = None, q_nm1: np.ndarray | None = None) -> None:
+        """Seeded initial field through the reference's restart semantics."""
+        if q_n is None:
+            q_n = self.ch.initial_conserved()
+        if q_nm1 is None:
+            q_nm1 = q_n
+        U_, U, Uq = reference_state(self.ch, self.get("J"), q_n, q_nm1)
+        self.set_state(U_, U, Uq)
+        self.set_force(self.force)
+
+    def q(self) -> np.ndarray:
+        out = [np.empty(self.shape) for _ in range(5)]
+        self._rc(self.L.cgli_get_state(self.h, _ptrs(out)))
+        return np.stack(out)
+
+    # ---------------------------------------------------- reference routines
+    def halo_x(self):
+        self._rc(self.L.cgli_halo_x(self.h))
+
+    def y_boundary_condition(self):
+        self._rc(self.L.cgli_y_boundary_condition(self.h))
+
+    def z_boundary_condition(self):
+        self._rc(self.L.cgli_z_boundary_condition(self.h))
+
+    def flux_x(self):
+        self._rc(self.L.cgli_flux_x(self.h))
+
+    def flux_y(self):
+        self._rc(self.L.cgli_flux_y(self.h))
+
+    def flux_z(self):
+        self._rc(self.L.cgli_flux_z(self.h))
+
+    def viscous_terms(self):
+        self._rc(self.L.cgli_viscous_terms(self.h))
+
+    def dual_time_stepping(self) -> np.ndarray:
+        er = (ctypes.c_double * 5)()
+        self._rc(self.L.cgli_dual_time_stepping(self.h, er))
+        return np.array(er[:])
+
+    def inner_iteration(self) -> np.ndarray:
+        er = (ctypes.c_double * 5)()
+        self._rc(self.L.cgli_inner_iteration(self.h, er))
+        return np.array(er[:])
+
+    def bulk_flux(self) -> float:
+        q = ctypes.c_double()
+        self._rc(self.L.cgli_driven_force(self.h, ctypes.byref(q)))
+        return q.value
+
+    def set_force(self, f: float) -> None:
+        self.force = f
+        self._rc(self.L.cgli_set_force(self.h, f))
+
+    def end_step(self, update_force: bool = True) -> None:
+        qb = self.bulk_flux()
+        self._rc(self.L.cgli_end_step(self.h))
+        if update_force:
+            self.set_force(C.force_update(self.ctrl, qb, self.ch))
+
+    def step(self, fixed_iters: int | None = 10, drop: float = 1e-3, cap: int = 30, update_force: bool = True):
+        """One physical step on the device (inner loop in C++), then the
+        force controller update from the converged bulk flux."""
+        it = ctypes.c_int()
+        er = (ctypes.c_double * 5)()
+        self._rc(self.L.cgli_step(self.h, fixed_iters or 0, drop, cap, ctypes.byref(it), er))
+        if update_force:
+            # the time-level shift leaves U_ = Q^(n+1): the converged bulk flux
+            self.set_force(C.force_update(self.ctrl, self.bulk_flux(), self.ch))
+        return it.value, np.array(er[:])
+
+
+def hyperplane_lists(nx: int, ny: int, nz: int):
+    """Nijk, ijk of Hyperplane.cpp through the C ABI (host only)."""
+    L = load_library()
+    nijk = np.zeros((nx + 2 + ny + 1 + nz + 1 + 1, 2), dtype=np.int32)
+    ijk = np.zeros((nx * ny * nz + 1, 3), dtype=np.int32)
+    rc = L.cgli_hyperplane(nx, ny, nz, nijk.ctypes.data, nijk.size, ijk.ctypes.data, ijk.size)
+    if rc:
+        raise CgliError(rc, L.cgli_last_error().decode())
+    return nijk, ijk
+
+
+def channel_metric_host(ch: C.Channel, name: str) -> np.ndarray:
+    """One metric array from the library's host-side generator (no GPU)."""
+    L = load_library()
+    out = np.empty(ch.shape)
+    rc = L.cgli_channel_metrics_host(ch.nx, ch.ny, ch.nz, ch.det, ch.high, C.STRETCH, name.encode(),
+                                     out.ctypes.data)
+    if rc:
+        raise CgliError(rc, L.cgli_last_error().decode())
+    return out

@@ -1,0 +1,135 @@
+/*
+ * cgli_fu_flow.h -- C ABI of the B200 implementation of the CGLI_Fu_Flow
+ * per-step hot path (MUSCL-5 / preconditioned Roe fluxes, viscous terms,
+ * BDF2 dual-time residual, two symmetric LU-SGS i+j+k wavefront sweeps,
+ * primitive update and residual norms, wall / periodic boundaries and the
+ * driving force), on one GPU.
+ *
+ * Conventions shared by every entry point:
+ *   - plain C types only; every call returns 0 on success and a negative
+ *     CGLI_E* code on failure, with a message from cgli_last_error();
+ *   - the caller owns host buffers; the library owns device memory, one CUDA
+ *     stream per context; a context is not thread-safe;
+ *   - host arrays use the reference layout of Array.h:7-186: one contiguous
+ *     double array per field, [X_np][Y_m][Z_m] with k fastest, X_np = Nx+6,
+ *     Y_m = Ny+4, Z_m = Nz+4, conserved variables stored as Q/J; face arrays
+ *     keep the reference's shifted indexing (x-face i+1/2 of cell (i,j,k) at
+ *     [i][j-1][k-1], y-face at [i-1][j][k-1], z-face at [i-1][j-1][k]);
+ *   - the x direction is periodic: the reference's MPI slab halos
+ *     (main.cpp:167-200, Dual_time_stepping.cpp:942-976) become a copy of the
+ *     slab's own far planes, with the same one-iteration lag.
+ */
+#ifndef CGLI_FU_FLOW_H
+#define CGLI_FU_FLOW_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CGLI_OK 0
+#define CGLI_EINVAL (-1)      /* bad argument / unknown array name / size out of range */
+#define CGLI_ECUDA (-2)       /* CUDA runtime error */
+#define CGLI_ENOMEM (-3)      /* device allocation failed */
+#define CGLI_ESTATE (-4)      /* call order violated (e.g. no metrics yet) */
+#define CGLI_EDIVERGED (-5)   /* residual norm not finite */
+#define CGLI_ETIMEOUT (-6)    /* a device-side wait gave up (wavefront flag) */
+
+#define CGLI_FP64 0           /* everything in double precision */
+#define CGLI_MIXED 1          /* LU-SGS sweeps, split Jacobians, diagonal in float */
+
+/* Runtime replacement of the compile-time parameters of Resolution.h,
+ * prm.h and Viscous_terms.h, plus the run constants main.cpp:44-70 fixes. */
+typedef struct cgli_params {
+  int nx, ny, nz;          /* interior cells (X_out of one slab, Y_out, Z_out) */
+  double dxi, det, dzt;    /* deltaXI, deltaET, deltaZT (Resolution.h:19-21) */
+  double dt;               /* physical time step deltaT (main.cpp:58) */
+  double e;                /* preconditioning floor e (main.cpp:57) */
+  double mu, pr;           /* mu_L, Pr_L (Viscous_terms.h:4-5) */
+  double twall_lo, twall_hi; /* wall temperatures (Y_boundary_condition.cpp:139,166) */
+  double force;            /* uniform x body force (replaces Dual_time_stepping.cpp:831) */
+  int precision;           /* CGLI_FP64 or CGLI_MIXED */
+} cgli_params;
+
+typedef struct cgli_ctx cgli_ctx;
+
+/* ---- lifecycle (replaces Array.h allocation and main.cpp:19-141 set-up) */
+int cgli_create(const cgli_params *p, cgli_ctx **out);
+int cgli_destroy(cgli_ctx *ctx);
+const char *cgli_last_error(void);
+/* device bytes the context holds */
+long long cgli_device_bytes(const cgli_ctx *ctx);
+
+/* ---- array transfer by reference name ("U1_".."U5_", "U1".."U5", "U1q".."U5q",
+ * "J", "xidx".."ztdz", the same with "_u"/"_v"/"_w" and "J_u"/"J_v"/"J_w",
+ * "inFx1".."inFz5", "vF2".."vF5", "MR1".."MR5", "NR1".."NR5", "EpX"/"EpY"/"EpZ",
+ * "Y_point").  Each transfers X_np*Y_m*Z_m doubles. */
+int cgli_set_array(cgli_ctx *ctx, const char *name, const double *host);
+int cgli_get_array(cgli_ctx *ctx, const char *name, double *host);
+
+/* Analytic channel metrics of Jacobian.cpp:61-243, Jacobian_u.cpp:59-101,
+ * Jacobian_v.cpp:79-151, Jacobian_w.cpp:61-106 (tanh wall clustering with
+ * parameter `stretch`, channel height `high`), generated on the host and
+ * uploaded; bit-identical to the reference's arrays, ghost-row copy typos
+ * included. */
+int cgli_channel_metrics(cgli_ctx *ctx, double high, double stretch);
+/* The same generator on the host only (no device, no context): writes the
+ * one metric array `name` ("J", "xidx".."ztdz", "J_u", "etdy_v", ...) of an
+ * Nx x Ny x Nz slab into `out` (X_np*Y_m*Z_m doubles). */
+int cgli_channel_metrics_host(int nx, int ny, int nz, double det, double high, double stretch,
+                              const char *name, double *out);
+
+/* Sets Q^(n+1,m) (U_), Q^n (U) and Q^(n-1) (Uq), 5 arrays each, in the
+ * reference layout (Initial_condition.cpp:111-236 and main.cpp:127-141). */
+int cgli_set_state(cgli_ctx *ctx, const double *const U_[5], const double *const U[5],
+                   const double *const Uq[5]);
+/* Reads back Q^(n+1,m) (5 arrays). */
+int cgli_get_state(cgli_ctx *ctx, double *const U_[5]);
+
+/* ---- the reference routines, one entry point each, acting on the device state */
+/* main.cpp:167-200: periodic 3-plane halo of U_ in x */
+int cgli_halo_x(cgli_ctx *ctx);
+/* Y_boundary_condition.cpp:19-186 (replaces Y_boundary_condition()) */
+int cgli_y_boundary_condition(cgli_ctx *ctx);
+/* Z_boundary_condition.cpp:15-69 (replaces Z_boundary_condition()) */
+int cgli_z_boundary_condition(cgli_ctx *ctx);
+/* Flux_X.cpp:12-359, Flux_Y.cpp:15-415, Flux_Z.cpp:15-360: fill inFx/inFy/inFz */
+int cgli_flux_x(cgli_ctx *ctx);
+int cgli_flux_y(cgli_ctx *ctx);
+int cgli_flux_z(cgli_ctx *ctx);
+/* Viscous_terms.cpp:15-907: fill vF2..vF5 */
+int cgli_viscous_terms(cgli_ctx *ctx);
+/* Dual_time_stepping.cpp:18-1795: residual, 2 x (forward + backward)
+ * hyperplane sweeps, update of U_, five norms er[v] = sqrt(sum)/(Nx Ny Nz)
+ * (the reference divides by its global X_out). Reads the inF and vF arrays
+ * filled by the three flux entry points and cgli_viscous_terms. */
+int cgli_dual_time_stepping(cgli_ctx *ctx, double er[5]);
+
+/* One complete inner iteration (main.cpp:167-264) through the fused fast
+ * path: halo + boundaries, one residual kernel (fluxes, viscous terms,
+ * dual-time residual), the wavefront sweeps and the update. */
+int cgli_inner_iteration(cgli_ctx *ctx, double er[5]);
+
+/* Driven_force.cpp:14-74: bulk mass flux (volume-weighted mean of rho*u) */
+int cgli_driven_force(cgli_ctx *ctx, double *bulk_flux);
+/* main.cpp:364-386: Q^(n-1) <- Q^n, Q^n <- Q^(n+1) */
+int cgli_end_step(cgli_ctx *ctx);
+/* uniform driving force used by the next residual assembly */
+int cgli_set_force(cgli_ctx *ctx, double force);
+
+/* One physical step (main.cpp:157-386): inner iterations until every one of
+ * the five norms has dropped by `drop` relative to the step's first
+ * iteration or `cap` iterations ran (fixed_iters > 0 runs exactly that many),
+ * then the time-level shift.  Returns the iteration count and final norms. */
+int cgli_step(cgli_ctx *ctx, int fixed_iters, double drop, int cap, int *iters, double er[5]);
+
+/* Hyperplane.cpp:18-80: cells of the interior slab listed by plane
+ * m = i+j+k (m = 7 .. Nx+Ny+Nz+4), then i, j, k; Nijk[2*m] = running end
+ * index, Nijk[2*m+1] = count; ijk[3*n..3*n+2] for n = 1..Nx*Ny*Nz.  Host
+ * only, O(N) (the reference's brute force is O(N * planes)).  nijk_len and
+ * ijk_len are the element counts of the buffers. */
+int cgli_hyperplane(int nx, int ny, int nz, int *Nijk, long nijk_len, int *ijk, long ijk_len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,103 @@
+"""Generates the golden fixtures of tests/golden/ from the reference itself.
+
+Runs the reference's own hot-path routines, compiled here by
+oracle/build_ref.py from the reference sources, on the seeded channel
+workload of cgli_fu_flow_b200.channel, and records for every stage of the
+first inner iteration and for three physical steps:
+  * the SHA-256 of the exact float64 bytes of each array (interior region),
+  * the five update norms and the driving-force sequence,
+  * the full final state Q^(n+1) of the interior cells (npz).
+The oracle must reproduce every hash bit for bit; the GPU path is compared
+with the stored state within tolerance.
+
+Usage:  python tests/golden/make_golden.py [nx ny nz]
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, REPO)
+
+from cgli_fu_flow_b200.channel import Channel  # noqa: E402
+from oracle.refrun import RefSolver  # noqa: E402
+
+STEPS = 3
+ITERS = 10
+
+
+def regions(ch):
+    nx, ny, nz = ch.nx, ch.ny, ch.nz
+    return {
+        "cell": np.s_[3:nx + 3, 2:ny + 2, 2:nz + 2],
+        "bc": np.s_[0:nx + 6, 1:ny + 3, 1:nz + 3],
+        "fx": np.s_[2:nx + 3, 1:ny + 1, 1:nz + 1],
+        "fy": np.s_[2:nx + 2, 1:ny + 2, 1:nz + 1],
+        "fz": np.s_[2:nx + 2, 1:ny + 1, 1:nz + 2],
+        "metric": np.s_[0:nx + 6, 1:ny + 3, 1:nz + 3],
+    }
+
+
+def digest(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a, dtype=np.float64).tobytes()).hexdigest()
+
+
+STAGES = {
+    "bc": [f"U{v}_" for v in range(1, 6)],
+    "fx": [f"inFx{v}" for v in range(1, 6)],
+    "fy": [f"inFy{v}" for v in range(1, 6)],
+    "fz": [f"inFz{v}" for v in range(1, 6)],
+    "visc": [f"vF{v}" for v in range(2, 6)],
+    "dts": [f"MR{v}" for v in range(1, 6)] + [f"NR{v}" for v in range(1, 6)] + [f"U{v}_" for v in range(1, 6)],
+}
+STAGE_REGION = {"bc": "bc", "fx": "fx", "fy": "fy", "fz": "fz", "visc": "cell", "dts": "cell"}
+METRICS = ["J", "xidx", "etdy", "ztdy", "ztdz", "J_u", "etdy_u", "J_v", "etdy_v", "J_w", "etdy_w", "ztdz_w"]
+
+
+def main(nx=8, ny=12, nz=8):
+    ch = Channel(nx, ny, nz)
+    reg = regions(ch)
+    r = RefSolver(ch, threads=1)
+    r.init()
+    out = {"workload": ch.name, "cells": [nx, ny, nz], "steps": STEPS, "iters_per_step": ITERS,
+           "hyperplane_mismatches": int(r.lib.ref_check_hyperplanes()),
+           "metrics": {m: digest(r.array(m)[reg["metric"]]) for m in METRICS}, "stages": {}}
+    r.lib.ref_halo_bc()
+    out["stages"]["bc"] = {n: digest(r.array(n)[reg["bc"]]) for n in STAGES["bc"]}
+    for st, fn in (("fx", "ref_flux_x"), ("fy", "ref_flux_y"), ("fz", "ref_flux_z"), ("visc", "ref_viscous")):
+        getattr(r.lib, fn)()
+        out["stages"][st] = {n: digest(r.array(n)[reg[STAGE_REGION[st]]]) for n in STAGES[st]}
+    import ctypes
+    er = (ctypes.c_double * 5)()
+    r.lib.ref_dts(er)
+    out["stages"]["dts"] = {n: digest(r.array(n)[reg["cell"]]) for n in STAGES["dts"]}
+    # the reference divides the norms by its global X_out = 3 Nx
+    out["first_norms"] = [3.0 * x for x in er[:]]
+    # restart and run whole steps
+    r2 = RefSolver(ch, threads=1, build=False)
+    r2.init()
+    forces, norms = [r2.force], []
+    for _ in range(STEPS):
+        _, e = r2.step(ITERS)
+        norms.append([3.0 * x for x in e])
+        forces.append(r2.force)
+    out["step_norms"] = norms
+    out["forces"] = forces
+    q = r2.q()[(slice(None),) + reg["cell"]]
+    out["final_state"] = digest(q)
+    base = os.path.join(HERE, ch.name)
+    np.savez_compressed(base + ".npz", q=q)
+    with open(base + ".json", "w") as fh:
+        json.dump(out, fh, indent=1)
+    print("wrote", base + ".json", base + ".npz")
+
+
+if __name__ == "__main__":
+    args = [int(a) for a in sys.argv[1:4]] or [8, 12, 8]
+    main(*args)
