@@ -15,6 +15,8 @@
 
 #include "host_setup.h"
 
+#include <algorithm>
+
 namespace {
 
 thread_local std::string g_err;
@@ -46,6 +48,9 @@ struct cgli_ctx {
   double *h_norms = nullptr;   // pinned, 8 doubles
   double *d_out = nullptr;     // device scratch for norms / bulk flux
   int update_blocks = 0;
+  int sweep_tiles = 0;
+  cgli::SweepArgs sw;
+  bool metrics_checked = false;
   cudaGraphExec_t iter_graph = nullptr;
   cudaGraphExec_t dts_graph = nullptr;
 };
@@ -123,14 +128,62 @@ int last_launch(const char *what) {
   return CGLI_OK;
 }
 
-int read_norms(cgli_ctx *c, double er[5]) {
+int read_norms(cgli_ctx *c, double er[5], int nblocks) {
   double scale = 1.0 / ((double)c->p.nx * c->p.ny * c->p.nz);
-  cgli::launch_norms(c->d, c->stream, c->update_blocks, scale, c->d_out);
+  cgli::launch_norms(c->d, c->stream, nblocks, scale, c->d_out);
   CUDA_TRY(cudaMemcpyAsync(c->h_norms, c->d_out, 5 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(cudaStreamSynchronize(c->stream));
+  int status = 0;
+  CUDA_TRY(cudaMemcpy(&status, c->d.status, sizeof(int), cudaMemcpyDeviceToHost));
+  if (status) {
+    int zero = 0;
+    cudaMemcpy(c->d.status, &zero, sizeof(int), cudaMemcpyHostToDevice);
+    return fail(CGLI_ETIMEOUT, "a wavefront tile gave up waiting for its neighbour (bounded spin)");
+  }
   for (int v = 0; v < 5; v++) er[v] = c->h_norms[v];
   for (int v = 0; v < 5; v++)
     if (!std::isfinite(er[v])) return fail(CGLI_EDIVERGED, "update norm is not finite");
+  return CGLI_OK;
+}
+
+void drop_graph(cgli_ctx *c) {
+  if (c->iter_graph) { cudaGraphExecDestroy(c->iter_graph); c->iter_graph = nullptr; }
+}
+
+// Decides whether the cell metrics are those of a grid uniform in x and z
+// (xidx = ztdz = 1, the other off-diagonal terms 0, J and etdy functions of
+// j alone) over every cell the sweeps read: planes 2..ie+1, rows 2..jn,
+// k = 2..kn.  If so the sweeps read J(j), etdy(j) from two small tables
+// instead of ten 3-D arrays.
+int check_channel_metrics(cgli_ctx *c) {
+  const cgli::Dev &d = c->d;
+  size_t n = (size_t)d.X * d.Y * d.Z;
+  std::vector<double> J(n), m[9];
+  CUDA_TRY(cudaMemcpy(J.data(), d.J, n * 8, cudaMemcpyDeviceToHost));
+  for (int v = 0; v < 9; v++) {
+    m[v].resize(n);
+    CUDA_TRY(cudaMemcpy(m[v].data(), d.m[v], n * 8, cudaMemcpyDeviceToHost));
+  }
+  const int ie = d.nx + 2, jn = d.ny + 1, kn = d.nz + 1;
+  std::vector<double> jt(d.Y, 0.0), et(d.Y, 0.0);
+  bool ok = true;
+  for (int j = 2; j <= jn && ok; j++) {
+    size_t r = cgli::ix(d, 3, j, 2);
+    jt[j] = J[r]; et[j] = m[4][r];
+    for (int i = 2; i <= ie + 1 && ok; i++)
+      for (int k = 2; k <= kn && ok; k++) {
+        size_t q = cgli::ix(d, i, j, k);
+        ok = J[q] == jt[j] && m[4][q] == et[j] && m[0][q] == 1.0 && m[8][q] == 1.0 && m[1][q] == 0.0 &&
+             m[2][q] == 0.0 && m[3][q] == 0.0 && m[5][q] == 0.0 && m[6][q] == 0.0 && m[7][q] == 0.0;
+      }
+  }
+  if (ok) {
+    CUDA_TRY(cudaMemcpy((void *)c->sw.Jtab, jt.data(), sizeof(double) * d.Y, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy((void *)c->sw.etdytab, et.data(), sizeof(double) * d.Y, cudaMemcpyHostToDevice));
+  }
+  c->sw.channel_metrics = ok ? 1 : 0;
+  c->metrics_checked = true;
+  drop_graph(c);
   return CGLI_OK;
 }
 
@@ -183,7 +236,37 @@ int cgli_create(const cgli_params *p, cgli_ctx **out) {
   if (rc == CGLI_OK) rc = alloc(c, 16 * sizeof(double), (void **)&c->d_out);
   if (rc == CGLI_OK) rc = alloc(c, 16 * sizeof(int), (void **)&d.status);
   c->update_blocks = p->nx * p->ny;
-  if (rc == CGLI_OK) rc = alloc(c, 5 * sizeof(double) * (size_t)c->update_blocks, (void **)&d.partial);
+  const int nti = (p->nx + cgli::SWEEP_TI - 1) / cgli::SWEEP_TI, ntj = (p->ny + cgli::SWEEP_TJ - 1) / cgli::SWEEP_TJ;
+  c->sweep_tiles = nti * ntj;
+  size_t nblk = (size_t)std::max(c->update_blocks, c->sweep_tiles);
+  if (rc == CGLI_OK) rc = alloc(c, 5 * sizeof(double) * nblk, (void **)&d.partial);
+  {
+    cgli::SweepArgs &a = c->sw;
+    memset(&a, 0, sizeof a);
+    size_t plane = (size_t)d.Y * d.Z * sizeof(double);
+    for (int v = 0; v < 5; v++) {
+      a.dq[v] = d.NL[v];
+      if (rc == CGLI_OK) rc = alloc(c, plane, (void **)&a.halo_f[v]);
+      if (rc == CGLI_OK) rc = alloc(c, plane, (void **)&a.halo_b[v]);
+    }
+    size_t xb = (size_t)c->sweep_tiles * cgli::SWEEP_TJ * p->nz * 5 * sizeof(double);
+    size_t yb = (size_t)c->sweep_tiles * cgli::SWEEP_TI * p->nz * 5 * sizeof(double);
+    if (rc == CGLI_OK) rc = alloc(c, xb, (void **)&a.xbuf);
+    if (rc == CGLI_OK) rc = alloc(c, yb, (void **)&a.ybuf);
+    if (rc == CGLI_OK) rc = alloc(c, sizeof(unsigned long long) * c->sweep_tiles, (void **)&a.prog);
+    if (rc == CGLI_OK) rc = alloc(c, 64, (void **)&a.ticket);
+    std::vector<int> order;
+    cgli::sweep_tile_order(nti, ntj, order);
+    int *dorder = nullptr;
+    if (rc == CGLI_OK) rc = alloc(c, sizeof(int) * order.size(), (void **)&dorder);
+    if (rc == CGLI_OK) cudaMemcpy(dorder, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice);
+    a.order = dorder;
+    double *jt = nullptr, *et = nullptr;
+    if (rc == CGLI_OK) rc = alloc(c, sizeof(double) * d.Y, (void **)&jt);
+    if (rc == CGLI_OK) rc = alloc(c, sizeof(double) * d.Y, (void **)&et);
+    a.Jtab = jt; a.etdytab = et;
+    a.spin_limit = 1 << 24;
+  }
   if (rc == CGLI_OK && cudaMallocHost(&c->h_norms, 16 * sizeof(double)) != cudaSuccess)
     rc = fail(CGLI_ENOMEM, "cudaMallocHost");
   if (rc == CGLI_OK && cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
@@ -222,7 +305,7 @@ int cgli_set_array(cgli_ctx *c, const char *name, const double *host) {
   size_t n = (size_t)c->d.X * c->d.Y * c->d.Z;
   CUDA_TRY(cudaMemcpyAsync(dst, host, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   CUDA_TRY(cudaStreamSynchronize(c->stream));
-  if (is_metric) c->have_metrics = true;
+  if (is_metric) { c->have_metrics = true; c->metrics_checked = false; c->sw.channel_metrics = 0; drop_graph(c); }
   return CGLI_OK;
 }
 
@@ -252,6 +335,8 @@ int cgli_channel_metrics(cgli_ctx *c, double high, double stretch) {
   }
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   c->have_metrics = true;
+  c->metrics_checked = false;
+  drop_graph(c);
   return CGLI_OK;
 }
 
@@ -306,17 +391,20 @@ int cgli_dual_time_stepping(cgli_ctx *c, double er[5]) {
   if (!er) return fail(CGLI_EINVAL, "null er");
   cgli::launch_dts(c->d, c->stream, c->update_blocks);
   rc = last_launch("dual_time_stepping"); if (rc) return rc;
-  return read_norms(c, er);
+  return read_norms(c, er, c->update_blocks);
 }
 
 int cgli_inner_iteration(cgli_ctx *c, double er[5]) {
   int rc = check(c); if (rc) return rc;
   rc = need_ready(c); if (rc) return rc;
   if (!er) return fail(CGLI_EINVAL, "null er");
+  if (!c->metrics_checked) {
+    rc = check_channel_metrics(c); if (rc) return rc;
+  }
   if (!c->iter_graph) {
     cudaGraph_t g;
     CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    cgli::launch_fused_iteration(c->d, c->stream, c->p.precision, c->update_blocks);
+    cgli::launch_fused_iteration(c->d, c->sw, c->stream, c->p.precision);
     cudaError_t e = cudaStreamEndCapture(c->stream, &g);
     if (e != cudaSuccess) return fail(CGLI_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
     e = cudaGraphInstantiate(&c->iter_graph, g, 0);
@@ -324,7 +412,7 @@ int cgli_inner_iteration(cgli_ctx *c, double er[5]) {
     if (e != cudaSuccess) return fail(CGLI_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
   }
   CUDA_TRY(cudaGraphLaunch(c->iter_graph, c->stream));
-  return read_norms(c, er);
+  return read_norms(c, er, c->sweep_tiles);
 }
 
 int cgli_driven_force(cgli_ctx *c, double *bulk_flux) {

@@ -1,17 +1,84 @@
-// Fast path of one inner iteration.
+// Fast path of one inner iteration: halo and boundaries, fluxes, viscous
+// terms, residual assembly, four wavefront sweep passes with the update
+// fused into the last one.
 #include "cgli_dev.cuh"
 #include "cgli_launch.h"
 
 namespace cgli {
 
-void launch_fused_iteration(const Dev &d, cudaStream_t s, int precision, int update_blocks) {
+// Dual_time_stepping.cpp:737-922 for the fast path: MR of every interior
+// cell, and D^-1 MR on planes ie and 3 as the lagged halos of the first sweep
+// (the reference initialises NL = NR = D^-1 MR, :897-908, and the sweep
+// exchanges planes ie and 3 before its first pass, :942-976)
+__global__ void k_residual_fast(Dev d, SweepArgs a) {
+  int k = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  int j = 2 + blockIdx.y;
+  int i = 3 + blockIdx.z;
+  if (k > d.nz + 1) return;
+  long long c = ix(d, i, j, k);
+  const double J = d.J[c], deltaT = d.dt;
+  CPrim<double> q = cprim<double>(d.U_[0][c], d.U_[1][c], d.U_[2][c], d.U_[3][c], d.U_[4][c], J, d.e);
+  double rho = q.rho, u = q.u, v = q.v, w = q.w, VV = q.VV, T = q.Tt, H = q.H, beta = q.beta;
+  double temp = rho * KG;
+  double d11 = -(H * (KG - 1) + VV - KG * (T + VV)) * beta;
+  double d12 = -(KG - 1) * u * beta, d13 = -(KG - 1) * v * beta, d14 = -(KG - 1) * w * beta;
+  double d15 = (KG - 1) * beta;
+  double d21 = -u / rho, d22 = 1 / rho;
+  double d31 = -v / rho;
+  double d41 = -w / rho;
+  double d51 = (KG - 1) * (VV + KG * T * beta + (KG - 1) * VV * beta + H * (-1 + beta - KG * beta)) / temp;
+  double d52 = -(KG - 1) * u * (1 + (KG - 1) * beta) / temp;
+  double d53 = -(KG - 1) * v * (1 + (KG - 1) * beta) / temp;
+  double d54 = -(KG - 1) * w * (1 + (KG - 1) * beta) / temp;
+  double d55 = (KG - 1) * (1 + (KG - 1) * beta) / temp;
+  long long fx1 = ix(d, i, j - 1, k - 1), fx0 = ix(d, i - 1, j - 1, k - 1);
+  long long fy1 = ix(d, i - 1, j, k - 1), fz1 = ix(d, i - 1, j - 1, k);
+  double Rk[5];
+  double f = d.scal[0];
+  for (int n = 0; n < 5; n++) {
+    double Rp = -(3 * d.U_[n][c] - 4 * d.U[n][c] + d.Uq[n][c]) / (2 * deltaT);
+    double Rf = -((d.inF[0][n][fx1] - d.inF[0][n][fx0]) / d.dxi + (d.inF[1][n][fy1] - d.inF[1][n][fx0]) / d.det +
+                  (d.inF[2][n][fz1] - d.inF[2][n][fx0]) / d.dzt);
+    Rk[n] = Rp + Rf;
+  }
+  Rk[1] = Rk[1] + d.vF[0][c] + f / J;
+  Rk[2] = Rk[2] + d.vF[1][c];
+  Rk[3] = Rk[3] + d.vF[2][c];
+  Rk[4] = Rk[4] + d.vF[3][c] + f * u / J;
+  double MR[5];
+  MR[0] = (d11 * Rk[0] + d12 * Rk[1] + d13 * Rk[2] + d14 * Rk[3] + d15 * Rk[4]);
+  MR[1] = (d21 * Rk[0] + d22 * Rk[1]);
+  MR[2] = (d31 * Rk[0] + d22 * Rk[2]);
+  MR[3] = (d41 * Rk[0] + d22 * Rk[3]);
+  MR[4] = (d51 * Rk[0] + d52 * Rk[1] + d53 * Rk[2] + d54 * Rk[3] + d55 * Rk[4]);
+  for (int n = 0; n < 5; n++) d.MR[n][c] = MR[n];
+  const int ie = d.nx + 2;
+  if (i == ie || i == 3) {
+    double mm[9];
+    for (int v2 = 0; v2 < 9; v2++) mm[v2] = d.m[v2][c];
+    Diag<double> dd = diag<double>(q, mm, d.dxi, d.det, d.dzt, deltaT);
+    double n5[5] = {dd.d11 * MR[0], dd.d22 * MR[1], dd.d22 * MR[2], dd.d22 * MR[3], dd.d51 * MR[0] + dd.d22 * MR[4]};
+    long long h = (long long)j * d.dj + k;
+    for (int n = 0; n < 5; n++) {
+      if (i == ie) a.halo_f[n][h] = n5[n];
+      if (i == 3) a.halo_b[n][h] = n5[n];
+    }
+  }
+}
+
+void launch_residual_fast(const Dev &d, const SweepArgs &a, cudaStream_t s) {
+  k_residual_fast<<<dim3((d.nz + 63) / 64, d.ny, d.nx), 64, 0, s>>>(d, a);
+}
+
+void launch_fused_iteration(const Dev &d, const SweepArgs &a, cudaStream_t s, int precision) {
   (void)precision;
   launch_halo_bc(d, s);
   launch_flux_x(d, s);
   launch_flux_y(d, s);
   launch_flux_z(d, s);
   launch_viscous(d, s);
-  launch_dts(d, s, update_blocks);
+  launch_residual_fast(d, a, s);
+  launch_sweeps(d, a, s);
 }
 
 }  // namespace cgli
