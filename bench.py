@@ -1,0 +1,337 @@
+"""Benchmark of the per-step hot path: Mcell-steps/s on the seeded channel.
+
+A step is one physical time step of the dual-time scheme on the
+256 x 192 x 192 channel (the plain-FP64-at-scale workload): inner LU-SGS
+iterations until every one of the five update norms has dropped by 1e-3
+relative to the step's first iteration (capped at 30), then the time-level
+shift and the driving-force update.  All state stays resident on the GPU for
+`value`; `e2e` repeats the measurement through the C ABI with the step's
+inputs copied from pinned host memory and its result copied back every step.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+With N > 1 (torchrun) every rank runs an independent replica of the workload
+(the solver does not shard: one x-slab per GPU with no exchange is the
+reference's own decomposition collapsed to one slab), `value` sums the ranks'
+cell-steps over the slowest rank's time.  `--impl reference` times the
+reference's own CPU build (compiled here from its sources into oracle/_ref)
+on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+import numpy as np  # noqa: E402
+
+from cgli_fu_flow_b200 import channel as C  # noqa: E402
+
+METRIC = "Mcell-steps/s at fixed inner-residual drop (1e-3, cap 30)"
+ITERS_FILE = os.path.join(HERE, "cgli_fu_flow_b200", "workload_iters.json")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="c2", choices=sorted(C.WORKLOADS))
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--drop", type=float, default=1e-3)
+    ap.add_argument("--cap", type=int, default=30)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-iters", type=int, default=2, help="reference inner iterations in the CPU sample")
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------- plumbing
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.dist = None
+        if self.world > 1:
+            import datetime
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            self.dist = dist
+            self.torch = torch
+
+    def barrier(self):
+        if self.dist:
+            self.dist.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.dist:
+            return x
+        t = self.torch.tensor([x], dtype=self.torch.float64, device="cuda")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x: float) -> float:
+        if not self.dist:
+            return x
+        t = self.torch.tensor([x], dtype=self.torch.float64, device="cuda")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.dist:
+            self.dist.destroy_process_group()
+
+
+class Clocks:
+    """Samples nvidia-smi every 200 ms while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------ GPU arm
+def run_gpu(a, dist: Dist) -> dict | None:
+    from cgli_fu_flow_b200.solver import Solver, FP64, MIXED
+    ch = C.Channel(*C.WORKLOADS[a.workload])
+    prec = FP64 if a.precision == "fp64" else MIXED
+    sol = Solver(ch, prec)
+    q0 = ch.initial_conserved()
+    sol.init(q0)
+    iters = []
+    for _ in range(a.warmup):
+        sol.step(None, a.drop, a.cap)
+    clocks = Clocks(dist.local)
+    dist.barrier()
+    sol.event(0)
+    clocks.start()
+    for _ in range(a.steps):
+        it, _ = sol.step(None, a.drop, a.cap)
+        iters.append(it)
+    sol.event(1)
+    ms = sol.elapsed_ms(0, 1)
+    ck = clocks.stop()
+    dist.barrier()
+    ms_max = dist.max(ms)
+    cells_steps = dist.sum(float(ch.cells) * a.steps)
+    value = cells_steps / (ms_max / 1e3) / 1e6
+    mean_iters = float(np.mean(iters))
+
+    # per-stage device times of one inner iteration (the roofline kernels)
+    stages = sol.profile_stages(reps=2)
+
+    # end to end through the C ABI with host buffers
+    e2e = None
+    if not a.no_e2e:
+        e2e = run_e2e(a, ch, prec, dist)
+    sol.close()
+    if dist.rank != 0:
+        return None
+    from cgli_fu_flow_b200 import roofline
+    roof = roofline.sweep_roofline(ch, stages, a.precision)
+    out = {
+        "metric": METRIC,
+        "value": round(value, 3),
+        "unit": "Mcell-steps/s",
+        "n_gpus": dist.world,
+        "steps": a.steps,
+        "warmup": a.warmup,
+        "ms_per_step": round(ms_max / a.steps, 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64" if a.precision == "fp64" else "f64 residual / f32 sweeps",
+        "data": "synthetic: seeded Poiseuille + 10% uniform perturbation channel (no dataset involved)",
+        "config": {"workload": f"channel {ch.nx}x{ch.ny}x{ch.nz} cells, Mach 0.2, Re_b 5600",
+                   "cells": ch.cells, "precision": a.precision,
+                   "inner": f"until 1e-3 drop of all five update norms, cap {a.cap}",
+                   "mean_inner_iterations": round(mean_iters, 2), "inner_iterations": iters,
+                   "parallelism": "replicas" if dist.world > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (state and records ~0.8 GB per field group)"},
+        "clocks": ck,
+        "stage_ms": {k: round(v, 4) for k, v in stages.items()},
+        "roofline": roof,
+        "gpu_launches": int(sum(15 * n + 2 for n in iters)),
+    }
+    if e2e:
+        out["e2e"] = e2e
+    return out
+
+
+def run_e2e(a, ch, prec, dist: Dist) -> dict:
+    """The same steps through the C ABI with pinned host buffers: every step
+    uploads U_, U, Uq (the step's inputs) and downloads U_ (its result)."""
+    import torch
+    from cgli_fu_flow_b200.solver import Solver, reference_state
+    sol = Solver(ch, prec)
+    J = sol.get("J")
+    U_, U, Uq = reference_state(ch, J, ch.initial_conserved(), ch.initial_conserved())
+    shape = (5,) + ch.shape
+    pin = {k: torch.empty(shape, dtype=torch.float64, pin_memory=True) for k in ("U_", "U", "Uq")}
+    hp = {k: v.numpy() for k, v in pin.items()}
+    hp["U_"][:] = U_
+    hp["U"][:] = U
+    hp["Uq"][:] = Uq
+    for _ in range(max(1, min(a.warmup, 2))):
+        sol.set_state(hp["U_"], hp["U"], hp["Uq"])
+        sol.step(None, a.drop, a.cap)
+    n = ch.shape[0] * ch.shape[1] * ch.shape[2] * 8
+    dist.barrier()
+    sol.event(2)
+    for _ in range(a.steps):
+        sol.set_state(hp["U_"], hp["U"], hp["Uq"])
+        sol.step(None, a.drop, a.cap)
+        out = sol.q()
+        # the host keeps the time levels: Q^(n-1) <- Q^n, Q^n <- Q^(n+1)
+        hp["Uq"][:] = hp["U"]
+        hp["U"][:] = out
+        hp["U_"][:] = out
+    sol.event(3)
+    ms = dist.max(sol.elapsed_ms(2, 3))
+    sol.close()
+    value = dist.sum(float(ch.cells) * a.steps) / (ms / 1e3) / 1e6
+    return {"value": round(value, 3), "unit": "Mcell-steps/s", "h2d_bytes_per_step": 15 * n,
+            "d2h_bytes_per_step": 5 * n}
+
+
+# ------------------------------------------------------------ CPU reference
+def mean_iters_for(workload: str, precision: str = "fp64", default: int = 30) -> float:
+    try:
+        with open(ITERS_FILE) as fh:
+            return float(json.load(fh)[f"{workload}/{precision}"])
+    except Exception:
+        return float(default)
+
+
+def cpu_reference_sample(ch, iters: int, warm: int = 1) -> dict:
+    """Times the reference's own compiled routines (oracle/_ref) on `iters`
+    inner iterations of the workload with every host core (OpenMP)."""
+    from oracle.refrun import RefSolver
+    cores = os.cpu_count() or 1
+    r = RefSolver(ch, threads=cores, build=False)
+    r.init()
+    for _ in range(warm):
+        r.inner_iteration()
+    t = time.perf_counter()
+    for _ in range(iters):
+        r.inner_iteration()
+    dt = (time.perf_counter() - t) / iters
+    return {"sec_per_inner_iteration": dt, "cores": cores}
+
+
+def run_reference(a, dist: Dist) -> dict | None:
+    if dist.rank != 0:
+        return None
+    ch = C.Channel(*C.WORKLOADS[a.workload])
+    lib = os.path.join(HERE, "oracle", "_ref", ch.name, "libref.so")
+    if not os.path.exists(lib):
+        return {"impl": "reference", "unavailable": f"reference build {lib} missing (build() compiles it where the "
+                                                    "reference sources are present)"}
+    m_it = mean_iters_for(a.workload, "fp64")
+    from oracle.refrun import RefSolver
+    cores = os.cpu_count() or 1
+    r = RefSolver(ch, threads=cores, build=False)
+    r.init()
+    per_step = []
+    for s in range(a.warmup + a.steps):
+        t = time.perf_counter()
+        r.inner_iteration()
+        dt = time.perf_counter() - t
+        if s >= a.warmup:
+            per_step.append(dt)
+    sec_iter = float(np.mean(per_step))
+    value = ch.cells / (sec_iter * m_it) / 1e6
+    sample = (f"{a.steps} timed inner iterations (after {a.warmup}) of the reference's routines on the "
+              f"{ch.nx}x{ch.ny}x{ch.nz} channel; one physical step = {m_it:g} inner iterations, the count the "
+              f"FP64 GPU path needs for the 1e-3 drop on this workload")
+    return {"impl": "reference", "metric": METRIC, "value": round(value, 5), "unit": "Mcell-steps/s",
+            "n_gpus": dist.world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": round(sec_iter * m_it * 1e3, 1), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic seeded channel",
+            "config": {"workload": f"channel {ch.nx}x{ch.ny}x{ch.nz} cells, Mach 0.2, Re_b 5600",
+                       "cells": ch.cells, "inner_iterations_per_step": m_it},
+            "cpu_baseline": {"value": round(value, 5), "unit": "Mcell-steps/s", "cores": cores,
+                             "kind": "reference", "sample": sample},
+            "e2e": {"value": round(value, 5), "unit": "Mcell-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    a = parse()
+    dist = Dist()
+    try:
+        if a.impl == "reference":
+            out = run_reference(a, dist)
+        else:
+            out = run_gpu(a, dist)
+            if out is not None and not a.no_cpu_baseline and dist.world == 1:
+                ch = C.Channel(*C.WORKLOADS[a.workload])
+                lib = os.path.join(HERE, "oracle", "_ref", ch.name, "libref.so")
+                if os.path.exists(lib):
+                    smp = cpu_reference_sample(ch, a.cpu_iters)
+                    m_it = out["config"]["mean_inner_iterations"]
+                    v = ch.cells / (smp["sec_per_inner_iteration"] * m_it) / 1e6
+                    out["cpu_baseline"] = {
+                        "value": round(v, 5), "unit": "Mcell-steps/s", "cores": smp["cores"], "kind": "reference",
+                        "sample": f"{a.cpu_iters} inner iterations of the reference's compiled routines on the same "
+                                  f"workload ({smp['sec_per_inner_iteration']:.2f} s each, OpenMP on "
+                                  f"{smp['cores']} threads), scaled by the GPU run's {m_it:g} iterations per step"}
+                else:
+                    out["cpu_baseline"] = {"value": None, "unit": "Mcell-steps/s", "cores": 0, "kind": "reference",
+                                           "sample": "reference build missing"}
+        if out is not None:
+            print(json.dumps(out), flush=True)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -159,10 +159,13 @@ class Channel:
         of `ranks` equal x-slabs: 10 fields [U1..U5 at n, U1..U5 at n-1],
         each of ranks*Nx x Ny x Nz doubles, this slab at x-offset Nx."""
         nx, ny, nz = self.nx, self.ny, self.nz
-        out = np.zeros((10, ranks * nx, ny, nz))
-        out[0:5, nx:2 * nx] = q_n
-        out[5:10, nx:2 * nx] = q_nm1
-        out.tofile(path)
+        field = ranks * nx * ny * nz * 8
+        with open(path, "wb") as fh:
+            fh.truncate(10 * field)          # sparse: only this slab's third is written
+            for f in range(10):
+                q = q_n if f < 5 else q_nm1
+                fh.seek(f * field + nx * ny * nz * 8)
+                fh.write(np.ascontiguousarray(q[f % 5], dtype=np.float64).tobytes())
 
 
 def force_update(state: dict, bulk_flux: float, ch: Channel, kp: float = 0.5, ki: float = 0.05) -> float:

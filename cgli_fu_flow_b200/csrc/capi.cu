@@ -53,6 +53,7 @@ struct cgli_ctx {
   bool metrics_checked = false;
   cudaGraphExec_t iter_graph = nullptr;
   cudaGraphExec_t dts_graph = nullptr;
+  cudaEvent_t events[8] = {};
 };
 
 namespace {
@@ -243,17 +244,38 @@ int cgli_create(const cgli_params *p, cgli_ctx **out) {
   {
     cgli::SweepArgs &a = c->sw;
     memset(&a, 0, sizeof a);
-    size_t plane = (size_t)d.Y * d.Z * sizeof(double);
+    const bool mixed = p->precision == CGLI_MIXED;
+    const size_t es = mixed ? sizeof(float) : sizeof(double);
+    const size_t nsk = (size_t)cgli::skew_size(d);
+    const size_t plane = (size_t)d.Y * d.Z;
     for (int v = 0; v < 5; v++) {
-      a.dq[v] = d.NL[v];
-      if (rc == CGLI_OK) rc = alloc(c, plane, (void **)&a.halo_f[v]);
-      if (rc == CGLI_OK) rc = alloc(c, plane, (void **)&a.halo_b[v]);
+      if (mixed) {
+        if (rc == CGLI_OK) rc = alloc(c, nsk * es, (void **)&a.dqf[v]);
+        if (rc == CGLI_OK) rc = alloc(c, nsk * es, (void **)&a.mrf[v]);
+        if (rc == CGLI_OK) rc = alloc(c, plane * es, (void **)&a.halo_ff[v]);
+        if (rc == CGLI_OK) rc = alloc(c, plane * es, (void **)&a.halo_bf[v]);
+      } else {
+        if (rc == CGLI_OK) rc = alloc(c, nsk * es, (void **)&a.dq[v]);
+        if (rc == CGLI_OK) rc = alloc(c, nsk * es, (void **)&a.mrs[v]);
+        if (rc == CGLI_OK) rc = alloc(c, plane * es, (void **)&a.halo_f[v]);
+        if (rc == CGLI_OK) rc = alloc(c, plane * es, (void **)&a.halo_b[v]);
+      }
     }
-    size_t xb = (size_t)c->sweep_tiles * cgli::SWEEP_TJ * p->nz * 5 * sizeof(double);
-    size_t yb = (size_t)c->sweep_tiles * cgli::SWEEP_TI * p->nz * 5 * sizeof(double);
-    if (rc == CGLI_OK) rc = alloc(c, xb, (void **)&a.xbuf);
-    if (rc == CGLI_OK) rc = alloc(c, yb, (void **)&a.ybuf);
-    if (rc == CGLI_OK) rc = alloc(c, sizeof(unsigned long long) * c->sweep_tiles, (void **)&a.prog);
+    for (int v = 0; v < cgli::REC_N; v++) {
+      if (mixed) {
+        if (rc == CGLI_OK) rc = alloc(c, nsk * es, (void **)&a.recf[v]);
+        if (rc == CGLI_OK) rc = alloc(c, plane * es, (void **)&a.hrecf_f[v]);
+        if (rc == CGLI_OK) rc = alloc(c, plane * es, (void **)&a.hrecf_b[v]);
+      } else {
+        if (rc == CGLI_OK) rc = alloc(c, nsk * es, (void **)&a.rec[v]);
+        if (rc == CGLI_OK) rc = alloc(c, plane * es, (void **)&a.hrec_f[v]);
+        if (rc == CGLI_OK) rc = alloc(c, plane * es, (void **)&a.hrec_b[v]);
+      }
+    }
+    size_t xb = (size_t)c->sweep_tiles * cgli::SWEEP_TJ * p->nz * 5 * es;
+    size_t yb = (size_t)c->sweep_tiles * cgli::SWEEP_TI * p->nz * 5 * es;
+    if (rc == CGLI_OK) rc = alloc(c, xb, mixed ? (void **)&a.xbuff : (void **)&a.xbuf);
+    if (rc == CGLI_OK) rc = alloc(c, yb, mixed ? (void **)&a.ybuff : (void **)&a.ybuf);
     if (rc == CGLI_OK) rc = alloc(c, 64, (void **)&a.ticket);
     std::vector<int> order;
     cgli::sweep_tile_order(nti, ntj, order);
@@ -265,12 +287,20 @@ int cgli_create(const cgli_params *p, cgli_ctx **out) {
     if (rc == CGLI_OK) rc = alloc(c, sizeof(double) * d.Y, (void **)&jt);
     if (rc == CGLI_OK) rc = alloc(c, sizeof(double) * d.Y, (void **)&et);
     a.Jtab = jt; a.etdytab = et;
-    a.spin_limit = 1 << 24;
+    a.spin_limit = 1 << 22;
   }
   if (rc == CGLI_OK && cudaMallocHost(&c->h_norms, 16 * sizeof(double)) != cudaSuccess)
     rc = fail(CGLI_ENOMEM, "cudaMallocHost");
   if (rc == CGLI_OK && cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
     rc = fail(CGLI_ECUDA, "cudaStreamCreate");
+  if (rc != CGLI_OK) {
+    std::string keep = g_err;
+    cgli_destroy(c);
+    g_err = keep;
+    return rc;
+  }
+  for (auto &e : c->events)
+    if (rc == CGLI_OK && cudaEventCreate(&e) != cudaSuccess) rc = fail(CGLI_ECUDA, "cudaEventCreate");
   if (rc != CGLI_OK) {
     std::string keep = g_err;
     cgli_destroy(c);
@@ -289,6 +319,8 @@ int cgli_destroy(cgli_ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->iter_graph) cudaGraphExecDestroy(c->iter_graph);
   if (c->dts_graph) cudaGraphExecDestroy(c->dts_graph);
+  for (auto &e : c->events)
+    if (e) cudaEventDestroy(e);
   for (void *p : c->allocs) cudaFree(p);
   if (c->h_norms) cudaFreeHost(c->h_norms);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -490,6 +522,64 @@ int cgli_channel_metrics_host(int nx, int ny, int nz, double det, double high, d
   }
   if (!src) return fail(CGLI_EINVAL, std::string("unknown metric ") + name);
   memcpy(out, src->data(), src->size() * sizeof(double));
+  return CGLI_OK;
+}
+
+int cgli_event_record(cgli_ctx *c, int slot) {
+  int rc = check(c); if (rc) return rc;
+  if (slot < 0 || slot >= 8) return fail(CGLI_EINVAL, "event slot out of range");
+  CUDA_TRY(cudaEventRecord(c->events[slot], c->stream));
+  return CGLI_OK;
+}
+
+int cgli_event_elapsed(cgli_ctx *c, int a, int b, float *ms) {
+  int rc = check(c); if (rc) return rc;
+  if (a < 0 || a >= 8 || b < 0 || b >= 8 || !ms) return fail(CGLI_EINVAL, "bad argument");
+  CUDA_TRY(cudaEventSynchronize(c->events[b]));
+  CUDA_TRY(cudaEventElapsedTime(ms, c->events[a], c->events[b]));
+  return CGLI_OK;
+}
+
+int cgli_profile_stages(cgli_ctx *c, int reps, double *ms) {
+  int rc = check(c); if (rc) return rc;
+  rc = need_ready(c); if (rc) return rc;
+  if (!ms || reps < 1) return fail(CGLI_EINVAL, "bad argument");
+  if (!c->metrics_checked) { rc = check_channel_metrics(c); if (rc) return rc; }
+  const bool mixed = c->p.precision == CGLI_MIXED;
+  cudaEvent_t ev[CGLI_NSTAGES + 1];
+  for (auto &e : ev) CUDA_TRY(cudaEventCreate(&e));
+  double tot[CGLI_NSTAGES] = {0};
+  for (int r = 0; r < reps; r++) {
+    // the sweep stages stand for two passes each; time the first of each kind
+    CUDA_TRY(cudaEventRecord(ev[0], c->stream));
+    cgli::launch_halo_bc(c->d, c->stream);
+    CUDA_TRY(cudaEventRecord(ev[1], c->stream));
+    cgli::launch_flux_x(c->d, c->stream);
+    CUDA_TRY(cudaEventRecord(ev[2], c->stream));
+    cgli::launch_flux_y(c->d, c->stream);
+    CUDA_TRY(cudaEventRecord(ev[3], c->stream));
+    cgli::launch_flux_z(c->d, c->stream);
+    CUDA_TRY(cudaEventRecord(ev[4], c->stream));
+    cgli::launch_viscous(c->d, c->stream);
+    CUDA_TRY(cudaEventRecord(ev[5], c->stream));
+    cgli::launch_residual_fast(c->d, c->sw, c->stream, mixed);
+    CUDA_TRY(cudaEventRecord(ev[6], c->stream));
+    cgli::launch_sweep_pass(c->d, c->sw, c->stream, mixed, false, false);
+    CUDA_TRY(cudaEventRecord(ev[7], c->stream));
+    cgli::launch_sweep_pass(c->d, c->sw, c->stream, mixed, true, false);
+    CUDA_TRY(cudaEventRecord(ev[8], c->stream));
+    cgli::launch_sweep_pass(c->d, c->sw, c->stream, mixed, false, false);
+    cgli::launch_sweep_pass(c->d, c->sw, c->stream, mixed, true, true);
+    rc = last_launch("profile_stages"); if (rc) return rc;
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    for (int s = 0; s < CGLI_NSTAGES; s++) {
+      float t = 0;
+      CUDA_TRY(cudaEventElapsedTime(&t, ev[s], ev[s + 1]));
+      tot[s] += t;
+    }
+  }
+  for (auto &e : ev) cudaEventDestroy(e);
+  for (int s = 0; s < CGLI_NSTAGES; s++) ms[s] = tot[s] / reps;
   return CGLI_OK;
 }
 

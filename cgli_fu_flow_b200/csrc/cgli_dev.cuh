@@ -266,4 +266,151 @@ __device__ __forceinline__ void block_sum5(double acc[5], double *out) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Coefficients of the LU-SGS sweeps with each division by a repeated divisor
+// replaced by one reciprocal and multiplications (the reference divides every
+// time; results differ from it by rounding only).  Used by the wavefront
+// sweeps, where these quantities are formed once per cell and pass.
+template <typename T>
+struct SweepCoef {
+  T d11, d22, d51;           // own diagonal, Dual_time_stepping.cpp:887-895
+  Split<T> A[3];             // split Jacobians in x, y, z (A+ entries and A- diagonals)
+  T rho, u, v, w, P, Tt;     // primitive state (for the update)
+};
+
+template <typename T>
+__device__ __forceinline__ Split<T> split_fast(T beta, T C, T P, T Tt, T rrho, T u, T v, T w, T mx, T my, T mz,
+                                               bool xdir, T &lam) {
+  const T K = (T)KG;
+  Split<T> a;
+  T U = mx * u + my * v + mz * w;
+  T S = sqrt(U * U * (beta - 1) * (beta - 1) + 4 * beta * C * (mx * mx + my * my + mz * mz));
+  T lambdaX = ((beta + 1) * fabs(U) + S) * (T)0.5;
+  lam = lambdaX;
+  T dd = fabs(lambdaX);
+  T hPKb = (T)0.5 * P * K * beta;
+  a.p11 = (T)0.5 * (beta * U + dd);
+  a.p12 = hPKb * mx;
+  a.p13 = hPKb * my;
+  a.p14 = hPKb * mz;
+  T hr = (T)0.5 * rrho;
+  a.p21 = hr * mx;
+  a.p22 = (T)0.5 * (U + dd);
+  a.p31 = hr * my;
+  a.p41 = hr * mz;
+  a.p51 = (T)0.5 * U * (K - 1) * (beta - 1) * rrho * (T)(1.0 / KG);
+  T hbT = xdir ? (T)0.5 * beta * Tt * (K - 1) : (T)0.5 * beta * Tt * (K - 1);
+  a.p52 = hbT * mx;
+  a.p53 = hbT * my;
+  a.p54 = hbT * mz;
+  a.m11 = (T)0.5 * (beta * U - dd);
+  a.m22 = (T)0.5 * (U - dd);
+  return a;
+}
+
+// q1..q5 = Q/J of the cell, J its Jacobian, mm its nine metric terms;
+// rdx = 1/deltaXI etc.
+template <typename T>
+__device__ __forceinline__ void sweep_coef(T q1, T q2, T q3, T q4, T q5, T J, const T mm[9], T e, T rdx, T rdy,
+                                           T rdz, T dt, SweepCoef<T> &c) {
+  const T K = (T)KG;
+  T rq1 = (T)1 / q1;
+  T rho = q1 * J;
+  T u = q2 * rq1, v = q3 * rq1, w = q4 * rq1;
+  T VV = u * u + v * v + w * w;
+  T P = (q5 * J - (T)0.5 * rho * VV) * (K - 1);
+  T rrho = (T)1 / rho;
+  T C = K * P * rrho;
+  T Tt = P * rrho;
+  T th = VV / C;
+  T beta = th > e ? th : e;
+  T lx, ly, lz;
+  c.A[0] = split_fast<T>(beta, C, P, Tt, rrho, u, v, w, mm[0], mm[1], mm[2], true, lx);
+  c.A[1] = split_fast<T>(beta, C, P, Tt, rrho, u, v, w, mm[3], mm[4], mm[5], false, ly);
+  c.A[2] = split_fast<T>(beta, C, P, Tt, rrho, u, v, w, mm[6], mm[7], mm[8], false, lz);
+  T lambda = lx * rdx + ly * rdy + lz * rdz;
+  T ld = 2 * lambda * dt;
+  T a1 = (T)1 / (3 * beta + ld);
+  T a2 = (T)1 / (3 + ld);
+  c.d11 = 2 * dt * a1;
+  c.d22 = 2 * dt * a2;
+  c.d51 = -(6 * (K - 1) * (beta - 1) * dt) * (a1 * a2) * rrho * (T)(1.0 / KG);
+  c.rho = rho; c.u = u; c.v = v; c.w = w; c.P = P; c.Tt = Tt;
+}
+
+// ---------------------------------------------------------------------------
+// Compact per-cell record of everything the sweeps need, formed once per inner
+// iteration by the residual kernel (the coefficients are the same in all four
+// passes).  With the face metric (mx, my, mz) of a direction the split
+// Jacobian entries are
+//   p11 = (beta U + lam)/2    p12..14 = h (mx, my, mz)    p21,31,41 = hr (mx, my, mz)
+//   p22 = (U + lam)/2         p51 = g U                   p52..54 = hbT (mx, my, mz)
+//   m11 = (beta U - lam)/2    m22 = (U - lam)/2
+// with U = mx u + my v + mz w the contravariant velocity, lam its spectral
+// radius (Dual_time_stepping.cpp:1040-1072 and :1384-1409), h = P K beta / 2,
+// hr = 1 / (2 rho), hbT = beta T (K-1) / 2, g = (K-1)(beta-1) / (2 rho K); the
+// own diagonal d11, d22, d51 of :887-895.
+constexpr int REC_N = 14;
+enum { R_BETA = 0, R_H, R_HR, R_HBT, R_G, R_UX, R_UY, R_UZ, R_LX, R_LY, R_LZ, R_D11, R_D22, R_D51 };
+
+__device__ __forceinline__ void make_record(double q1, double q2, double q3, double q4, double q5, double J,
+                                            const double mm[9], double e, double rdx, double rdy, double rdz,
+                                            double dt, double r[REC_N]) {
+  const double K = KG;
+  double rq1 = 1.0 / q1;
+  double rho = q1 * J;
+  double u = q2 * rq1, v = q3 * rq1, w = q4 * rq1;
+  double VV = u * u + v * v + w * w;
+  double P = (q5 * J - 0.5 * rho * VV) * (K - 1);
+  double rrho = 1.0 / rho;
+  double C = K * P * rrho;
+  double Tt = P * rrho;
+  double th = VV / C;
+  double beta = th > e ? th : e;
+  double lam[3], U[3];
+#pragma unroll
+  for (int dd = 0; dd < 3; dd++) {
+    double mx = mm[3 * dd], my = mm[3 * dd + 1], mz = mm[3 * dd + 2];
+    U[dd] = mx * u + my * v + mz * w;
+    double S = sqrt(U[dd] * U[dd] * (beta - 1) * (beta - 1) + 4 * beta * C * (mx * mx + my * my + mz * mz));
+    lam[dd] = ((beta + 1) * fabs(U[dd]) + S) * 0.5;
+  }
+  double lambda = lam[0] * rdx + lam[1] * rdy + lam[2] * rdz;
+  double ld = 2 * lambda * dt;
+  double a1 = 1.0 / (3 * beta + ld);
+  double a2 = 1.0 / (3 + ld);
+  r[R_BETA] = beta;
+  r[R_H] = 0.5 * P * K * beta;
+  r[R_HR] = 0.5 * rrho;
+  r[R_HBT] = 0.5 * beta * Tt * (K - 1);
+  r[R_G] = 0.5 * (K - 1) * (beta - 1) * rrho * (1.0 / KG);
+  r[R_UX] = U[0]; r[R_UY] = U[1]; r[R_UZ] = U[2];
+  r[R_LX] = lam[0]; r[R_LY] = lam[1]; r[R_LZ] = lam[2];
+  r[R_D11] = 2 * dt * a1;
+  r[R_D22] = 2 * dt * a2;
+  r[R_D51] = -(6 * (K - 1) * (beta - 1) * dt) * (a1 * a2) * rrho * (1.0 / KG);
+}
+
+// split Jacobian entries of one direction from a record
+template <typename T>
+__device__ __forceinline__ Split<T> split_from_record(const T r[REC_N], int dir, T mx, T my, T mz) {
+  const T U = r[R_UX + dir], lam = r[R_LX + dir], beta = r[R_BETA];
+  Split<T> a;
+  a.p11 = (T)0.5 * (beta * U + lam);
+  a.p12 = r[R_H] * mx;
+  a.p13 = r[R_H] * my;
+  a.p14 = r[R_H] * mz;
+  a.p21 = r[R_HR] * mx;
+  a.p31 = r[R_HR] * my;
+  a.p41 = r[R_HR] * mz;
+  a.p22 = (T)0.5 * (U + lam);
+  a.p51 = r[R_G] * U;
+  a.p52 = r[R_HBT] * mx;
+  a.p53 = r[R_HBT] * my;
+  a.p54 = r[R_HBT] * mz;
+  a.m11 = (T)0.5 * (beta * U - lam);
+  a.m22 = (T)0.5 * (U - lam);
+  return a;
+}
+
 }  // namespace cgli

@@ -15,10 +15,19 @@ constexpr int CGLI_TIMEOUT_CODE = 6;
 
 // buffers of the tile-wavefront sweeps (kernels_sweep.cu)
 struct SweepArgs {
+  // per-cell sweep data in the tile-skewed layout: slot (tile, forward step,
+  // thread) = (tile * S + s) * TI*TJ + t, S = Nz + TI + TJ - 2
   double *dq[5];                  // dQ: forward result, then backward result (in place)
-  double *halo_f[5], *halo_b[5];  // lagged periodic halo planes, Y_m x Z_m each
+  double *mrs[5];                 // residual MR
+  double *rec[REC_N];             // split-Jacobian / diagonal record
+  // the same in float for CGLI_MIXED
+  float *dqf[5], *mrf[5], *recf[REC_N];
+  // periodic lagged halos, indexed j*Z_m + k: dQ of plane ie (forward) / 3
+  // (backward) and the records of planes 2 / ie+1
+  double *halo_f[5], *halo_b[5], *hrec_f[REC_N], *hrec_b[REC_N];
+  float *halo_ff[5], *halo_bf[5], *hrecf_f[REC_N], *hrecf_b[REC_N];
   double *xbuf, *ybuf;            // products handed between tiles
-  unsigned long long *prog;       // per-tile progress counters
+  float *xbuff, *ybuff;
   unsigned int *ticket;           // tile ticket counter
   const int *order;               // tile visiting order (anti-diagonals)
   const double *Jtab, *etdytab;   // per-j metrics of a grid uniform in x and z
@@ -27,10 +36,26 @@ struct SweepArgs {
   int spin_limit;                 // bounded wait (polls) for a neighbouring tile
 };
 
+// slot of cell (i, j, k) in the tile-skewed layout
+__host__ __device__ __forceinline__ long long skew_slot(const Dev &d, int i, int j, int k) {
+  const int ntj = (d.ny + SWEEP_TJ - 1) / SWEEP_TJ;
+  const int S = d.nz + SWEEP_TI + SWEEP_TJ - 2;
+  const int il = (i - 3) % SWEEP_TI, jl = (j - 2) % SWEEP_TJ;
+  const int tile = ((i - 3) / SWEEP_TI) * ntj + (j - 2) / SWEEP_TJ;
+  const int s = (k - 2) + il + jl;
+  return ((long long)tile * S + s) * (SWEEP_TI * SWEEP_TJ) + il * SWEEP_TJ + jl;
+}
+__host__ __device__ __forceinline__ long long skew_size(const Dev &d) {
+  const long long ntiles = (long long)((d.nx + SWEEP_TI - 1) / SWEEP_TI) * ((d.ny + SWEEP_TJ - 1) / SWEEP_TJ);
+  return ntiles * (d.nz + SWEEP_TI + SWEEP_TJ - 2) * (SWEEP_TI * SWEEP_TJ);
+}
+
 void sweep_tile_order(int nti, int ntj, std::vector<int> &order);
-void launch_sweeps(const Dev &d, const SweepArgs &a, cudaStream_t s);
+void launch_sweeps(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed);
+// one pass (forward / backward, final with the update) of the sweeps
+void launch_sweep_pass(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed, bool backward, bool final_pass);
 // residual assembly writing MR and the first sweep's lagged halo planes
-void launch_residual_fast(const Dev &d, const SweepArgs &a, cudaStream_t s);
+void launch_residual_fast(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed);
 
 void launch_halo_bc(const Dev &d, cudaStream_t s);
 void launch_halo_x(const Dev &d, cudaStream_t s);

@@ -10,13 +10,39 @@ namespace cgli {
 // cell, and D^-1 MR on planes ie and 3 as the lagged halos of the first sweep
 // (the reference initialises NL = NR = D^-1 MR, :897-908, and the sweep
 // exchanges planes ie and 3 before its first pass, :942-976)
+template <bool MIXED>
 __global__ void k_residual_fast(Dev d, SweepArgs a) {
   int k = 2 + blockIdx.x * blockDim.x + threadIdx.x;
   int j = 2 + blockIdx.y;
-  int i = 3 + blockIdx.z;
+  int i = 2 + blockIdx.z;
   if (k > d.nz + 1) return;
   long long c = ix(d, i, j, k);
   const double J = d.J[c], deltaT = d.dt;
+  const int ie = d.nx + 2;
+  const bool halo_plane = (i == 2 || i == ie + 1);
+  const long long slot = halo_plane ? 0 : skew_slot(d, i, j, k);
+  {
+    // the cell's sweep record; planes 2 and ie+1 (the periodic halo copies)
+    // go to the per-(j,k) halo records
+    double mm[9], r[REC_N];
+    for (int v2 = 0; v2 < 9; v2++) mm[v2] = d.m[v2][c];
+    make_record(d.U_[0][c], d.U_[1][c], d.U_[2][c], d.U_[3][c], d.U_[4][c], J, mm, d.e, 1.0 / d.dxi, 1.0 / d.det,
+                1.0 / d.dzt, deltaT, r);
+    const long long h = (long long)j * d.dj + k;
+    for (int v2 = 0; v2 < REC_N; v2++) {
+      if (MIXED) {
+        float rv = (float)r[v2];
+        if (i == 2) a.hrecf_f[v2][h] = rv;
+        else if (i == ie + 1) a.hrecf_b[v2][h] = rv;
+        else a.recf[v2][slot] = rv;
+      } else {
+        if (i == 2) a.hrec_f[v2][h] = r[v2];
+        else if (i == ie + 1) a.hrec_b[v2][h] = r[v2];
+        else a.rec[v2][slot] = r[v2];
+      }
+    }
+  }
+  if (halo_plane) return;
   CPrim<double> q = cprim<double>(d.U_[0][c], d.U_[1][c], d.U_[2][c], d.U_[3][c], d.U_[4][c], J, d.e);
   double rho = q.rho, u = q.u, v = q.v, w = q.w, VV = q.VV, T = q.Tt, H = q.H, beta = q.beta;
   double temp = rho * KG;
@@ -51,8 +77,10 @@ __global__ void k_residual_fast(Dev d, SweepArgs a) {
   MR[2] = (d31 * Rk[0] + d22 * Rk[2]);
   MR[3] = (d41 * Rk[0] + d22 * Rk[3]);
   MR[4] = (d51 * Rk[0] + d52 * Rk[1] + d53 * Rk[2] + d54 * Rk[3] + d55 * Rk[4]);
-  for (int n = 0; n < 5; n++) d.MR[n][c] = MR[n];
-  const int ie = d.nx + 2;
+  for (int n = 0; n < 5; n++) {
+    if (MIXED) a.mrf[n][slot] = (float)MR[n];
+    else a.mrs[n][slot] = MR[n];
+  }
   if (i == ie || i == 3) {
     double mm[9];
     for (int v2 = 0; v2 < 9; v2++) mm[v2] = d.m[v2][c];
@@ -60,25 +88,32 @@ __global__ void k_residual_fast(Dev d, SweepArgs a) {
     double n5[5] = {dd.d11 * MR[0], dd.d22 * MR[1], dd.d22 * MR[2], dd.d22 * MR[3], dd.d51 * MR[0] + dd.d22 * MR[4]};
     long long h = (long long)j * d.dj + k;
     for (int n = 0; n < 5; n++) {
-      if (i == ie) a.halo_f[n][h] = n5[n];
-      if (i == 3) a.halo_b[n][h] = n5[n];
+      if (MIXED) {
+        if (i == ie) a.halo_ff[n][h] = (float)n5[n];
+        if (i == 3) a.halo_bf[n][h] = (float)n5[n];
+      } else {
+        if (i == ie) a.halo_f[n][h] = n5[n];
+        if (i == 3) a.halo_b[n][h] = n5[n];
+      }
     }
   }
 }
 
-void launch_residual_fast(const Dev &d, const SweepArgs &a, cudaStream_t s) {
-  k_residual_fast<<<dim3((d.nz + 63) / 64, d.ny, d.nx), 64, 0, s>>>(d, a);
+void launch_residual_fast(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed) {
+  dim3 g((d.nz + 63) / 64, d.ny, d.nx + 2);
+  if (mixed) k_residual_fast<true><<<g, 64, 0, s>>>(d, a);
+  else k_residual_fast<false><<<g, 64, 0, s>>>(d, a);
 }
 
 void launch_fused_iteration(const Dev &d, const SweepArgs &a, cudaStream_t s, int precision) {
-  (void)precision;
   launch_halo_bc(d, s);
   launch_flux_x(d, s);
   launch_flux_y(d, s);
   launch_flux_z(d, s);
   launch_viscous(d, s);
-  launch_residual_fast(d, a, s);
-  launch_sweeps(d, a, s);
+  const bool mixed = precision == 1;
+  launch_residual_fast(d, a, s, mixed);
+  launch_sweeps(d, a, s, mixed);
 }
 
 }  // namespace cgli

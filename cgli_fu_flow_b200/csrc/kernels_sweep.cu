@@ -4,21 +4,27 @@
 // (i+j+k = m, Dual_time_stepping.cpp:983-1664), one OpenMP barrier per
 // plane.  A cell's update depends only on its three upwind neighbours, so
 // any order that respects that dependency graph gives the same numbers.
-// Here each CTA owns a TI x TJ tile of (i, j) columns and marches along k
-// (the contiguous direction, so every thread streams its own k-line).
-// Thread (il, jl) handles cell k = 2 + s - il - jl at step s: its i- and
-// j-neighbours were handled by the neighbouring threads one step earlier and
-// hand over their lower-triangular products through shared memory; its
-// k-neighbour is its own previous step.  Tiles exchange the products of their
-// last row / column through global buffers, guarded by per-tile progress
-// counters with a bounded spin (no unbounded waits: on timeout the kernel
-// records CGLI_ETIMEOUT in the status word and carries on).  Tiles take
-// tickets in an order where every dependency holds a smaller ticket, so a
-// waiting CTA only waits on CTAs that are already running.
+// Here each CTA owns a TI x TJ tile of (i, j) columns and marches along k.
+// Thread (il, jl) handles cell k = 2 + s - il - jl at step s of the forward
+// pass: its i- and j-neighbours were handled by the neighbouring threads one
+// step earlier and hand over their products A.dQ through shared memory; its
+// k-neighbour is its own previous step.  The backward pass runs the mirror
+// image, and its step s visits exactly the cells of forward step S-1-s.
 //
-// Every cell computes its own primitive state, diagonal and split Jacobians
-// once per pass (the reference recomputes each neighbour's Jacobians for
-// every consumer), and each product A+ . dQ is formed by the cell that owns A+.
+// Storage.  Everything the sweeps read per cell -- the split-Jacobian /
+// diagonal record, the residual MR and dQ -- lives in a tile-skewed layout,
+// slot (tile, forward step, thread), so at every step the threads of a tile
+// read and write consecutive words (the residual kernel writes it).  Only the
+// final update touches the reference layout.
+//
+// Hand-over between tiles.  Tiles pass the products of their last row /
+// column through global buffers filled with a sentinel bit pattern before the
+// pass; the consumer spins (bounded) on the values themselves until none is
+// the sentinel, so a hand-over needs no fence and no counter (4- and 8-byte
+// stores are single-copy atomic).  On timeout the kernel records the timeout
+// code in the status word and carries on; the host reports CGLI_ETIMEOUT.
+// Tiles take tickets in an order where every dependency holds a smaller
+// ticket, so a waiting CTA only ever waits on CTAs that are already running.
 //
 // The periodic x halo keeps the reference's lag: the forward pass at i = 3
 // uses dQ of plane Nx+2 as it was at the start of the sweep (halo_f), the
@@ -26,56 +32,137 @@
 // the first sweep writes both halos for the second sweep; the final backward
 // pass also applies the primitive update of Dual_time_stepping.cpp:1702-1743
 // and accumulates the squared increments of the residual norms.
+//
+// T is the arithmetic type of the sweep (double, or float for CGLI_MIXED).
 #include "cgli_dev.cuh"
 #include "cgli_launch.h"
 
 namespace cgli {
 
-// cell metrics: general 3-D arrays, or a grid uniform in x and z (channel)
-// whose only varying terms are J(j) and etdy(j)
+template <typename T> struct SweepPtrs;
+template <> struct SweepPtrs<double> {
+  __device__ __forceinline__ static double *const *dq(const SweepArgs &a) { return a.dq; }
+  __device__ __forceinline__ static double *const *mr(const SweepArgs &a) { return a.mrs; }
+  __device__ __forceinline__ static double *const *rec(const SweepArgs &a) { return a.rec; }
+  __device__ __forceinline__ static double *const *hf(const SweepArgs &a) { return a.halo_f; }
+  __device__ __forceinline__ static double *const *hb(const SweepArgs &a) { return a.halo_b; }
+  __device__ __forceinline__ static double *const *hrec(const SweepArgs &a, bool b) { return b ? a.hrec_b : a.hrec_f; }
+  __device__ __forceinline__ static double *xb(const SweepArgs &a) { return a.xbuf; }
+  __device__ __forceinline__ static double *yb(const SweepArgs &a) { return a.ybuf; }
+};
+template <> struct SweepPtrs<float> {
+  __device__ __forceinline__ static float *const *dq(const SweepArgs &a) { return a.dqf; }
+  __device__ __forceinline__ static float *const *mr(const SweepArgs &a) { return a.mrf; }
+  __device__ __forceinline__ static float *const *rec(const SweepArgs &a) { return a.recf; }
+  __device__ __forceinline__ static float *const *hf(const SweepArgs &a) { return a.halo_ff; }
+  __device__ __forceinline__ static float *const *hb(const SweepArgs &a) { return a.halo_bf; }
+  __device__ __forceinline__ static float *const *hrec(const SweepArgs &a, bool b) { return b ? a.hrecf_b : a.hrecf_f; }
+  __device__ __forceinline__ static float *xb(const SweepArgs &a) { return a.xbuff; }
+  __device__ __forceinline__ static float *yb(const SweepArgs &a) { return a.ybuff; }
+};
+
+// face-direction metrics of a cell: general 3-D arrays, or a grid uniform in
+// x and z (channel) whose only varying term is etdy(j), held in shared memory
 struct MetricsGeneral {
-  __device__ __forceinline__ static void load(const Dev &d, const SweepArgs &, long long c, int, double &J, double mm[9]) {
-    J = d.J[c];
+  static constexpr bool kChannel = false;
+  template <typename T>
+  __device__ __forceinline__ static void dirs(const Dev &d, const double *, long long c, int, T mm[9]) {
 #pragma unroll
-    for (int v = 0; v < 9; v++) mm[v] = d.m[v][c];
+    for (int v = 0; v < 9; v++) mm[v] = (T)d.m[v][c];
   }
 };
 struct MetricsChannel {
-  __device__ __forceinline__ static void load(const Dev &, const SweepArgs &a, long long, int j, double &J, double mm[9]) {
-    J = a.Jtab[j];
+  static constexpr bool kChannel = true;
+  template <typename T>
+  __device__ __forceinline__ static void dirs(const Dev &, const double *et, long long, int jl, T mm[9]) {
     mm[0] = 1; mm[1] = 0; mm[2] = 0;
-    mm[3] = 0; mm[4] = a.etdytab[j]; mm[5] = 0;
+    mm[3] = 0; mm[4] = (T)et[jl]; mm[5] = 0;
     mm[6] = 0; mm[7] = 0; mm[8] = 1;
   }
 };
 
-// bounded wait until counter >= need; thread 0 only
-__device__ __forceinline__ void wait_counter(const unsigned long long *ctr, unsigned long long need,
-                                             unsigned long long &cache, int *status, int spin_limit) {
-  if (cache >= need) return;
-  int it = 0;
-  while (true) {
-    unsigned long long v;
-    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(ctr) : "memory");
-    cache = v;
-    if (v >= need) return;
-    if (++it > spin_limit) {
+__device__ __forceinline__ double ld_gpu(const double *p) {
+  double v;
+  asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ float ld_gpu(const float *p) {
+  float v;
+  asm volatile("ld.relaxed.gpu.global.f32 %0, [%1];" : "=f"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ bool is_sentinel(double v) { return __double_as_longlong(v) == -1ll; }
+__device__ __forceinline__ bool is_sentinel(float v) { return __float_as_int(v) == -1; }
+
+// bounded spin on five values handed over by a neighbouring tile
+template <typename T>
+__device__ __forceinline__ void recv5(const T *src, T out[5], int *status, int limit) {
+  for (int it = 0;; it++) {
+    bool ok = true;
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+      out[v] = ld_gpu(src + v);
+      ok = ok && !is_sentinel(out[v]);
+    }
+    if (ok) return;
+    if (it >= limit) {
       atomicExch(status, CGLI_TIMEOUT_CODE);
-      cache = need;  // give up waiting; results of this pass are invalid
       return;
     }
-    __nanosleep(64);
+    __nanosleep(20);
   }
 }
 
-__device__ __forceinline__ void publish(unsigned long long *ctr, unsigned long long v) {
-  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(ctr), "l"(v) : "memory");
+// one cell's sweep inputs
+template <typename T>
+struct Cell {
+  bool active;
+  long long slot;   // tile-skewed slot
+  T rec[REC_N];     // split-Jacobian / diagonal record
+  T mr[5];          // forward: MR; backward: this cell's forward result
+  T hx[5];          // product from the periodic lagged halo (x edge of the slab)
+  bool has_hx;
+};
+
+template <int TI, int TJ, class Met, bool BACKWARD, typename T>
+__device__ __forceinline__ void fetch_cell(const Dev &d, const SweepArgs &a, const double *et, int il, int jl,
+                                           int j, int s, int S, long long tile_base, bool inside, bool halo_edge,
+                                           Cell<T> &x) {
+  const int rel = BACKWARD ? s - (TI - 1 - il) - (TJ - 1 - jl) : s - il - jl;
+  x.active = inside && rel >= 0 && rel < d.nz;
+  x.has_hx = false;
+  if (!x.active) return;
+  const int sf = BACKWARD ? S - 1 - s : s;   // forward step of this cell
+  const long long slot = tile_base + (long long)sf * (TI * TJ) + threadIdx.x;
+  x.slot = slot;
+#pragma unroll
+  for (int v = 0; v < REC_N; v++) x.rec[v] = SweepPtrs<T>::rec(a)[v][slot];
+#pragma unroll
+  for (int v = 0; v < 5; v++) x.mr[v] = BACKWARD ? SweepPtrs<T>::dq(a)[v][slot] : SweepPtrs<T>::mr(a)[v][slot];
+  if (halo_edge) {
+    // periodic lagged halo: the x neighbour is plane 2 (forward) or ie+1
+    // (backward), a copy of plane ie / 3 made by the Q halo exchange; its
+    // record and the lagged dQ are kept per (j, k)
+    const int kl = BACKWARD ? d.nz - 1 - rel : rel;
+    const long long h = (long long)j * d.dj + 2 + kl;
+    T rn[REC_N], mm[9];
+#pragma unroll
+    for (int v = 0; v < REC_N; v++) rn[v] = SweepPtrs<T>::hrec(a, BACKWARD)[v][h];
+    Met::template dirs<T>(d, et, h + (BACKWARD ? (long long)(d.nx + 3) : 2LL) * d.di, jl, mm);
+    Split<T> An = split_from_record<T>(rn, 0, mm[0], mm[1], mm[2]);
+    T nh[5];
+#pragma unroll
+    for (int v = 0; v < 5; v++) nh[v] = BACKWARD ? SweepPtrs<T>::hb(a)[v][h] : SweepPtrs<T>::hf(a)[v][h];
+    if (BACKWARD) upper_terms<T>(An, nh, x.hx); else lower_terms<T>(An, nh, x.hx);
+    x.has_hx = true;
+  }
 }
 
-template <int TI, int TJ, class Met, bool BACKWARD>
+template <int TI, int TJ, class Met, bool BACKWARD, typename T>
 __global__ void __launch_bounds__(TI *TJ) k_sweep(Dev d, SweepArgs a) {
-  __shared__ double sx[2][TI][TJ][5];   // i-direction products, double-buffered by step parity
-  __shared__ double sy[2][TI][TJ][5];   // j-direction products
+  __shared__ T sx[2][TI][TJ][5];   // i-direction products, double-buffered by step parity
+  __shared__ T sy[2][TI][TJ][5];   // j-direction products
+  __shared__ double s_jt[TJ], s_et[TJ];
   __shared__ int s_tile;
   __shared__ double s_red[5];
   const int il = threadIdx.x / TJ, jl = threadIdx.x % TJ;
@@ -84,184 +171,160 @@ __global__ void __launch_bounds__(TI *TJ) k_sweep(Dev d, SweepArgs a) {
   __syncthreads();
   const int ticket = s_tile;
   if (ticket >= ntiles) return;
-  // tickets follow anti-diagonals of the tile grid (reversed for the backward pass)
   const int tile = a.order[BACKWARD ? ntiles - 1 - ticket : ticket];
   const int ta = tile / ntj, tb = tile % ntj;
   const int ie = d.nx + 2, jn = d.ny + 1;
   const int i = 3 + ta * TI + il, j = 2 + tb * TJ + jl;
   const bool inside = (i <= ie) && (j <= jn);
+  if (threadIdx.x < TJ) {
+    int jj = 2 + tb * TJ + threadIdx.x;
+    s_jt[threadIdx.x] = (Met::kChannel && jj <= jn) ? a.Jtab[jj] : 1.0;
+    s_et[threadIdx.x] = (Met::kChannel && jj <= jn) ? a.etdytab[jj] : 0.0;
+  }
+  __syncthreads();
   const int Nz = d.nz;
   const int S = Nz + TI - 1 + TJ - 1;
-  // neighbouring tiles this one depends on
+  const long long tile_base = (long long)tile * S * (TI * TJ);
   const int pa = BACKWARD ? ta + 1 : ta - 1, pb = BACKWARD ? tb + 1 : tb - 1;
-  const bool has_pa = pa >= 0 && pa < nti, has_pb = pb >= 0 && pb < ntj;
   const int tile_pa = pa * ntj + tb, tile_pb = ta * ntj + pb;
-  // threads on the tile edge that read from / write to the neighbour tiles
-  const bool recv_x = BACKWARD ? (il == TI - 1 || i == ie) : (il == 0);
+  const bool halo_edge = BACKWARD ? (i == ie) : (i == 3);
+  const bool recv_x = !halo_edge && (BACKWARD ? il == TI - 1 : il == 0);
   const bool recv_y = BACKWARD ? (jl == TJ - 1 || j == jn) : (jl == 0);
+  const bool wall_y = BACKWARD ? (j == jn) : (j == 2);
   const bool send_x = BACKWARD ? (il == 0) : (il == TI - 1);
   const bool send_y = BACKWARD ? (jl == 0) : (jl == TJ - 1);
-  const double rdx = 1.0 / d.dxi, rdy = 1.0 / d.det, rdz = 1.0 / d.dzt;
-  (void)rdx; (void)rdy; (void)rdz;
-  unsigned long long cache_a = 0, cache_b = 0;
-  double carry_z[5] = {0, 0, 0, 0, 0};
+  const T rdx = (T)(1.0 / d.dxi), rdy = (T)(1.0 / d.det), rdz = (T)(1.0 / d.dzt);
+  T *xb = SweepPtrs<T>::xb(a), *yb = SweepPtrs<T>::yb(a);
+  T *const *dq = SweepPtrs<T>::dq(a);
+  T carry_z[5] = {0, 0, 0, 0, 0};
   double acc[5] = {0, 0, 0, 0, 0};
-  const bool last_x_tile = BACKWARD ? (ta == nti - 1) : (ta == 0);
+
+  Cell<T> cur, nxt;
+  fetch_cell<TI, TJ, Met, BACKWARD, T>(d, a, s_et, il, jl, j, 0, S, tile_base, inside, halo_edge, cur);
 
   for (int s = 0; s < S; s++) {
     const int rel = BACKWARD ? s - (TI - 1 - il) - (TJ - 1 - jl) : s - il - jl;
     const int kl = BACKWARD ? Nz - 1 - rel : rel;
-    const bool active = inside && rel >= 0 && rel < Nz;
-    const int k = 2 + kl;
-    const long long c = active ? ix(d, i, j, k) : 0;
-    // own state and coefficients (independent of the sweep)
-    CPrim<double> q;
-    Diag<double> dg;
-    Split<double> Ax, Ay, Az;
-    double mr[5];
-    double J = 1.0;
-    if (active) {
-      double mm[9];
-      Met::load(d, a, c, j, J, mm);
-      q = cprim<double>(d.U_[0][c], d.U_[1][c], d.U_[2][c], d.U_[3][c], d.U_[4][c], J, d.e);
-      dg = diag<double>(q, mm, d.dxi, d.det, d.dzt, d.dt);
-      Ax = split<double>(q, mm[0], mm[1], mm[2], true);
-      Ay = split<double>(q, mm[3], mm[4], mm[5], false);
-      Az = split<double>(q, mm[6], mm[7], mm[8], false);
+    // loads of the next cell go out first and land during the dependent part
+    if (s + 1 < S) fetch_cell<TI, TJ, Met, BACKWARD, T>(d, a, s_et, il, jl, j, s + 1, S, tile_base, inside, halo_edge, nxt);
+    else nxt.active = false;
+    if (cur.active) {
+      const int pbuf = (s - 1) & 1;
+      T tx[5], ty[5];
+      if (cur.has_hx) {
 #pragma unroll
-      for (int v = 0; v < 5; v++) mr[v] = BACKWARD ? a.dq[v][c] : d.MR[v][c];
-    }
-    // wait for the neighbouring tiles' products of this step
-    if (threadIdx.x == 0) {
-      if (has_pa) wait_counter(a.prog + tile_pa, (unsigned long long)min(s + TI, S), cache_a, d.status, a.spin_limit);
-      if (has_pb) wait_counter(a.prog + tile_pb, (unsigned long long)min(s + TJ, S), cache_b, d.status, a.spin_limit);
-    }
-    __syncthreads();
-    if (active) {
-      double tx[5], ty[5], tz[5];
-      const int pb_ = (s - 1) & 1;
-      // x neighbour
-      if (!recv_x) {
+        for (int v = 0; v < 5; v++) tx[v] = cur.hx[v];
+      } else if (!recv_x) {
         const int sil = BACKWARD ? il + 1 : il - 1;
 #pragma unroll
-        for (int v = 0; v < 5; v++) tx[v] = sx[pb_][sil][jl][v];
-      } else if (last_x_tile && (BACKWARD ? i == ie : i == 3)) {
-        // periodic lagged halo: the neighbour is plane 2 (forward) / ie+1 (backward)
-        const long long cn = BACKWARD ? c + d.di : c - d.di;
-        double Jn, mn[9];
-        Met::load(d, a, cn, j, Jn, mn);
-        CPrim<double> qn = cprim<double>(d.U_[0][cn], d.U_[1][cn], d.U_[2][cn], d.U_[3][cn], d.U_[4][cn], Jn, d.e);
-        Split<double> An = split<double>(qn, mn[0], mn[1], mn[2], true);
-        const long long h = (long long)j * d.dj + k;
-        double nh[5];
-#pragma unroll
-        for (int v = 0; v < 5; v++) nh[v] = BACKWARD ? a.halo_b[v][h] : a.halo_f[v][h];
-        if (BACKWARD) upper_terms<double>(An, nh, tx); else lower_terms<double>(An, nh, tx);
-      } else if (has_pa) {
-        const double *src = a.xbuf + (((long long)tile_pa * TJ + jl) * Nz + kl) * 5;
-#pragma unroll
-        for (int v = 0; v < 5; v++) tx[v] = __ldcg(src + v);
+        for (int v = 0; v < 5; v++) tx[v] = sx[pbuf][sil][jl][v];
       } else {
-#pragma unroll
-        for (int v = 0; v < 5; v++) tx[v] = 0;
+        recv5<T>(xb + (((long long)tile_pa * TJ + jl) * Nz + kl) * 5, tx, d.status, a.spin_limit);
       }
-      // y neighbour
       if (!recv_y) {
         const int sjl = BACKWARD ? jl + 1 : jl - 1;
 #pragma unroll
-        for (int v = 0; v < 5; v++) ty[v] = sy[pb_][il][sjl][v];
-      } else if (has_pb && (BACKWARD ? j < jn : j > 2)) {
-        const double *src = a.ybuf + (((long long)tile_pb * TI + il) * Nz + kl) * 5;
-#pragma unroll
-        for (int v = 0; v < 5; v++) ty[v] = __ldcg(src + v);
+        for (int v = 0; v < 5; v++) ty[v] = sy[pbuf][il][sjl][v];
+      } else if (!wall_y) {
+        recv5<T>(yb + (((long long)tile_pb * TI + il) * Nz + kl) * 5, ty, d.status, a.spin_limit);
       } else {
 #pragma unroll
         for (int v = 0; v < 5; v++) ty[v] = 0;  // wall ghost row: dQ = 0 there
       }
-      // k neighbour: own previous step (zero next to the z ghost rows)
+      const bool zedge = rel == 0;             // z ghost row: dQ = 0 there
+      T L[5];
 #pragma unroll
-      for (int v = 0; v < 5; v++) tz[v] = (rel > 0) ? carry_z[v] : 0.0;
-      double L[5];
-#pragma unroll
-      for (int v = 0; v < 5; v++) L[v] = tx[v] / d.dxi + ty[v] / d.det + tz[v] / d.dzt;
-      double n[5];
+      for (int v = 0; v < 5; v++) L[v] = tx[v] * rdx + ty[v] * rdy + (zedge ? (T)0 : carry_z[v]) * rdz;
+      const T d11 = cur.rec[R_D11], d22 = cur.rec[R_D22], d51 = cur.rec[R_D51];
+      T n[5];
       if (!BACKWARD) {
         // Dual_time_stepping.cpp:1289-1293
-        double r1 = mr[0] - L[0];
-        n[0] = dg.d11 * r1;
-        n[1] = dg.d22 * (mr[1] - L[1]);
-        n[2] = dg.d22 * (mr[2] - L[2]);
-        n[3] = dg.d22 * (mr[3] - L[3]);
-        n[4] = dg.d51 * r1 + dg.d22 * (mr[4] - L[4]);
+        T r1 = cur.mr[0] - L[0];
+        n[0] = d11 * r1;
+        n[1] = d22 * (cur.mr[1] - L[1]);
+        n[2] = d22 * (cur.mr[2] - L[2]);
+        n[3] = d22 * (cur.mr[3] - L[3]);
+        n[4] = d51 * r1 + d22 * (cur.mr[4] - L[4]);
       } else {
         // Dual_time_stepping.cpp:1651-1655 (mr holds this cell's forward result)
-        n[0] = mr[0] - dg.d11 * L[0];
-        n[1] = mr[1] - dg.d22 * L[1];
-        n[2] = mr[2] - dg.d22 * L[2];
-        n[3] = mr[3] - dg.d22 * L[3];
-        n[4] = mr[4] - (dg.d51 * L[0] + dg.d22 * L[4]);
+        n[0] = cur.mr[0] - d11 * L[0];
+        n[1] = cur.mr[1] - d22 * L[1];
+        n[2] = cur.mr[2] - d22 * L[2];
+        n[3] = cur.mr[3] - d22 * L[3];
+        n[4] = cur.mr[4] - (d51 * L[0] + d22 * L[4]);
       }
-      if (BACKWARD && a.final_pass) {
-        // Dual_time_stepping.cpp:1702-1743: primitive update in place
-        double P = q.P + n[0] * J, U = q.u + n[1] * J, V = q.v + n[2] * J, W = q.w + n[3] * J;
-        double T = q.Tt + n[4] * J;
-        double rho = P / T;
-        d.U_[0][c] = rho / J;
-        d.U_[1][c] = rho * U / J;
-        d.U_[2][c] = rho * V / J;
-        d.U_[3][c] = rho * W / J;
-        d.U_[4][c] = (P / (KG - 1) + 0.5 * rho * (U * U + V * V + W * W)) / J;
-        acc[0] += (rho - q.rho) * (rho - q.rho);
-        acc[1] += (U - q.u) * (U - q.u);
-        acc[2] += (V - q.v) * (V - q.v);
-        acc[3] += (W - q.w) * (W - q.w);
-        acc[4] += (T - q.Tt) * (T - q.Tt);
-      } else {
-#pragma unroll
-        for (int v = 0; v < 5; v++) a.dq[v][c] = n[v];
+      const long long c = Met::kChannel ? 0 : ix(d, i, j, 2 + kl);
+      T mm[9];
+      Met::template dirs<T>(d, s_et, c, jl, mm);
+      T ox[5], oy[5];
+      {
+        Split<T> Ax = split_from_record<T>(cur.rec, 0, mm[0], mm[1], mm[2]);
+        Split<T> Ay = split_from_record<T>(cur.rec, 1, mm[3], mm[4], mm[5]);
+        Split<T> Az = split_from_record<T>(cur.rec, 2, mm[6], mm[7], mm[8]);
         if (BACKWARD) {
-          // lagged halos of the next sweep: plane ie feeds its forward pass,
-          // plane 3 its backward pass
-          const long long h = (long long)j * d.dj + k;
-          if (i == ie)
-            for (int v = 0; v < 5; v++) a.halo_f[v][h] = n[v];
-          if (i == 3)
-            for (int v = 0; v < 5; v++) a.halo_b[v][h] = n[v];
+          upper_terms<T>(Ax, n, ox);
+          upper_terms<T>(Ay, n, oy);
+          upper_terms<T>(Az, n, carry_z);
+        } else {
+          lower_terms<T>(Ax, n, ox);
+          lower_terms<T>(Ay, n, oy);
+          lower_terms<T>(Az, n, carry_z);
         }
       }
-      // products handed to the downwind neighbours
-      double ox[5], oy[5];
-      if (BACKWARD) {
-        upper_terms<double>(Ax, n, ox);
-        upper_terms<double>(Ay, n, oy);
-        upper_terms<double>(Az, n, carry_z);
-      } else {
-        lower_terms<double>(Ax, n, ox);
-        lower_terms<double>(Ay, n, oy);
-        lower_terms<double>(Az, n, carry_z);
-      }
       const int cb = s & 1;
+#pragma unroll
+      for (int v = 0; v < 5; v++) { sx[cb][il][jl][v] = ox[v]; sy[cb][il][jl][v] = oy[v]; }
       if (send_x) {
-        double *dst = a.xbuf + (((long long)tile * TJ + jl) * Nz + kl) * 5;
+        T *dst = xb + (((long long)tile * TJ + jl) * Nz + kl) * 5;
 #pragma unroll
         for (int v = 0; v < 5; v++) __stcg(dst + v, ox[v]);
       }
-#pragma unroll
-      for (int v = 0; v < 5; v++) sx[cb][il][jl][v] = ox[v];
       if (send_y) {
-        double *dst = a.ybuf + (((long long)tile * TI + il) * Nz + kl) * 5;
+        T *dst = yb + (((long long)tile * TI + il) * Nz + kl) * 5;
 #pragma unroll
         for (int v = 0; v < 5; v++) __stcg(dst + v, oy[v]);
       }
+      if (BACKWARD && a.final_pass) {
+        // Dual_time_stepping.cpp:1702-1743: primitive update in place (FP64)
+        const long long cc = ix(d, i, j, 2 + kl);
+        const double J = Met::kChannel ? s_jt[jl] : d.J[cc];
+        double q1 = d.U_[0][cc];
+        double rhoold = q1 * J;
+        double Uold = d.U_[1][cc] / q1, Vold = d.U_[2][cc] / q1, Wold = d.U_[3][cc] / q1;
+        double VVold = Uold * Uold + Vold * Vold + Wold * Wold;
+        double Pold = (d.U_[4][cc] * J - 0.5 * rhoold * VVold) * (KG - 1);
+        double Told = Pold / rhoold;
+        double P = Pold + (double)n[0] * J, U = Uold + (double)n[1] * J, V = Vold + (double)n[2] * J;
+        double W = Wold + (double)n[3] * J, Tn = Told + (double)n[4] * J;
+        double rho = P / Tn;
+        d.U_[0][cc] = rho / J;
+        d.U_[1][cc] = rho * U / J;
+        d.U_[2][cc] = rho * V / J;
+        d.U_[3][cc] = rho * W / J;
+        d.U_[4][cc] = (P / (KG - 1) + 0.5 * rho * (U * U + V * V + W * W)) / J;
+        acc[0] += (rho - rhoold) * (rho - rhoold);
+        acc[1] += (U - Uold) * (U - Uold);
+        acc[2] += (V - Vold) * (V - Vold);
+        acc[3] += (W - Wold) * (W - Wold);
+        acc[4] += (Tn - Told) * (Tn - Told);
+      } else {
 #pragma unroll
-      for (int v = 0; v < 5; v++) sy[cb][il][jl][v] = oy[v];
-      if (send_x || send_y) __threadfence();
+        for (int v = 0; v < 5; v++) dq[v][cur.slot] = n[v];
+        if (BACKWARD) {
+          // lagged halos of the next sweep: plane ie feeds its forward pass,
+          // plane 3 its backward pass
+          const long long h = (long long)j * d.dj + 2 + kl;
+          if (i == ie)
+            for (int v = 0; v < 5; v++) SweepPtrs<T>::hf(a)[v][h] = n[v];
+          if (i == 3)
+            for (int v = 0; v < 5; v++) SweepPtrs<T>::hb(a)[v][h] = n[v];
+        }
+      }
     }
+    cur = nxt;
     __syncthreads();
-    if (threadIdx.x == 0) publish(a.prog + tile, (unsigned long long)(s + 1));
   }
   if (BACKWARD && a.final_pass) {
-    __syncthreads();
     block_sum5(acc, s_red);
     __syncthreads();
     if (threadIdx.x == 0)
@@ -279,25 +342,60 @@ void sweep_tile_order(int nti, int ntj, std::vector<int> &order) {
     }
 }
 
-template <int TI, int TJ, class Met>
+template <int TI, int TJ, class Met, typename T>
 static void run_sweeps(const Dev &d, const SweepArgs &a, cudaStream_t s) {
   const int nti = (d.nx + TI - 1) / TI, ntj = (d.ny + TJ - 1) / TJ, ntiles = nti * ntj;
+  const size_t xbytes = (size_t)ntiles * TJ * d.nz * 5 * sizeof(T), ybytes = (size_t)ntiles * TI * d.nz * 5 * sizeof(T);
+  T *xb = sizeof(T) == 8 ? (T *)a.xbuf : (T *)a.xbuff;
+  T *yb = sizeof(T) == 8 ? (T *)a.ybuf : (T *)a.ybuff;
   for (int sweep = 0; sweep < 2; sweep++) {
     SweepArgs f = a, b = a;
     f.final_pass = 0;
     b.final_pass = sweep == 1;
-    cudaMemsetAsync(a.ticket, 0, sizeof(unsigned int), s);
-    cudaMemsetAsync(a.prog, 0, sizeof(unsigned long long) * ntiles, s);
-    k_sweep<TI, TJ, Met, false><<<ntiles, TI * TJ, 0, s>>>(d, f);
-    cudaMemsetAsync(a.ticket, 0, sizeof(unsigned int), s);
-    cudaMemsetAsync(a.prog, 0, sizeof(unsigned long long) * ntiles, s);
-    k_sweep<TI, TJ, Met, true><<<ntiles, TI * TJ, 0, s>>>(d, b);
+    for (int pass = 0; pass < 2; pass++) {
+      // ticket reset and sentinel fill of the hand-over buffers
+      cudaMemsetAsync(a.ticket, 0, sizeof(unsigned int), s);
+      cudaMemsetAsync(xb, 0xff, xbytes, s);
+      cudaMemsetAsync(yb, 0xff, ybytes, s);
+      if (pass == 0) k_sweep<TI, TJ, Met, false, T><<<ntiles, TI * TJ, 0, s>>>(d, f);
+      else k_sweep<TI, TJ, Met, true, T><<<ntiles, TI * TJ, 0, s>>>(d, b);
+    }
   }
 }
 
-void launch_sweeps(const Dev &d, const SweepArgs &a, cudaStream_t s) {
-  if (a.channel_metrics) run_sweeps<SWEEP_TI, SWEEP_TJ, MetricsChannel>(d, a, s);
-  else run_sweeps<SWEEP_TI, SWEEP_TJ, MetricsGeneral>(d, a, s);
+template <int TI, int TJ, class Met, typename T>
+static void run_one_pass(const Dev &d, const SweepArgs &a, cudaStream_t s, bool backward, bool final_pass) {
+  const int nti = (d.nx + TI - 1) / TI, ntj = (d.ny + TJ - 1) / TJ, ntiles = nti * ntj;
+  const size_t xbytes = (size_t)ntiles * TJ * d.nz * 5 * sizeof(T), ybytes = (size_t)ntiles * TI * d.nz * 5 * sizeof(T);
+  T *xb = sizeof(T) == 8 ? (T *)a.xbuf : (T *)a.xbuff;
+  T *yb = sizeof(T) == 8 ? (T *)a.ybuf : (T *)a.ybuff;
+  SweepArgs b = a;
+  b.final_pass = final_pass;
+  cudaMemsetAsync(a.ticket, 0, sizeof(unsigned int), s);
+  cudaMemsetAsync(xb, 0xff, xbytes, s);
+  cudaMemsetAsync(yb, 0xff, ybytes, s);
+  if (!backward) k_sweep<TI, TJ, Met, false, T><<<ntiles, TI * TJ, 0, s>>>(d, b);
+  else k_sweep<TI, TJ, Met, true, T><<<ntiles, TI * TJ, 0, s>>>(d, b);
+}
+
+void launch_sweep_pass(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed, bool backward, bool final_pass) {
+  if (mixed) {
+    if (a.channel_metrics) run_one_pass<SWEEP_TI, SWEEP_TJ, MetricsChannel, float>(d, a, s, backward, final_pass);
+    else run_one_pass<SWEEP_TI, SWEEP_TJ, MetricsGeneral, float>(d, a, s, backward, final_pass);
+  } else {
+    if (a.channel_metrics) run_one_pass<SWEEP_TI, SWEEP_TJ, MetricsChannel, double>(d, a, s, backward, final_pass);
+    else run_one_pass<SWEEP_TI, SWEEP_TJ, MetricsGeneral, double>(d, a, s, backward, final_pass);
+  }
+}
+
+void launch_sweeps(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed) {
+  if (mixed) {
+    if (a.channel_metrics) run_sweeps<SWEEP_TI, SWEEP_TJ, MetricsChannel, float>(d, a, s);
+    else run_sweeps<SWEEP_TI, SWEEP_TJ, MetricsGeneral, float>(d, a, s);
+  } else {
+    if (a.channel_metrics) run_sweeps<SWEEP_TI, SWEEP_TJ, MetricsChannel, double>(d, a, s);
+    else run_sweeps<SWEEP_TI, SWEEP_TJ, MetricsGeneral, double>(d, a, s);
+  }
 }
 
 }  // namespace cgli

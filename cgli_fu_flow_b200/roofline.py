@@ -1,0 +1,48 @@
+"""Roofline bookkeeping of the dominant kernel (the wavefront sweep passes).
+
+Algorithmic bytes of one sweep pass per cell, the per-unit figure of the
+hot-path scope (compulsory traffic with each array touched once per pass):
+the FP64 pass reads Q/J (5), J and nine metric terms (10) and MR or NL (5)
+and writes NL or NR (5): 25 doubles = 200 B; with the sweep state, metrics
+and MR/NL/NR in float (CGLI_MIXED) the same 25 words are 100 B.  The bound is
+HBM bandwidth (no dense contraction); the peak is the measured copy bandwidth
+of this GPU type (MEASURED_PEAKS.json, the burst figure, since the pass is
+timed alone), else 6650 GB/s, an earlier measurement on the same hardware.
+"""
+from __future__ import annotations
+
+import json
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PEAKS = os.path.join(os.path.dirname(HERE), "MEASURED_PEAKS.json")
+
+SWEEP_BYTES_PER_CELL = {"fp64": 25 * 8, "mixed": 25 * 4}
+
+# DRAM bytes (read + write) per cell of one sweep pass from an ncu capture of
+# k_sweep (gpu__time_duration / dram__bytes_read.sum + dram__bytes_write.sum,
+# forward and backward averaged), on the 160x128x128 channel; traffic grows
+# with the cell count, so it is scaled to the benchmark grid.  See
+# profiles/k_sweep_channel_160x128x128.md.
+MEASURED_TRAFFIC_PER_CELL = {"fp64": None, "mixed": None}
+
+
+def hbm_peak() -> tuple[float, str]:
+    try:
+        with open(PEAKS) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def sweep_roofline(ch, stage_ms: dict, precision: str) -> dict:
+    cells = ch.cells
+    bpc = SWEEP_BYTES_PER_CELL[precision]
+    dur_ms = 0.5 * (stage_ms["sweep_forward"] + stage_ms["sweep_backward"])
+    achieved = bpc * cells / (dur_ms / 1e3) / 1e9
+    peak, kind = hbm_peak()
+    tpc = MEASURED_TRAFFIC_PER_CELL.get(precision)
+    return {"kernel": "k_sweep (LU-SGS wavefront pass, forward/backward mean)", "bound": "hbm",
+            "achieved": round(achieved, 1), "peak": peak, "peak_kind": kind, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "traffic": None if tpc is None else int(tpc * cells),
+            "algorithmic_bytes_per_launch": bpc * cells, "launch_ms": round(dur_ms, 4)}

@@ -45,7 +45,7 @@ EXPORTS = [
     "cgli_y_boundary_condition", "cgli_z_boundary_condition", "cgli_flux_x", "cgli_flux_y",
     "cgli_flux_z", "cgli_viscous_terms", "cgli_dual_time_stepping", "cgli_inner_iteration",
     "cgli_driven_force", "cgli_end_step", "cgli_set_force", "cgli_step", "cgli_hyperplane",
-    "cgli_channel_metrics_host",
+    "cgli_channel_metrics_host", "cgli_profile_stages", "cgli_event_record", "cgli_event_elapsed",
 ]
 
 _lib = None
@@ -81,6 +81,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cgli_set_force.argtypes = [P, D]
     L.cgli_step.argtypes = [P, ctypes.c_int, D, ctypes.c_int, ctypes.POINTER(ctypes.c_int), DP]
     L.cgli_hyperplane.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, P, ctypes.c_long, P, ctypes.c_long]
+    L.cgli_profile_stages.argtypes = [P, ctypes.c_int, DP]
+    L.cgli_event_record.argtypes = [P, ctypes.c_int]
+    L.cgli_event_elapsed.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
     L.cgli_channel_metrics_host.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, D, D, D, ctypes.c_char_p, P]
     _lib = L
     return L
@@ -215,6 +218,23 @@ class Solver:
         er = (ctypes.c_double * 5)()
         self._rc(self.L.cgli_inner_iteration(self.h, er))
         return np.array(er[:])
+
+    def event(self, slot: int) -> None:
+        """Records CUDA event `slot` on the context's stream."""
+        self._rc(self.L.cgli_event_record(self.h, slot))
+
+    def elapsed_ms(self, a: int, b: int) -> float:
+        ms = ctypes.c_float()
+        self._rc(self.L.cgli_event_elapsed(self.h, a, b, ctypes.byref(ms)))
+        return ms.value
+
+    STAGES = ["halo_bc", "flux_x", "flux_y", "flux_z", "viscous", "residual", "sweep_forward", "sweep_backward"]
+
+    def profile_stages(self, reps: int = 3) -> dict:
+        """Mean milliseconds per stage of one fast-path inner iteration."""
+        ms = (ctypes.c_double * 8)()
+        self._rc(self.L.cgli_profile_stages(self.h, reps, ms))
+        return dict(zip(self.STAGES, ms[:]))
 
     def bulk_flux(self) -> float:
         q = ctypes.c_double()

@@ -122,6 +122,20 @@ int cgli_set_force(cgli_ctx *ctx, double force);
  * then the time-level shift.  Returns the iteration count and final norms. */
 int cgli_step(cgli_ctx *ctx, int fixed_iters, double drop, int cap, int *iters, double er[5]);
 
+/* Device timing on the context stream: record CUDA event `slot` (0..7) and
+ * read the milliseconds between two recorded slots (synchronises on b). */
+int cgli_event_record(cgli_ctx *ctx, int slot);
+int cgli_event_elapsed(cgli_ctx *ctx, int a, int b, float *ms);
+
+/* Stage timing of one inner iteration of the fast path, each stage launched
+ * on its own between CUDA events on the context stream, `reps` times; writes
+ * the mean milliseconds of CGLI_NSTAGES stages to ms[] in the order
+ * halo+boundaries, x flux, y flux, z flux, viscous terms, residual assembly,
+ * forward sweep pass, backward sweep pass (the last one with the update).
+ * Leaves the state advanced by `reps` inner iterations. */
+#define CGLI_NSTAGES 8
+int cgli_profile_stages(cgli_ctx *ctx, int reps, double *ms);
+
 /* Hyperplane.cpp:18-80: cells of the interior slab listed by plane
  * m = i+j+k (m = 7 .. Nx+Ny+Nz+4), then i, j, k; Nijk[2*m] = running end
  * index, Nijk[2*m+1] = count; ijk[3*n..3*n+2] for n = 1..Nx*Ny*Nz.  Host
