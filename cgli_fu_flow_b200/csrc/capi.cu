@@ -37,6 +37,10 @@ const char *kMetricNames[9] = {"xidx", "xidy", "xidz", "etdx", "etdy", "etdz", "
 
 }  // namespace
 
+namespace cgli {
+void set_last_error(const std::string &msg) { g_err = msg; }
+}  // namespace cgli
+
 struct cgli_ctx {
   cgli_params p;
   cgli::Dev d;

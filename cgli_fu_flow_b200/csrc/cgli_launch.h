@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <string>
 #include <vector>
 
 #include "cgli_dev.cuh"
@@ -77,6 +78,9 @@ void launch_end_step(const Dev &d, cudaStream_t s);
 
 // one complete inner iteration on the fast path (halo, boundaries, residual,
 // sweeps, update, partial norms); capturable into a CUDA graph
+// message returned by cgli_last_error() on this thread
+void set_last_error(const std::string &msg);
+
 void launch_fused_iteration(const Dev &d, const SweepArgs &a, cudaStream_t s, int precision);
 
 }  // namespace cgli

@@ -136,6 +136,31 @@ int cgli_event_elapsed(cgli_ctx *ctx, int a, int b, float *ms);
 #define CGLI_NSTAGES 8
 int cgli_profile_stages(cgli_ctx *ctx, int reps, double *ms);
 
+/* No counterpart in the reference.  The primitive update and the five
+ * residual norms of one inner iteration (the arithmetic of
+ * Dual_time_stepping.cpp:1702-1782 and of the context path) on caller-owned
+ * device arrays, for callers that cannot allocate device memory when they
+ * need this step: a host code whose memory pool owns every device buffer, a
+ * time loop that must not pay the synchronisation an allocation can imply,
+ * or a process that has committed the whole GPU to its own arrays.  Nothing
+ * is allocated: the per-row partial sums live in one static device array of
+ * CGLI_NOALLOC_MAX_ROWS x 5 doubles (5 MiB, held by every GPU that loads the
+ * library until the process exits).
+ *   U_[5]  Q^(n+1,m)/J, updated in place; J; NR[5] the final sweep increments,
+ *          all device pointers in the reference layout of an Nx x Ny x Nz slab;
+ *   er[5]  host output, sqrt(sum of squared increments) / (Nx Ny Nz) for
+ *          rho, u, v, w, p/rho; stream: a cudaStream_t or NULL.
+ * Rejects Nx*Ny > CGLI_NOALLOC_MAX_ROWS with CGLI_EINVAL.  The first call on a
+ * device (with that device current) looks up the array's device address once;
+ * make that first call before any stream capture.  All calls share the array
+ * and it keeps the last call's contents (each call overwrites the rows it
+ * reads, nothing has to start at zero), so calls that overlap on the GPU --
+ * concurrent streams, host threads, devices sharing the process -- race and
+ * must be serialised by the caller.  Returns after the norms are on the host. */
+#define CGLI_NOALLOC_MAX_ROWS 131072
+int cgli_update_norms_noalloc(int nx, int ny, int nz, double *const U_[5], const double *J,
+                              const double *const NR[5], double er[5], void *stream);
+
 /* Hyperplane.cpp:18-80: cells of the interior slab listed by plane
  * m = i+j+k (m = 7 .. Nx+Ny+Nz+4), then i, j, k; Nijk[2*m] = running end
  * index, Nijk[2*m+1] = count; ijk[3*n..3*n+2] for n = 1..Nx*Ny*Nz.  Host
