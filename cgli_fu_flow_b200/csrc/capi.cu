@@ -58,6 +58,9 @@ struct cgli_ctx {
   cudaGraphExec_t iter_graph = nullptr;
   cudaGraphExec_t dts_graph = nullptr;
   cudaEvent_t events[8] = {};
+  double Emax[5] = {0, 0, 0, 0, 0};   // running maximum of the norms over the run
+  int history = 0;                    // completed steps since the state was set
+  int predictor = 0;                  // 0 previous level, 1 extrapolation, 2 learned
 };
 
 namespace {
@@ -89,6 +92,7 @@ double *lookup(cgli_ctx *c, const char *name, bool *is_metric = nullptr) {
     snprintf(buf, sizeof buf, "U%d_", v + 1); if (!strcmp(name, buf)) return d.U_[v];
     snprintf(buf, sizeof buf, "U%d", v + 1); if (!strcmp(name, buf)) return d.U[v];
     snprintf(buf, sizeof buf, "U%dq", v + 1); if (!strcmp(name, buf)) return d.Uq[v];
+    snprintf(buf, sizeof buf, "U%dqq", v + 1); if (!strcmp(name, buf)) return d.Uqq[v];
     snprintf(buf, sizeof buf, "MR%d", v + 1); if (!strcmp(name, buf)) return d.MR[v];
     snprintf(buf, sizeof buf, "NR%d", v + 1); if (!strcmp(name, buf)) return d.NR[v];
     snprintf(buf, sizeof buf, "NL%d", v + 1); if (!strcmp(name, buf)) return d.NL[v];
@@ -223,7 +227,7 @@ int cgli_create(const cgli_params *p, cgli_ctx **out) {
   int rc = CGLI_OK;
 #define F(x) if (rc == CGLI_OK) rc = field(c, &(x))
   for (int v = 0; v < 5; v++) {
-    F(d.U_[v]); F(d.U[v]); F(d.Uq[v]); F(d.MR[v]); F(d.NL[v]); F(d.NR[v]);
+    F(d.U_[v]); F(d.U[v]); F(d.Uq[v]); F(d.Uqq[v]); F(d.MR[v]); F(d.NL[v]); F(d.NR[v]);
     for (int f = 0; f < 3; f++) F(d.inF[f][v]);
   }
   for (int v = 0; v < 4; v++) {
@@ -385,9 +389,12 @@ int cgli_set_state(cgli_ctx *c, const double *const U_[5], const double *const U
     CUDA_TRY(cudaMemcpyAsync(c->d.U_[v], U_[v], n, cudaMemcpyHostToDevice, c->stream));
     CUDA_TRY(cudaMemcpyAsync(c->d.U[v], U[v], n, cudaMemcpyHostToDevice, c->stream));
     CUDA_TRY(cudaMemcpyAsync(c->d.Uq[v], Uq[v], n, cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(c->d.Uqq[v], Uq[v], n, cudaMemcpyHostToDevice, c->stream));
   }
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   c->have_state = true;
+  c->history = 0;
+  for (double &e : c->Emax) e = 0;
   return CGLI_OK;
 }
 
@@ -480,28 +487,43 @@ int cgli_set_force(cgli_ctx *c, double force) {
   return CGLI_OK;
 }
 
+int cgli_set_predictor(cgli_ctx *c, int mode) {
+  int rc = check(c); if (rc) return rc;
+  if (mode < 0 || mode > 1) return fail(CGLI_EINVAL, "predictor mode must be 0 (previous level) or 1 (extrapolation)");
+  c->predictor = mode;
+  return CGLI_OK;
+}
+
 int cgli_step(cgli_ctx *c, int fixed_iters, double drop, int cap, int *iters, double er[5]) {
   int rc = check(c); if (rc) return rc;
+  rc = need_ready(c); if (rc) return rc;
   if (!iters || !er) return fail(CGLI_EINVAL, "null argument");
   if (fixed_iters <= 0 && (cap <= 0 || !(drop > 0))) return fail(CGLI_EINVAL, "need fixed_iters > 0 or cap > 0 and drop > 0");
-  double first[5] = {1, 1, 1, 1, 1};
+  if (c->predictor >= 1 && c->history >= 1) {
+    cgli::launch_predict(c->d, c->stream, c->history >= 2 ? 2 : 1);
+    rc = last_launch("predict"); if (rc) return rc;
+  }
   int it = 0;
   while (true) {
     it++;
     rc = cgli_inner_iteration(c, er);
     if (rc) return rc;
-    if (it == 1)
-      for (int v = 0; v < 5; v++) first[v] = er[v] > 0 ? er[v] : 1.0;
+    // main.cpp:287-304: norms divided by their running maximum over the run
+    bool done = true;
+    for (int v = 0; v < 5; v++) {
+      c->Emax[v] = std::max(c->Emax[v], er[v]);
+      done = done && (c->Emax[v] > 0 ? er[v] / c->Emax[v] < drop : true);
+    }
     if (fixed_iters > 0) {
       if (it >= fixed_iters) break;
-    } else {
-      bool done = true;
-      for (int v = 0; v < 5; v++) done = done && (er[v] / first[v] < drop);
-      if (done || it >= cap) break;
+    } else if (done || it >= cap) {
+      break;
     }
   }
   *iters = it;
-  return cgli_end_step(c);
+  rc = cgli_end_step(c);
+  if (rc == CGLI_OK) c->history++;
+  return rc;
 }
 
 int cgli_channel_metrics_host(int nx, int ny, int nz, double det, double high, double stretch,

@@ -23,6 +23,7 @@ struct Dev {
   long long di, dj;       // strides of i and j (k stride is 1)
   double dxi, det, dzt, dt, e, mu, pr, twl, twh;
   double *U_[5], *U[5], *Uq[5];
+  double *Uqq[5];         // Q^(n-2)/J for the extrapolated initial guess
   double *J, *m[9];
   double *Jf[3], *mf[3][9];
   double *inF[3][5], *vF[4];

@@ -75,6 +75,8 @@ void launch_norms(const Dev &d, cudaStream_t s, int nblocks, double scale, doubl
 void launch_bulk_flux(const Dev &d, cudaStream_t s, double *out);
 // time-level shift over planes 2..ie+1 (main.cpp:364-386)
 void launch_end_step(const Dev &d, cudaStream_t s);
+// extrapolated initial guess of a step (order 1 or 2) on the interior cells
+void launch_predict(const Dev &d, cudaStream_t s, int order);
 
 // one complete inner iteration on the fast path (halo, boundaries, residual,
 // sweeps, update, partial norms); capturable into a CUDA graph

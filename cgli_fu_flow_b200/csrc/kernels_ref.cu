@@ -488,15 +488,35 @@ __global__ void k_bulk_flux(Dev d, double *out) {
   if (threadIdx.x == 0) out[0] = tot[0] / d.nx / d.nz;
 }
 
-// main.cpp:364-386 over planes 2..ie+1, all rows
+// main.cpp:364-386 over planes 2..ie+1, all rows; Q^(n-2) is kept as well
 __global__ void k_end_step(Dev d) {
   long long n = (long long)(d.nx + 2) * d.di;
   long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= n) return;
   int v = blockIdx.y;
   long long c = 2 * d.di + t;
+  d.Uqq[v][c] = d.Uq[v][c];
   d.Uq[v][c] = d.U[v][c];
   d.U[v][c] = d.U_[v][c];
+}
+
+// initial guess of the inner iteration on the interior cells: order 1 gives
+// 2Q^n - Q^(n-1), order 2 gives 3Q^n - 3Q^(n-1) + Q^(n-2) (of Q/J; the grid
+// is fixed in time, so extrapolating Q/J is extrapolating Q)
+__global__ void k_predict(Dev d, int order) {
+  int k = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  int j = 2 + blockIdx.y;
+  int i = 3 + blockIdx.z;
+  if (k > d.nz + 1) return;
+  long long c = ix(d, i, j, k);
+  for (int v = 0; v < 5; v++) {
+    double q = d.U[v][c], q1 = d.Uq[v][c];
+    d.U_[v][c] = order >= 2 ? 3 * q - 3 * q1 + d.Uqq[v][c] : 2 * q - q1;
+  }
+}
+
+void launch_predict(const Dev &d, cudaStream_t s, int order) {
+  k_predict<<<dim3((d.nz + 63) / 64, d.ny, d.nx), 64, 0, s>>>(d, order);
 }
 
 void launch_norms(const Dev &d, cudaStream_t s, int nblocks, double scale, double *out) {

@@ -116,11 +116,18 @@ int cgli_end_step(cgli_ctx *ctx);
 /* uniform driving force used by the next residual assembly */
 int cgli_set_force(cgli_ctx *ctx, double force);
 
-/* One physical step (main.cpp:157-386): inner iterations until every one of
- * the five norms has dropped by `drop` relative to the step's first
- * iteration or `cap` iterations ran (fixed_iters > 0 runs exactly that many),
- * then the time-level shift.  Returns the iteration count and final norms. */
+/* One physical step (main.cpp:157-386): the initial guess of the chosen
+ * predictor, inner iterations until every one of the five norms divided by
+ * its running maximum over the run (main.cpp:287-297, reset by
+ * cgli_set_state) is below `drop`, or `cap` iterations ran (fixed_iters > 0
+ * runs exactly that many), then the time-level shift (Q^(n-2) is kept too).
+ * Returns the iteration count and the final norms. */
 int cgli_step(cgli_ctx *ctx, int fixed_iters, double drop, int cap, int *iters, double er[5]);
+/* Initial guess of each step's inner iteration.  0: Q^(n+1,0) = Q^n, as
+ * main.cpp:364-386 leaves it; 1: second-order extrapolation
+ * 3Q^n - 3Q^(n-1) + Q^(n-2) (2Q^n - Q^(n-1) for the first step after
+ * cgli_set_state has one level of history). */
+int cgli_set_predictor(cgli_ctx *ctx, int mode);
 
 /* Device timing on the context stream: record CUDA event `slot` (0..7) and
  * read the milliseconds between two recorded slots (synchronises on b). */

@@ -124,18 +124,38 @@ class Oracle:
             self.force = self.C.force_update(self.ctrl, qb, self.ch)
             self.L.or_set_force(self.s, self.force)
 
-    def step(self, fixed_iters: int | None = 10, drop: float = 1e-3, cap: int = 30):
-        first = None
+    def predict(self) -> None:
+        """Second-order extrapolated initial guess on the interior cells,
+        3Q^n - 3Q^(n-1) + Q^(n-2) (2Q^n - Q^(n-1) with one level of history),
+        with Q^(n-2) kept on the Python side."""
+        ch = self.ch
+        sl = np.s_[3:ch.nx + 3, 2:ch.ny + 2, 2:ch.nz + 2]
+        hist = getattr(self, "history", 0)
+        for v in range(1, 6):
+            u_, u, uq = self.array(f"U{v}_"), self.array(f"U{v}"), self.array(f"U{v}q")
+            if hist >= 2:
+                u_[sl] = 3 * u[sl] - 3 * uq[sl] + self.uqq[v - 1][sl]
+            elif hist == 1:
+                u_[sl] = 2 * u[sl] - uq[sl]
+
+    def step(self, fixed_iters: int | None = 10, drop: float = 1e-3, cap: int = 30, predictor: int = 0):
+        if predictor:
+            self.predict()
+        # main.cpp:287-304: norms over their running maximum over the run
+        if not hasattr(self, "Emax"):
+            self.Emax = np.zeros(5)
         it = 0
         while True:
             it += 1
             er = self.inner_iteration()
-            if first is None:
-                first = np.where(er > 0, er, 1.0)
+            self.Emax = np.maximum(self.Emax, er)
+            rel = np.where(self.Emax > 0, er / np.where(self.Emax > 0, self.Emax, 1.0), 0.0)
             if fixed_iters is not None:
                 if it >= fixed_iters:
                     break
-            elif np.all(er / first < drop) or it >= cap:
+            elif np.all(rel < drop) or it >= cap:
                 break
+        self.uqq = [self.array(f"U{v}q").copy() for v in range(1, 6)]
         self.end_step()
+        self.history = getattr(self, "history", 0) + 1
         return it, er

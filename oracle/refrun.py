@@ -86,16 +86,17 @@ class RefSolver:
 
     def step(self, fixed_iters: int | None = 10, drop: float = 1e-3, cap: int = 30) -> tuple[int, np.ndarray]:
         """One physical step.  fixed_iters=N runs exactly N inner iterations;
-        fixed_iters=None iterates until every one of the five update norms has
-        dropped by `drop` relative to the step's first iteration, or `cap`."""
-        first = None
+        fixed_iters=None iterates until every one of the five update norms,
+        divided by its running maximum over the run, is below `drop`, or `cap`."""
+        # main.cpp:287-304: norms over their running maximum over the run
+        if not hasattr(self, "Emax"):
+            self.Emax = np.zeros(5)
         it = 0
         while True:
             it += 1
             er = self.inner_iteration()
-            if first is None:
-                first = np.where(er > 0, er, 1.0)
-            rel = er / first
+            self.Emax = np.maximum(self.Emax, er)
+            rel = np.where(self.Emax > 0, er / np.where(self.Emax > 0, self.Emax, 1.0), 0.0)
             if fixed_iters is not None:
                 if it >= fixed_iters:
                     break

@@ -174,3 +174,19 @@ def test_c1_twenty_steps_match_reference_build(lib):
     errs = [rel_l2(qg[v], qr[v]) for v in range(5)]
     print("C1 20-step relative L2 per variable:", errs)
     assert max(errs) <= STEP_TOL
+
+
+def test_extrapolated_predictor_matches_oracle(lib):
+    """Second-order extrapolated initial guess: same states as the oracle
+    with the same predictor."""
+    ch = Channel(10, 12, 8)
+    g, o = pair(ch)
+    g.set_predictor(1)
+    for _ in range(4):
+        g.step(8)
+        o.step(8, predictor=1)
+    reg = regions(ch)
+    sl = (slice(None),) + reg["cell"]
+    qg, qo = g.q()[sl], o.q()[sl]
+    for v in range(5):
+        assert rel_l2(qg[v], qo[v]) <= STEP_TOL, v
