@@ -126,6 +126,22 @@ class Channel:
         eta = (j - 1.5) * self.det
         return (0.5 * self.high) * (1 - 1. / math.tanh(g) * np.tanh(g * (1 - 2 * eta)))
 
+    def y_point(self) -> np.ndarray:
+        """Cell-centre y in the reference layout [X_np][Y_m][Z_m], the input
+        of the filter's y pass: interior rows from cell_y(), wall ghost rows
+        mirrored as Grid.cpp:86-90 writes them (j=1: -y(2); j=nyy:
+        y(ny) + 2 y(2)) and z ghosts copied as Grid.cpp:104-111, on every
+        x plane of the slab (Grid.cpp:82-83)."""
+        X, Y, Z = self.shape
+        ny, nz = self.ny + 1, self.nz + 1
+        yp = np.zeros((X, Y, Z))
+        yp[:, 2:ny + 1, 2:nz + 1] = self.cell_y()[None, :, None]
+        yp[:, 1, 2:nz + 1] = -yp[:, 2, 2:nz + 1]
+        yp[:, ny + 1, 2:nz + 1] = yp[:, ny, 2:nz + 1] + 2 * yp[:, 2, 2:nz + 1]
+        yp[:, 1:ny + 2, 1] = yp[:, 1:ny + 2, 2]
+        yp[:, 1:ny + 2, nz + 1] = yp[:, 1:ny + 2, nz]
+        return yp
+
     def initial_primitives(self) -> tuple[np.ndarray, ...]:
         """rho, u, v, w, p on the interior cells, shape (Nx, Ny, Nz)."""
         nx, ny, nz = self.nx, self.ny, self.nz

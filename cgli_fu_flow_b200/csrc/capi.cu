@@ -11,6 +11,7 @@
 
 #include "../../include/cgli_fu_flow.h"
 #include "cgli_dev.cuh"
+#include "cgli_filter.h"
 #include "cgli_launch.h"
 
 #include "host_setup.h"
@@ -61,6 +62,8 @@ struct cgli_ctx {
   double Emax[5] = {0, 0, 0, 0, 0};   // running maximum of the norms over the run
   int history = 0;                    // completed steps since the state was set
   int predictor = 0;                  // 0 previous level, 1 extrapolation, 2 learned
+  cgli::FilterBufs fb;                // allocated on first use of the filter
+  bool have_filter = false, have_ypoint = false;
 };
 
 namespace {
@@ -80,6 +83,28 @@ int alloc(cgli_ctx *c, size_t bytes, void **out) {
 int field(cgli_ctx *c, double **out) {
   size_t n = (size_t)c->d.X * c->d.Y * c->d.Z;
   return alloc(c, n * sizeof(double), (void **)out);
+}
+
+bool is_filter_name(const char *name) {
+  return !strcmp(name, "Y_point") || !strcmp(name, "EpX") || !strcmp(name, "EpY") || !strcmp(name, "EpZ");
+}
+
+// the filter's 18 fields: Y_point, EpX/Y/Z, two levels and the high-pass
+// sum of 4 variables, E at h and 2h
+int ensure_filter(cgli_ctx *c) {
+  if (c->have_filter) return CGLI_OK;
+  cgli::FilterBufs &b = c->fb;
+  int rc = field(c, &b.yp);
+  for (int f = 0; f < 3 && !rc; f++) rc = field(c, &b.ep[f]);
+  for (int v = 0; v < 4 && !rc; v++) {
+    rc = field(c, &b.lev[0][v]);
+    if (!rc) rc = field(c, &b.lev[1][v]);
+    if (!rc) rc = field(c, &b.acc[v]);
+  }
+  if (!rc) rc = field(c, &b.eh);
+  if (!rc) rc = field(c, &b.e2h);
+  if (!rc) c->have_filter = true;
+  return rc;
 }
 
 // device array of a reference name; *is_metric tells whether it is one of
@@ -102,6 +127,12 @@ double *lookup(cgli_ctx *c, const char *name, bool *is_metric = nullptr) {
   }
   for (int v = 0; v < 4; v++) {
     snprintf(buf, sizeof buf, "vF%d", v + 2); if (!strcmp(name, buf)) return d.vF[v];
+  }
+  if (c->have_filter) {
+    if (!strcmp(name, "Y_point")) return c->fb.yp;
+    if (!strcmp(name, "EpX")) return c->fb.ep[0];
+    if (!strcmp(name, "EpY")) return c->fb.ep[1];
+    if (!strcmp(name, "EpZ")) return c->fb.ep[2];
   }
   if (is_metric) *is_metric = true;
   if (!strcmp(name, "J")) return d.J;
@@ -339,6 +370,7 @@ int cgli_destroy(cgli_ctx *c) {
 int cgli_set_array(cgli_ctx *c, const char *name, const double *host) {
   int rc = check(c); if (rc) return rc;
   if (!name || !host) return fail(CGLI_EINVAL, "null argument");
+  if (is_filter_name(name)) { rc = ensure_filter(c); if (rc) return rc; }
   bool is_metric = false;
   double *dst = lookup(c, name, &is_metric);
   if (!dst) return fail(CGLI_EINVAL, std::string("unknown array ") + name);
@@ -346,12 +378,14 @@ int cgli_set_array(cgli_ctx *c, const char *name, const double *host) {
   CUDA_TRY(cudaMemcpyAsync(dst, host, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   if (is_metric) { c->have_metrics = true; c->metrics_checked = false; c->sw.channel_metrics = 0; drop_graph(c); }
+  if (!strcmp(name, "Y_point")) c->have_ypoint = true;
   return CGLI_OK;
 }
 
 int cgli_get_array(cgli_ctx *c, const char *name, double *host) {
   int rc = check(c); if (rc) return rc;
   if (!name || !host) return fail(CGLI_EINVAL, "null argument");
+  if (is_filter_name(name)) { rc = ensure_filter(c); if (rc) return rc; }
   double *src = lookup(c, name);
   if (!src) return fail(CGLI_EINVAL, std::string("unknown array ") + name);
   size_t n = (size_t)c->d.X * c->d.Y * c->d.Z;
@@ -491,6 +525,16 @@ int cgli_set_predictor(cgli_ctx *c, int mode) {
   int rc = check(c); if (rc) return rc;
   if (mode < 0 || mode > 1) return fail(CGLI_EINVAL, "predictor mode must be 0 (previous level) or 1 (extrapolation)");
   c->predictor = mode;
+  return CGLI_OK;
+}
+
+int cgli_filter(cgli_ctx *c, double roe_criterion, double e_high, double e_low) {
+  int rc = check(c); if (rc) return rc;
+  rc = need_ready(c); if (rc) return rc;
+  if (!c->have_ypoint) return fail(CGLI_ESTATE, "Y_point not set (cgli_set_array(ctx, \"Y_point\", ...))");
+  rc = ensure_filter(c); if (rc) return rc;
+  CUDA_TRY(cgli::launch_filter(c->d, c->fb, roe_criterion, e_high, e_low, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
   return CGLI_OK;
 }
 

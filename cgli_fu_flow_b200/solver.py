@@ -46,7 +46,7 @@ EXPORTS = [
     "cgli_flux_z", "cgli_viscous_terms", "cgli_dual_time_stepping", "cgli_inner_iteration",
     "cgli_driven_force", "cgli_end_step", "cgli_set_force", "cgli_step", "cgli_hyperplane",
     "cgli_channel_metrics_host", "cgli_profile_stages", "cgli_event_record", "cgli_event_elapsed",
-    "cgli_update_norms_noalloc", "cgli_set_predictor",
+    "cgli_update_norms_noalloc", "cgli_set_predictor", "cgli_filter",
 ]
 
 _lib = None
@@ -84,6 +84,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cgli_hyperplane.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, P, ctypes.c_long, P, ctypes.c_long]
     L.cgli_profile_stages.argtypes = [P, ctypes.c_int, DP]
     L.cgli_set_predictor.argtypes = [P, ctypes.c_int]
+    L.cgli_filter.argtypes = [P, D, D, D]
     L.cgli_update_norms_noalloc.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P, DP, P]
     L.cgli_event_record.argtypes = [P, ctypes.c_int]
     L.cgli_event_elapsed.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
@@ -257,6 +258,13 @@ class Solver:
     def set_predictor(self, mode: int) -> None:
         """0: previous time level (reference); 1: second-order extrapolation."""
         self._rc(self.L.cgli_set_predictor(self.h, mode))
+
+    def filter(self, y_point: np.ndarray, roe_criterion: float, e_high: float, e_low: float) -> list[np.ndarray]:
+        """Filter.cpp's sensor on the current U_ (cgli_filter): EpX, EpY, EpZ
+        in the reference layout."""
+        self.set("Y_point", y_point)
+        self._rc(self.L.cgli_filter(self.h, roe_criterion, e_high, e_low))
+        return [self.get(n) for n in ("EpX", "EpY", "EpZ")]
 
     def step(self, fixed_iters: int | None = 10, drop: float = 1e-3, cap: int = 30, update_force: bool = True):
         """One physical step on the device (inner loop in C++), then the

@@ -129,6 +129,19 @@ int cgli_step(cgli_ctx *ctx, int fixed_iters, double drop, int cap, int *iters, 
  * cgli_set_state has one level of history). */
 int cgli_set_predictor(cgli_ctx *ctx, int mode);
 
+/* ---- high-order filter sensor (replaces Filter(myid, Roe_criterion, E_high,
+ * E_low, U1_..U5_, Y_point, EpX, EpY, EpZ, J), Filter.cpp:12-1720, prototype
+ * main.h:948-974).  Reads U_ as stored (ghost planes included, like the
+ * reference: call cgli_halo_x and the boundary conditions first for fresh
+ * ghosts), J and "Y_point" (set with cgli_set_array first, otherwise
+ * CGLI_ESTATE); writes "EpX"/"EpY"/"EpZ" (read them with cgli_get_array)
+ * over the reference's face ranges, E_high where the h / 2h velocity-energy
+ * ratio of the face is >= roe_criterion, else E_low.  The two x-end faces of
+ * EpX read the periodic image of the slab (the reference leaves those planes
+ * of its E arrays unset on an interior rank).  The filter buffers (18 fields)
+ * are allocated on first use. */
+int cgli_filter(cgli_ctx *ctx, double roe_criterion, double e_high, double e_low);
+
 /* Device timing on the context stream: record CUDA event `slot` (0..7) and
  * read the milliseconds between two recorded slots (synchronises on b). */
 int cgli_event_record(cgli_ctx *ctx, int slot);

@@ -84,6 +84,13 @@ class RefSolver:
             self.force = _c().force_update(self.ctrl, qb, self.ch)
             self.lib.ref_set_force(self.force)
 
+    def filter(self, y_point: np.ndarray, roe_criterion: float, e_high: float, e_low: float):
+        """Filter.cpp on the current U_ with the given Y_point; returns copies
+        of EpX, EpY, EpZ."""
+        self.array("Y_point")[...] = y_point
+        self.lib.ref_filter(roe_criterion, e_high, e_low)
+        return [self.array(n).copy() for n in ("EpX", "EpY", "EpZ")]
+
     def step(self, fixed_iters: int | None = 10, drop: float = 1e-3, cap: int = 30) -> tuple[int, np.ndarray]:
         """One physical step.  fixed_iters=N runs exactly N inner iterations;
         fixed_iters=None iterates until every one of the five update norms,

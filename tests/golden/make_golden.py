@@ -10,7 +10,10 @@ first inner iteration and for three physical steps:
 The oracle must reproduce every hash bit for bit; the GPU path is compared
 with the stored state within tolerance.
 
-Usage:  python tests/golden/make_golden.py [nx ny nz]
+It also records the reference's filter sensor (Filter.cpp) on the seeded
+field at five thresholds (filter_<workload>.npz).
+
+Usage:  python tests/golden/make_golden.py [--filter] [nx ny nz]
 """
 from __future__ import annotations
 
@@ -98,6 +101,49 @@ def main(nx=8, ny=12, nz=8):
     print("wrote", base + ".json", base + ".npz")
 
 
+FILTER_QUANTILES = (0.1, 0.3, 0.5, 0.7, 0.9)
+FILTER_E_HIGH, FILTER_E_LOW = 2.0, 1.0
+
+
+def filter_input(ch, U_from):
+    """The filter fixture's input: the seeded initial field after the halo
+    exchange and the wall / periodic boundary conditions, with Y_point from
+    Channel.y_point()."""
+    return [U_from(f"U{v}_") for v in range(1, 6)], ch.y_point()
+
+
+def main_filter(nx=8, ny=12, nz=8):
+    """EpX/EpY/EpZ of the reference's Filter.cpp at five thresholds (the 10..90 %
+    quantiles of the face ratios, so each threshold splits the faces), coded
+    0 = face not in the reference's range (or an x-end face whose E planes
+    the reference leaves unset), 1 = E_low, 2 = E_high."""
+    from oracle import filter_oracle as F
+    ch = Channel(nx, ny, nz)
+    r = RefSolver(ch, threads=1)
+    r.init()
+    r.lib.ref_halo_bc()
+    U, yp = filter_input(ch, lambda n: r.array(n).copy())
+    J = r.array("J").copy()
+    R = F.sensor(U, J, yp, ch.nx, ch.ny, ch.nz, x_ends=None)
+    M = F.face_masks(ch.nx, ch.ny, ch.nz, J.shape, x_ends=None)
+    fin = R[0][M[0] & np.isfinite(R[0])]
+    crits = [float(np.quantile(fin, q)) for q in FILTER_QUANTILES]
+    codes = np.zeros((len(crits), 3) + J.shape, np.uint8)
+    for n, crit in enumerate(crits):
+        ep = r.filter(yp, crit, FILTER_E_HIGH, FILTER_E_LOW)
+        for f in range(3):
+            codes[n, f][M[f] & (ep[f] == FILTER_E_LOW)] = 1
+            codes[n, f][M[f] & (ep[f] == FILTER_E_HIGH)] = 2
+    base = os.path.join(HERE, "filter_" + ch.name)
+    np.savez_compressed(base + ".npz", codes=codes, crits=np.array(crits),
+                        input_sha256=np.array([digest(np.stack(U))]))
+    print("wrote", base + ".npz")
+
+
 if __name__ == "__main__":
-    args = [int(a) for a in sys.argv[1:4]] or [8, 12, 8]
-    main(*args)
+    argv = sys.argv[1:]
+    which = main
+    if argv and argv[0] == "--filter":
+        which, argv = main_filter, argv[1:]
+    args = [int(a) for a in argv[0:3]] or [8, 12, 8]
+    which(*args)
