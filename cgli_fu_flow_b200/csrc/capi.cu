@@ -12,6 +12,7 @@
 #include "../../include/cgli_fu_flow.h"
 #include "cgli_dev.cuh"
 #include "cgli_filter.h"
+#include "cnn.h"
 #include "cgli_launch.h"
 
 #include "host_setup.h"
@@ -62,6 +63,7 @@ struct cgli_ctx {
   double Emax[5] = {0, 0, 0, 0, 0};   // running maximum of the norms over the run
   int history = 0;                    // completed steps since the state was set
   int predictor = 0;                  // 0 previous level, 1 extrapolation, 2 learned
+  cgli_cnn *cnn = nullptr;            // learned initial guess (not owned)
   cgli::FilterBufs fb;                // allocated on first use of the filter
   bool have_filter = false, have_ypoint = false;
 };
@@ -523,7 +525,9 @@ int cgli_set_force(cgli_ctx *c, double force) {
 
 int cgli_set_predictor(cgli_ctx *c, int mode) {
   int rc = check(c); if (rc) return rc;
-  if (mode < 0 || mode > 1) return fail(CGLI_EINVAL, "predictor mode must be 0 (previous level) or 1 (extrapolation)");
+  if (mode < 0 || mode > 2)
+    return fail(CGLI_EINVAL, "predictor mode must be 0 (previous level), 1 (extrapolation) or 2 (learned)");
+  if (mode == 2 && !c->cnn) return fail(CGLI_ESTATE, "predictor 2 needs a network (cgli_set_learned_guess)");
   c->predictor = mode;
   return CGLI_OK;
 }
@@ -538,12 +542,32 @@ int cgli_filter(cgli_ctx *c, double roe_criterion, double e_high, double e_low) 
   return CGLI_OK;
 }
 
+int cgli_set_learned_guess(cgli_ctx *c, cgli_cnn *n) {
+  int rc = check(c); if (rc) return rc;
+  if (n && !cgli::cnn_matches(n, c->p.nx, c->p.ny, c->p.nz))
+    return fail(CGLI_EINVAL, "network grid differs from the context's grid");
+  c->cnn = n;
+  if (!n && c->predictor == 2) c->predictor = 1;
+  return CGLI_OK;
+}
+
+int cgli_cnn_push_level(cgli_cnn *n, cgli_ctx *c) {
+  int rc = check(c); if (rc) return rc;
+  if (!n || !cgli::cnn_matches(n, c->p.nx, c->p.ny, c->p.nz))
+    return fail(CGLI_EINVAL, "network grid differs from the context's grid");
+  if (!c->have_state) return fail(CGLI_ESTATE, "state not set (cgli_set_state)");
+  return cgli::cnn_store_level(n, c->d, c->stream);
+}
+
 int cgli_step(cgli_ctx *c, int fixed_iters, double drop, int cap, int *iters, double er[5]) {
   int rc = check(c); if (rc) return rc;
   rc = need_ready(c); if (rc) return rc;
   if (!iters || !er) return fail(CGLI_EINVAL, "null argument");
   if (fixed_iters <= 0 && (cap <= 0 || !(drop > 0))) return fail(CGLI_EINVAL, "need fixed_iters > 0 or cap > 0 and drop > 0");
-  if (c->predictor >= 1 && c->history >= 1) {
+  if (c->predictor == 2 && c->history >= 2) {
+    CUDA_TRY(cgli::cnn_predict(c->cnn, c->d, c->stream));
+  } else if (c->predictor >= 1 && c->history >= 1) {
+    // extrapolation, also the learned guess's fallback without two levels of history
     cgli::launch_predict(c->d, c->stream, c->history >= 2 ? 2 : 1);
     rc = last_launch("predict"); if (rc) return rc;
   }

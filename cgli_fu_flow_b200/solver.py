@@ -47,6 +47,10 @@ EXPORTS = [
     "cgli_driven_force", "cgli_end_step", "cgli_set_force", "cgli_step", "cgli_hyperplane",
     "cgli_channel_metrics_host", "cgli_profile_stages", "cgli_event_record", "cgli_event_elapsed",
     "cgli_update_norms_noalloc", "cgli_set_predictor", "cgli_filter",
+    "cgli_cnn_param_count", "cgli_cnn_create", "cgli_cnn_destroy", "cgli_cnn_last_error", "cgli_cnn_set_params",
+    "cgli_cnn_get_params", "cgli_cnn_set_scales", "cgli_cnn_forward_host", "cgli_cnn_loss_grad_host",
+    "cgli_cnn_reserve_levels", "cgli_cnn_levels", "cgli_cnn_push_level_host", "cgli_cnn_push_level",
+    "cgli_cnn_pair_loss", "cgli_cnn_train", "cgli_set_learned_guess",
 ]
 
 _lib = None
@@ -85,6 +89,26 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cgli_profile_stages.argtypes = [P, ctypes.c_int, DP]
     L.cgli_set_predictor.argtypes = [P, ctypes.c_int]
     L.cgli_filter.argtypes = [P, D, D, D]
+    F = ctypes.c_float
+    FP = ctypes.POINTER(ctypes.c_float)
+    LL = ctypes.c_longlong
+    L.cgli_cnn_param_count.restype = LL
+    L.cgli_cnn_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(P)]
+    L.cgli_cnn_destroy.argtypes = [P]
+    L.cgli_cnn_last_error.restype = ctypes.c_char_p
+    L.cgli_cnn_set_params.argtypes = [P, P]
+    L.cgli_cnn_get_params.argtypes = [P, P]
+    L.cgli_cnn_set_scales.argtypes = [P, P, P, P]
+    L.cgli_cnn_forward_host.argtypes = [P, P, P]
+    L.cgli_cnn_loss_grad_host.argtypes = [P, P, P, FP, P]
+    L.cgli_cnn_reserve_levels.argtypes = [P, ctypes.c_int]
+    L.cgli_cnn_levels.argtypes = [P]
+    L.cgli_cnn_levels.restype = LL
+    L.cgli_cnn_push_level_host.argtypes = [P, P]
+    L.cgli_cnn_push_level.argtypes = [P, P]
+    L.cgli_cnn_pair_loss.argtypes = [P, LL, FP]
+    L.cgli_cnn_train.argtypes = [P, ctypes.c_int, F, ctypes.c_ulonglong, LL, LL, FP]
+    L.cgli_set_learned_guess.argtypes = [P, P]
     L.cgli_update_norms_noalloc.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P, DP, P]
     L.cgli_event_record.argtypes = [P, ctypes.c_int]
     L.cgli_event_elapsed.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
@@ -256,8 +280,14 @@ class Solver:
             self.set_force(C.force_update(self.ctrl, qb, self.ch))
 
     def set_predictor(self, mode: int) -> None:
-        """0: previous time level (reference); 1: second-order extrapolation."""
+        """0: previous time level (reference); 1: second-order extrapolation;
+        2: extrapolation plus the learned correction (set_learned_guess)."""
         self._rc(self.L.cgli_set_predictor(self.h, mode))
+
+    def set_learned_guess(self, net) -> None:
+        """Attach a cgli_fu_flow_b200.cnn.Network (None detaches)."""
+        self._rc(self.L.cgli_set_learned_guess(self.h, net.h if net is not None else None))
+        self._net = net
 
     def filter(self, y_point: np.ndarray, roe_criterion: float, e_high: float, e_low: float) -> list[np.ndarray]:
         """Filter.cpp's sensor on the current U_ (cgli_filter): EpX, EpY, EpZ

@@ -126,8 +126,48 @@ int cgli_step(cgli_ctx *ctx, int fixed_iters, double drop, int cap, int *iters, 
 /* Initial guess of each step's inner iteration.  0: Q^(n+1,0) = Q^n, as
  * main.cpp:364-386 leaves it; 1: second-order extrapolation
  * 3Q^n - 3Q^(n-1) + Q^(n-2) (2Q^n - Q^(n-1) for the first step after
- * cgli_set_state has one level of history). */
+ * cgli_set_state has one level of history); 2: extrapolation plus the
+ * learned correction of the network given to cgli_set_learned_guess
+ * (extrapolation while fewer than two levels of history exist, and in any
+ * cell where the network's output is not finite). */
 int cgli_set_predictor(cgli_ctx *ctx, int mode);
+
+/* ---- learned initial guess (no counterpart in the reference).  A 3-D
+ * convolutional network, 15 -> 32 -> 32 -> 32 -> 32 -> 5 channels, 3x3x3
+ * kernels, GELU after the first four layers, periodic in x and z, zero
+ * padded at the walls, BF16 weights and activations with FP32 accumulation
+ * on the tensor cores.  Input: Q = U*J of Q^n, Q^(n-1), Q^(n-2), channel
+ * level*5 + v, normalised (Q_v - mean_v) / std_v; output: the correction
+ * (Q^(n+1) - (3Q^n - 3Q^(n-1) + Q^(n-2)))_v / oscale_v.
+ * Parameters: a flat float array, per layer W[27][cout][cin] (tap
+ * t = (dx*3 + dy)*3 + dz for offsets dx-1, dy-1, dz-1) then b[cout].
+ * The grid must have Ny a multiple of 4 and Nz a multiple of 32. */
+typedef struct cgli_cnn cgli_cnn;
+long long cgli_cnn_param_count(void);
+int cgli_cnn_create(int nx, int ny, int nz, cgli_cnn **out);
+int cgli_cnn_destroy(cgli_cnn *cnn);
+const char *cgli_cnn_last_error(void);
+int cgli_cnn_set_params(cgli_cnn *cnn, const float *theta);   /* also resets Adam */
+int cgli_cnn_get_params(cgli_cnn *cnn, float *theta);
+int cgli_cnn_set_scales(cgli_cnn *cnn, const double mean[5], const double std[5], const double oscale[5]);
+/* x0: [15][Nx][Ny][Nz] already normalised; out: [5][Nx][Ny][Nz] */
+int cgli_cnn_forward_host(cgli_cnn *cnn, const float *x0, float *out);
+/* mean squared error against target [5][Nx][Ny][Nz] and its gradient with
+ * respect to the flat parameters (the training step without the update) */
+int cgli_cnn_loss_grad_host(cgli_cnn *cnn, const float *x0, const float *target, float *loss, float *grad);
+/* training data: a ring of `count` stored time levels (physical Q, float) on
+ * the device; pair p = (levels p, p+1, p+2 as history, level p+3 as target) */
+int cgli_cnn_reserve_levels(cgli_cnn *cnn, int count);
+long long cgli_cnn_levels(const cgli_cnn *cnn);
+int cgli_cnn_push_level_host(cgli_cnn *cnn, const float *q);  /* [5][Nx][Ny][Nz] */
+int cgli_cnn_push_level(cgli_cnn *cnn, cgli_ctx *ctx);         /* the context's Q^n (after cgli_step) */
+int cgli_cnn_pair_loss(cgli_cnn *cnn, long long pair, float *loss);
+/* `steps` Adam steps (learning rate lr) on pairs drawn uniformly (seeded)
+ * from [first_pair, first_pair + npairs); mean training loss */
+int cgli_cnn_train(cgli_cnn *cnn, int steps, float lr, unsigned long long seed, long long first_pair,
+                   long long npairs, float *mean_loss);
+/* use the network for predictor mode 2 (null detaches it) */
+int cgli_set_learned_guess(cgli_ctx *ctx, cgli_cnn *cnn);
 
 /* ---- high-order filter sensor (replaces Filter(myid, Roe_criterion, E_high,
  * E_low, U1_..U5_, Y_point, EpX, EpY, EpZ, J), Filter.cpp:12-1720, prototype
