@@ -64,6 +64,7 @@ struct cgli_ctx {
   int history = 0;                    // completed steps since the state was set
   int predictor = 0;                  // 0 previous level, 1 extrapolation, 2 learned
   cgli_cnn *cnn = nullptr;            // learned initial guess (not owned)
+  std::vector<double> step_norms;     // the five norms of every inner iteration of the last step
   cgli::FilterBufs fb;                // allocated on first use of the filter
   bool have_filter = false, have_ypoint = false;
 };
@@ -542,6 +543,15 @@ int cgli_filter(cgli_ctx *c, double roe_criterion, double e_high, double e_low) 
   return CGLI_OK;
 }
 
+int cgli_step_norms(cgli_ctx *c, double *norms, int max_iters, int *iters) {
+  int rc = check(c); if (rc) return rc;
+  if (!norms || !iters || max_iters < 0) return fail(CGLI_EINVAL, "null argument");
+  const int n = (int)(c->step_norms.size() / 5);
+  *iters = n;
+  std::copy(c->step_norms.begin(), c->step_norms.begin() + 5 * std::min(n, max_iters), norms);
+  return CGLI_OK;
+}
+
 int cgli_set_learned_guess(cgli_ctx *c, cgli_cnn *n) {
   int rc = check(c); if (rc) return rc;
   if (n && !cgli::cnn_matches(n, c->p.nx, c->p.ny, c->p.nz))
@@ -572,10 +582,12 @@ int cgli_step(cgli_ctx *c, int fixed_iters, double drop, int cap, int *iters, do
     rc = last_launch("predict"); if (rc) return rc;
   }
   int it = 0;
+  c->step_norms.clear();
   while (true) {
     it++;
     rc = cgli_inner_iteration(c, er);
     if (rc) return rc;
+    c->step_norms.insert(c->step_norms.end(), er, er + 5);
     // main.cpp:287-304: norms divided by their running maximum over the run
     bool done = true;
     for (int v = 0; v < 5; v++) {

@@ -68,6 +68,52 @@ __device__ __forceinline__ double m2(const double *u, const double *J, long long
   return t * (u[a] + u[b]);
 }
 
+// One side of a face for all five variables: the weight
+// t = 1 / sum(c_p / J_p) is computed once and applied to each variable's
+// sum(c_p u_p) (the reference's m5L/m5R/m3L/m3R/m2 expressions, same
+// evaluation order).
+template <int N>
+__device__ __forceinline__ void muscl_side(const Dev &d, const long long (&o)[N], const double (&c)[N], double out[5]) {
+  double s = c[0] / d.J[o[0]];
+#pragma unroll
+  for (int p = 1; p < N; p++) s += c[p] / d.J[o[p]];
+  const double t = 1. / s;
+#pragma unroll
+  for (int v = 0; v < 5; v++) {
+    const double *u = d.U_[v];
+    double a = c[0] * u[o[0]];
+#pragma unroll
+    for (int p = 1; p < N; p++) a += c[p] * u[o[p]];
+    out[v] = t * a;
+  }
+}
+// stencil kinds: 5L, 5R on (a..e); 3L, 3R on (a, b, c); 2 on (a, b)
+__device__ __forceinline__ void side5L(const Dev &d, long long a, long long st, double out[5]) {
+  const long long o[5] = {a, a + st, a + 2 * st, a + 3 * st, a + 4 * st};
+  const double c[5] = {2, -13, 47, 27, -3};
+  muscl_side<5>(d, o, c, out);
+}
+__device__ __forceinline__ void side5R(const Dev &d, long long a, long long st, double out[5]) {
+  const long long o[5] = {a, a + st, a + 2 * st, a + 3 * st, a + 4 * st};
+  const double c[5] = {-3, 27, 47, -13, 2};
+  muscl_side<5>(d, o, c, out);
+}
+__device__ __forceinline__ void side3L(const Dev &d, long long a, long long st, double out[5]) {
+  const long long o[3] = {a, a + st, a + 2 * st};
+  const double c[3] = {-1, 5, 2};
+  muscl_side<3>(d, o, c, out);
+}
+__device__ __forceinline__ void side3R(const Dev &d, long long a, long long st, double out[5]) {
+  const long long o[3] = {a, a + st, a + 2 * st};
+  const double c[3] = {2, 5, -1};
+  muscl_side<3>(d, o, c, out);
+}
+__device__ __forceinline__ void side2(const Dev &d, long long a, long long b, double out[5]) {
+  const long long o[2] = {a, b};
+  const double c[2] = {1, 1};
+  muscl_side<2>(d, o, c, out);
+}
+
 // ------------------------------------------------------------- Roe flux
 // Preconditioned Roe flux through one face, Flux_X.cpp:229-350 (same
 // statements in Flux_Y.cpp:291-396 and Flux_Z.cpp:250-354; the pressure-jump
@@ -77,58 +123,69 @@ __device__ __forceinline__ double m2(const double *u, const double *J, long long
 __device__ __forceinline__ void roe_face(const double L[5], const double R[5], double mx, double my,
                                          double mz, double Jf, double e, double F[5], double &Fav3o,
                                          double &ppo) {
-  double insqr = 1.0 / sqrt(mx * mx + my * my + mz * mz);
-  double NX = mx * insqr, NY = my * insqr, NZ = mz * insqr;
-  double _rho = L[0], _u = L[1] / _rho, _v = L[2] / _rho, _w = L[3] / _rho;
-  double iU = mx * _u + my * _v + mz * _w;
-  double _VV = _u * _u + _v * _v + _w * _w;
-  double iP = (L[4] - 0.5 * _rho * _VV) * (KG - 1);
-  double iC = KG * iP / _rho;
-  double _H = 0.5 * _VV + iC / (KG - 1);
-  double rho_ = R[0], u_ = R[1] / rho_, v_ = R[2] / rho_, w_ = R[3] / rho_;
-  double U_ = mx * u_ + my * v_ + mz * w_;
-  double VV_ = u_ * u_ + v_ * v_ + w_ * w_;
-  double P_ = (R[4] - 0.5 * rho_ * VV_) * (KG - 1);
-  double C_ = KG * P_ / rho_;
-  double H_ = 0.5 * VV_ + C_ / (KG - 1);
-  double temp5 = sqrt(_rho), temp6 = sqrt(rho_);
-  double temp4 = temp5 + temp6;
-  double rho = sqrt(_rho * rho_);
-  double u = (temp5 * _u + temp6 * u_) / temp4;
-  double v = (temp5 * _v + temp6 * v_) / temp4;
-  double w = (temp5 * _w + temp6 * w_) / temp4;
-  double U = (temp5 * iU + temp6 * U_) / temp4;
-  double VV = u * u + v * v + w * w;
-  double H = (temp5 * _H + temp6 * H_) / temp4;
-  double C = (H - 0.5 * VV) * (KG - 1);
-  double dU1 = rho_ - _rho;
-  double dU2 = rho_ * u_ - _rho * _u;
-  double dU3 = rho_ * v_ - _rho * _v;
-  double dU4 = rho_ * w_ - _rho * _w;
-  double dU5 = (P_ / (KG - 1) + 0.5 * rho_ * VV_) - (iP / (KG - 1) + 0.5 * _rho * _VV);
-  double beta = VV / C > e ? VV / C : e;   // max() macro semantics
-  double temp = 0.5 * (1 + beta) * U * insqr;
-  double S = 0.5 * sqrt(4 * beta * C + U * insqr * U * insqr * (1 - beta) * (1 - beta));
-  double theda_p = VV / C;
-  double U_p = 0.5 * (1 + theda_p) * U * insqr;
-  double C_p = 0.5 * sqrt(4 * C * theda_p + U * insqr * U * insqr * (1 - theda_p) * (1 - theda_p));
-  double temp1 = (P_ - iP) / rho / beta / C;
-  double temp2 = U_p / S * (U_ - iU) * insqr;
-  double temp3 = 0.5 * (1 - beta) * U * insqr * temp / S;
-  temp4 = 0.5 * (1 - theda_p) * U * insqr * U_p / S;
-  double deltaU = (S - temp3 - beta * fabs(U) * insqr) * temp1 + temp2;
-  double deltaP = U_p / S * (P_ - iP) + (C_p - fabs(U) * insqr + temp4) * rho * (U_ - iU) * insqr;
-  double aU = fabs(U * insqr);
-  double Fav1 = aU * dU1 + deltaU * rho;
-  double Fav2 = aU * dU2 + deltaU * rho * u + deltaP * NX;
-  double Fav3 = aU * dU3 + deltaU * rho * v + deltaP * NY;
-  double Fav4 = aU * dU4 + deltaU * rho * w + deltaP * NZ;
-  double Fav5 = aU * dU5 + deltaU * rho * H + deltaP * U * insqr;
-  F[0] = 0.5 * ((_rho * iU + rho_ * U_) - Fav1 / insqr) / Jf;
-  F[1] = 0.5 * ((_rho * _u * iU + rho_ * u_ * U_ + mx * (iP + P_)) - Fav2 / insqr) / Jf;
-  F[2] = 0.5 * ((_rho * _v * iU + rho_ * v_ * U_ + my * (iP + P_)) - Fav3 / insqr) / Jf;
-  F[3] = 0.5 * ((_rho * _w * iU + rho_ * w_ * U_ + mz * (iP + P_)) - Fav4 / insqr) / Jf;
-  F[4] = 0.5 * ((iU * (3.5 * iP + 0.5 * _rho * _VV) + U_ * (3.5 * P_ + 0.5 * rho_ * VV_)) - Fav5 / insqr) / Jf;
+  // The reference's statements in its order; each group of divisions by one
+  // denominator is one reciprocal and products (results differ from the
+  // reference's in the last bits only).
+  const double sq = sqrt(mx * mx + my * my + mz * mz);
+  const double insqr = 1.0 / sq;
+  const double NX = mx * insqr, NY = my * insqr, NZ = mz * insqr;
+  const double _rho = L[0], irl = 1.0 / _rho;
+  const double _u = L[1] * irl, _v = L[2] * irl, _w = L[3] * irl;
+  const double iU = mx * _u + my * _v + mz * _w;
+  const double _VV = _u * _u + _v * _v + _w * _w;
+  const double iP = (L[4] - 0.5 * _rho * _VV) * (KG - 1);
+  const double iC = KG * iP * irl;
+  const double _H = 0.5 * _VV + iC / (KG - 1);
+  const double rho_ = R[0], irr = 1.0 / rho_;
+  const double u_ = R[1] * irr, v_ = R[2] * irr, w_ = R[3] * irr;
+  const double U_ = mx * u_ + my * v_ + mz * w_;
+  const double VV_ = u_ * u_ + v_ * v_ + w_ * w_;
+  const double P_ = (R[4] - 0.5 * rho_ * VV_) * (KG - 1);
+  const double C_ = KG * P_ * irr;
+  const double H_ = 0.5 * VV_ + C_ / (KG - 1);
+  const double temp5 = sqrt(_rho), temp6 = sqrt(rho_);
+  const double i4 = 1.0 / (temp5 + temp6);
+  const double rho = sqrt(_rho * rho_);
+  const double u = (temp5 * _u + temp6 * u_) * i4;
+  const double v = (temp5 * _v + temp6 * v_) * i4;
+  const double w = (temp5 * _w + temp6 * w_) * i4;
+  const double U = (temp5 * iU + temp6 * U_) * i4;
+  const double VV = u * u + v * v + w * w;
+  const double H = (temp5 * _H + temp6 * H_) * i4;
+  const double C = (H - 0.5 * VV) * (KG - 1);
+  const double iCc = 1.0 / C;
+  const double dU1 = rho_ - _rho;
+  const double dU2 = rho_ * u_ - _rho * _u;
+  const double dU3 = rho_ * v_ - _rho * _v;
+  const double dU4 = rho_ * w_ - _rho * _w;
+  const double dU5 = (P_ / (KG - 1) + 0.5 * rho_ * VV_) - (iP / (KG - 1) + 0.5 * _rho * _VV);
+  const double theda_p = VV * iCc;
+  const double beta = theda_p > e ? theda_p : e;   // max() macro semantics
+  const double Un = U * insqr;
+  const double temp = 0.5 * (1 + beta) * Un;
+  const double S = 0.5 * sqrt(4 * beta * C + Un * Un * (1 - beta) * (1 - beta));
+  const double iS = 1.0 / S;
+  const double U_p = 0.5 * (1 + theda_p) * Un;
+  const double C_p = 0.5 * sqrt(4 * C * theda_p + Un * Un * (1 - theda_p) * (1 - theda_p));
+  const double dP = P_ - iP, dUn = (U_ - iU) * insqr;
+  const double temp1 = dP * iCc / (rho * beta);
+  const double temp2 = U_p * iS * dUn;
+  const double temp3 = 0.5 * (1 - beta) * Un * temp * iS;
+  const double temp4 = 0.5 * (1 - theda_p) * Un * U_p * iS;
+  const double deltaU = (S - temp3 - beta * fabs(U) * insqr) * temp1 + temp2;
+  const double deltaP = U_p * iS * dP + (C_p - fabs(U) * insqr + temp4) * rho * dUn;
+  const double aU = fabs(Un);
+  const double Fav1 = aU * dU1 + deltaU * rho;
+  const double Fav2 = aU * dU2 + deltaU * rho * u + deltaP * NX;
+  const double Fav3 = aU * dU3 + deltaU * rho * v + deltaP * NY;
+  const double Fav4 = aU * dU4 + deltaU * rho * w + deltaP * NZ;
+  const double Fav5 = aU * dU5 + deltaU * rho * H + deltaP * Un;
+  const double h = 0.5 / Jf;
+  F[0] = ((_rho * iU + rho_ * U_) - Fav1 * sq) * h;
+  F[1] = ((_rho * _u * iU + rho_ * u_ * U_ + mx * (iP + P_)) - Fav2 * sq) * h;
+  F[2] = ((_rho * _v * iU + rho_ * v_ * U_ + my * (iP + P_)) - Fav3 * sq) * h;
+  F[3] = ((_rho * _w * iU + rho_ * w_ * U_ + mz * (iP + P_)) - Fav4 * sq) * h;
+  F[4] = ((iU * (3.5 * iP + 0.5 * _rho * _VV) + U_ * (3.5 * P_ + 0.5 * rho_ * VV_)) - Fav5 * sq) * h;
   Fav3o = Fav3;
   ppo = iP + P_;
 }
@@ -144,16 +201,20 @@ template <typename T>
 __device__ __forceinline__ CPrim<T> cprim(T q1, T q2, T q3, T q4, T q5, T J, T e) {
   CPrim<T> r;
   const T K = (T)KG;
+  // divisions by one denominator as one reciprocal and products
+  const T iq1 = (T)1 / q1;
   r.rho = q1 * J;
-  r.u = q2 / q1;
-  r.v = q3 / q1;
-  r.w = q4 / q1;
+  r.u = q2 * iq1;
+  r.v = q3 * iq1;
+  r.w = q4 * iq1;
   r.VV = r.u * r.u + r.v * r.v + r.w * r.w;
   r.P = (q5 * J - (T)0.5 * r.rho * r.VV) * (K - 1);
-  r.C = K * r.P / r.rho;
-  r.Tt = r.P / r.rho;
+  const T irho = (T)1 / r.rho;
+  r.C = K * r.P * irho;
+  r.Tt = r.P * irho;
   r.H = (T)0.5 * r.VV + r.C / (K - 1);
-  r.beta = r.VV / r.C > e ? r.VV / r.C : e;
+  const T th = r.VV / r.C;
+  r.beta = th > e ? th : e;
   return r;
 }
 

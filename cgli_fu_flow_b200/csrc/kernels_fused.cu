@@ -45,32 +45,35 @@ __global__ void k_residual_fast(Dev d, SweepArgs a) {
   if (halo_plane) return;
   CPrim<double> q = cprim<double>(d.U_[0][c], d.U_[1][c], d.U_[2][c], d.U_[3][c], d.U_[4][c], J, d.e);
   double rho = q.rho, u = q.u, v = q.v, w = q.w, VV = q.VV, T = q.Tt, H = q.H, beta = q.beta;
-  double temp = rho * KG;
+  // Gamma^-1 of Dual_time_stepping.cpp:771-802; divisions by rho and by
+  // rho*gamma as reciprocals
+  const double irho = 1 / rho, itemp = 1 / (rho * KG);
   double d11 = -(H * (KG - 1) + VV - KG * (T + VV)) * beta;
   double d12 = -(KG - 1) * u * beta, d13 = -(KG - 1) * v * beta, d14 = -(KG - 1) * w * beta;
   double d15 = (KG - 1) * beta;
-  double d21 = -u / rho, d22 = 1 / rho;
-  double d31 = -v / rho;
-  double d41 = -w / rho;
-  double d51 = (KG - 1) * (VV + KG * T * beta + (KG - 1) * VV * beta + H * (-1 + beta - KG * beta)) / temp;
-  double d52 = -(KG - 1) * u * (1 + (KG - 1) * beta) / temp;
-  double d53 = -(KG - 1) * v * (1 + (KG - 1) * beta) / temp;
-  double d54 = -(KG - 1) * w * (1 + (KG - 1) * beta) / temp;
-  double d55 = (KG - 1) * (1 + (KG - 1) * beta) / temp;
+  double d21 = -u * irho, d22 = irho;
+  double d31 = -v * irho;
+  double d41 = -w * irho;
+  double d51 = (KG - 1) * (VV + KG * T * beta + (KG - 1) * VV * beta + H * (-1 + beta - KG * beta)) * itemp;
+  double d52 = -(KG - 1) * u * (1 + (KG - 1) * beta) * itemp;
+  double d53 = -(KG - 1) * v * (1 + (KG - 1) * beta) * itemp;
+  double d54 = -(KG - 1) * w * (1 + (KG - 1) * beta) * itemp;
+  double d55 = (KG - 1) * (1 + (KG - 1) * beta) * itemp;
   long long fx1 = ix(d, i, j - 1, k - 1), fx0 = ix(d, i - 1, j - 1, k - 1);
   long long fy1 = ix(d, i - 1, j, k - 1), fz1 = ix(d, i - 1, j - 1, k);
   double Rk[5];
   double f = d.scal[0];
+  const double i2dt = 1 / (2 * deltaT), idx = 1 / d.dxi, idy = 1 / d.det, idz = 1 / d.dzt, iJ = 1 / J;
   for (int n = 0; n < 5; n++) {
-    double Rp = -(3 * d.U_[n][c] - 4 * d.U[n][c] + d.Uq[n][c]) / (2 * deltaT);
-    double Rf = -((d.inF[0][n][fx1] - d.inF[0][n][fx0]) / d.dxi + (d.inF[1][n][fy1] - d.inF[1][n][fx0]) / d.det +
-                  (d.inF[2][n][fz1] - d.inF[2][n][fx0]) / d.dzt);
+    double Rp = -(3 * d.U_[n][c] - 4 * d.U[n][c] + d.Uq[n][c]) * i2dt;
+    double Rf = -((d.inF[0][n][fx1] - d.inF[0][n][fx0]) * idx + (d.inF[1][n][fy1] - d.inF[1][n][fx0]) * idy +
+                  (d.inF[2][n][fz1] - d.inF[2][n][fx0]) * idz);
     Rk[n] = Rp + Rf;
   }
-  Rk[1] = Rk[1] + d.vF[0][c] + f / J;
+  Rk[1] = Rk[1] + d.vF[0][c] + f * iJ;
   Rk[2] = Rk[2] + d.vF[1][c];
   Rk[3] = Rk[3] + d.vF[2][c];
-  Rk[4] = Rk[4] + d.vF[3][c] + f * u / J;
+  Rk[4] = Rk[4] + d.vF[3][c] + f * u * iJ;
   double MR[5];
   MR[0] = (d11 * Rk[0] + d12 * Rk[1] + d13 * Rk[2] + d14 * Rk[3] + d15 * Rk[4]);
   MR[1] = (d21 * Rk[0] + d22 * Rk[1]);

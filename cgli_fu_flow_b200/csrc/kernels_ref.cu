@@ -71,34 +71,28 @@ __global__ void k_flux_x(Dev d) {
   // left state ML[i] from cells i-2..i+2, right state MR[i] from i-1..i+3
   long long c = ix(d, i, j + 1, k + 1);
   double L[5], R[5], F[5], fav3, pp;
-  for (int v = 0; v < 5; v++) {
-    L[v] = m5L(d.U_[v], d.J, c - 2 * d.di, c - d.di, c, c + d.di, c + 2 * d.di);
-    R[v] = m5R(d.U_[v], d.J, c - d.di, c, c + d.di, c + 2 * d.di, c + 3 * d.di);
-  }
+  side5L(d, c - 2 * d.di, d.di, L);
+  side5R(d, c - d.di, d.di, R);
   roe_face(L, R, d.mf[0][0][f], d.mf[0][1][f], d.mf[0][2][f], d.Jf[0][f], d.e, F, fav3, pp);
   for (int v = 0; v < 5; v++) d.inF[0][v][f] = F[v];
 }
 
-// left / right MUSCL states at y face j+1/2 of column (i,k), with the
-// reduced stencils of Flux_Y.cpp:135-250 (valid for Ny >= 6)
-__device__ __forceinline__ void muscl_y(const Dev &d, int v, int i, int j, int k, double &L, double &R) {
-  int jn = d.ny + 1;
-  const double *u = d.U_[v], *J = d.J;
-  long long dj = d.dj;
-  long long c = ix(d, i, j, k);
-  if (j == 1) L = m2(u, J, c, c + dj);
-  else if (j == 2) L = m2(u, J, c, c + dj);
-  else if (j == 3) L = m3L(u, J, c - dj, c, c + dj);
-  else if (j == jn - 1) L = m3L(u, J, c - dj, c, c + dj);
-  else if (j == jn) L = m2(u, J, c, c - dj);
-  else L = m5L(u, J, c - 2 * dj, c - dj, c, c + dj, c + 2 * dj);
-  long long r = c + dj;  // cell j+1
-  if (j == 1) R = m2(u, J, r, r + dj);
-  else if (j == 2) R = m3R(u, J, r - dj, r, r + dj);
-  else if (j == jn - 2) R = m3R(u, J, r - dj, r, r + dj);
-  else if (j == jn - 1) R = m2(u, J, r, r - dj);
-  else if (j == jn) R = m2(u, J, c, c + dj);
-  else R = m5R(u, J, r - 2 * dj, r - dj, r, r + dj, r + 2 * dj);
+// left / right MUSCL states of all five variables at y face j+1/2 of column
+// (i,k), with the reduced stencils of Flux_Y.cpp:135-250 (valid for Ny >= 6)
+__device__ __forceinline__ void muscl_y(const Dev &d, int i, int j, int k, double L[5], double R[5]) {
+  const int jn = d.ny + 1;
+  const long long dj = d.dj;
+  const long long c = ix(d, i, j, k);
+  if (j == 1 || j == 2) side2(d, c, c + dj, L);
+  else if (j == 3 || j == jn - 1) side3L(d, c - dj, dj, L);
+  else if (j == jn) side2(d, c, c - dj, L);
+  else side5L(d, c - 2 * dj, dj, L);
+  const long long r = c + dj;  // cell j+1
+  if (j == 1) side2(d, r, r + dj, R);
+  else if (j == 2 || j == jn - 2) side3R(d, r - dj, dj, R);
+  else if (j == jn - 1) side2(d, r, r - dj, R);
+  else if (j == jn) side2(d, c, c + dj, R);
+  else side5R(d, r - 2 * dj, dj, R);
 }
 
 // y faces j = 1..jn, i = 2..ie-1, k = 1..kn-1 (Flux_Y.cpp:94-413)
@@ -110,7 +104,7 @@ __global__ void k_flux_y(Dev d) {
   int jn = d.ny + 1;
   long long f = ix(d, i, j, k);
   double L[5], R[5], F[5], fav3, pp;
-  for (int v = 0; v < 5; v++) muscl_y(d, v, i + 1, j, k + 1, L[v], R[v]);
+  muscl_y(d, i + 1, j, k + 1, L, R);
   double ety = d.mf[1][4][f], Jf = d.Jf[1][f];
   roe_face(L, R, d.mf[1][3][f], ety, d.mf[1][5][f], Jf, d.e, F, fav3, pp);
   if (j == 1 || j == jn) {
@@ -120,20 +114,18 @@ __global__ void k_flux_y(Dev d) {
   for (int v = 0; v < 5; v++) d.inF[1][v][f] = F[v];
 }
 
-// left / right states at z face k+1/2 (Flux_Z.cpp:105-216, valid for Nz >= 4)
-__device__ __forceinline__ void muscl_z(const Dev &d, int v, int i, int j, int k, double &L, double &R) {
-  int kn = d.nz + 1;
-  const double *u = d.U_[v], *J = d.J;
-  long long c = ix(d, i, j, k);
-  if (k == 1) L = m2(u, J, c, c + 1);
-  else if (k == 2) L = m3L(u, J, c - 1, c, c + 1);
-  else if (k == kn) L = m3L(u, J, c - 1, c, c + 1);
-  else L = m5L(u, J, c - 2, c - 1, c, c + 1, c + 2);
-  long long r = c + 1;
-  if (k == 1) R = m3R(u, J, r - 1, r, r + 1);
-  else if (k == kn - 1) R = m3R(u, J, r - 1, r, r + 1);
-  else if (k == kn) R = m2(u, J, c, c + 1);
-  else R = m5R(u, J, r - 2, r - 1, r, r + 1, r + 2);
+// left / right states of all five variables at z face k+1/2
+// (Flux_Z.cpp:105-216, valid for Nz >= 4)
+__device__ __forceinline__ void muscl_z(const Dev &d, int i, int j, int k, double L[5], double R[5]) {
+  const int kn = d.nz + 1;
+  const long long c = ix(d, i, j, k);
+  if (k == 1) side2(d, c, c + 1, L);
+  else if (k == 2 || k == kn) side3L(d, c - 1, 1, L);
+  else side5L(d, c - 2, 1, L);
+  const long long r = c + 1;
+  if (k == 1 || k == kn - 1) side3R(d, r - 1, 1, R);
+  else if (k == kn) side2(d, c, c + 1, R);
+  else side5R(d, r - 2, 1, R);
 }
 
 // z faces k = 1..kn, i = 2..ie-1, j = 1..jn-1 (Flux_Z.cpp:91-359)
@@ -144,7 +136,7 @@ __global__ void k_flux_z(Dev d) {
   if (k > d.nz + 1) return;
   long long f = ix(d, i, j, k);
   double L[5], R[5], F[5], fav3, pp;
-  for (int v = 0; v < 5; v++) muscl_z(d, v, i + 1, j + 1, k, L[v], R[v]);
+  muscl_z(d, i + 1, j + 1, k, L, R);
   roe_face(L, R, d.mf[2][6][f], d.mf[2][7][f], d.mf[2][8][f], d.Jf[2][f], d.e, F, fav3, pp);
   for (int v = 0; v < 5; v++) d.inF[2][v][f] = F[v];
 }

@@ -72,8 +72,11 @@ __device__ __forceinline__ MetricProducts metric_products(const double x[9]) {
   return q;
 }
 
+// Sutherland's law as Viscous_terms.cpp:527 writes it, with (T/Tref)^1.5
+// evaluated as x*sqrt(x) (the same value to rounding, without pow)
 __device__ __forceinline__ double sutherland_mu(double mu, double T) {
-  return mu * pow((T / 298.0592), 1.5) * (298.0592 + 110.) / (T + 110.);
+  const double x = T * (1.0 / 298.0592);
+  return mu * (x * sqrt(x)) * (298.0592 + 110.) / (T + 110.);
 }
 
 // x face i-1/2, Viscous_terms.cpp:399-546
@@ -84,6 +87,7 @@ __device__ __forceinline__ void visc_face_x(double dxi, double det, double dzt, 
                                             const double mm[9], double Jf, double out[4]) {
   const double invXI = 1. / (dxi), inv4ET = 1. / (4 * det), inv4ZT = 1. / (4 * dzt);
   const double CvK = CV * KG;
+  const double iJf = 1.0 / Jf, ipr = 1.0 / pr;
   double U = o.U, V = o.V, W = o.W, T = o.T;
   double du_dx = (U - im.U) * invXI, dv_dx = (V - im.V) * invXI, dw_dx = (W - im.W) * invXI;
   double du2_dx = (U * U - im.U * im.U) * invXI, dv2_dx = (V * V - im.V * im.V) * invXI,
@@ -107,18 +111,18 @@ __device__ __forceinline__ void visc_face_x(double dxi, double det, double dzt, 
   double Ux = 0.5 * (U + im.U), Vx = 0.5 * (V + im.V), Wx = 0.5 * (W + im.W), Tx = 0.5 * (T + im.T);
   double mu_E = sutherland_mu(mu, Tx);
   out[0] = mu_E * (q.a1 * du_dx + q.a5 * dv_dx + q.a7 * dw_dx + q.d1 * du_dy + q.d7 * dv_dy + q.d9 * dw_dy +
-                   q.e1 * du_dz + q.e7 * dv_dz + q.e9 * dw_dz) / Jf;
+                   q.e1 * du_dz + q.e7 * dv_dz + q.e9 * dw_dz) * iJf;
   out[1] = mu_E * (q.a5 * du_dx + q.a2 * dv_dx + q.a6 * dw_dx + q.d5 * du_dy + q.d2 * dv_dy + q.d10 * dw_dy +
-                   q.e5 * du_dz + q.e2 * dv_dz + q.e10 * dw_dz) / Jf;
+                   q.e5 * du_dz + q.e2 * dv_dz + q.e10 * dw_dz) * iJf;
   out[2] = mu_E * (q.a7 * du_dx + q.a6 * dv_dx + q.a3 * dw_dx + q.d6 * du_dy + q.d8 * dv_dy + q.d3 * dw_dy +
-                   q.e6 * du_dz + q.e8 * dv_dz + q.e3 * dw_dz) / Jf;
+                   q.e6 * du_dz + q.e8 * dv_dz + q.e3 * dw_dz) * iJf;
   out[3] = mu_E * (0.5 * q.a1 * du2_dx + 0.5 * q.a2 * dv2_dx + 0.5 * q.a3 * dw2_dx + q.a5 * duv_dx + q.a6 * dvw_dx +
-                   q.a7 * duw_dx + CvK * q.a4 * dT_dx / (pr) + 0.5 * q.d1 * du2_dy + 0.5 * q.d2 * dv2_dy +
+                   q.a7 * duw_dx + CvK * q.a4 * dT_dx * ipr + 0.5 * q.d1 * du2_dy + 0.5 * q.d2 * dv2_dy +
                    0.5 * q.d3 * dw2_dy + q.d5 * Vx * du_dy + q.d6 * Wx * du_dy + q.d7 * Ux * dv_dy +
-                   q.d8 * Wx * dv_dy + q.d9 * Ux * dw_dy + q.d10 * Vx * dw_dy + CvK * q.d4 * dT_dy / (pr) +
+                   q.d8 * Wx * dv_dy + q.d9 * Ux * dw_dy + q.d10 * Vx * dw_dy + CvK * q.d4 * dT_dy * ipr +
                    0.5 * q.e1 * du2_dz + 0.5 * q.e2 * dv2_dz + 0.5 * q.e3 * dw2_dz + q.e5 * Vx * du_dz +
                    q.e6 * Wx * du_dz + q.e7 * Ux * dv_dz + q.e8 * Wx * dv_dz + q.e9 * Ux * dw_dz +
-                   q.e10 * Vx * dw_dz + CvK * q.e4 * dT_dz / (pr)) / Jf;
+                   q.e10 * Vx * dw_dz + CvK * q.e4 * dT_dz * ipr) * iJf;
 }
 
 // y face j-1/2, Viscous_terms.cpp:549-700
@@ -129,6 +133,7 @@ __device__ __forceinline__ void visc_face_y(double dxi, double det, double dzt, 
                                             const double mm[9], double Jf, double out[4]) {
   const double inv4XI = 1. / (4 * dxi), invET = 1. / (det), inv4ZT = 1. / (4 * dzt);
   const double CvK = CV * KG;
+  const double iJf = 1.0 / Jf, ipr = 1.0 / pr;
   double U = o.U, V = o.V, W = o.W, T = o.T;
   double du_dx = (ip.U + jI.U - im.U - ijm.U) * inv4XI, dv_dx = (ip.V + jI.V - im.V - ijm.V) * inv4XI,
          dw_dx = (ip.W + jI.W - im.W - ijm.W) * inv4XI;
@@ -152,18 +157,18 @@ __device__ __forceinline__ void visc_face_y(double dxi, double det, double dzt, 
   double Uy = 0.5 * (U + jm.U), Vy = 0.5 * (V + jm.V), Wy = 0.5 * (W + jm.W), Ty = 0.5 * (T + jm.T);
   double mu_E = sutherland_mu(mu, Ty);
   out[0] = mu_E * (q.d1 * du_dx + q.d5 * dv_dx + q.d6 * dw_dx + q.b1 * du_dy + q.b5 * dv_dy + q.b7 * dw_dy +
-                   q.f1 * du_dz + q.f7 * dv_dz + q.f9 * dw_dz) / Jf;
+                   q.f1 * du_dz + q.f7 * dv_dz + q.f9 * dw_dz) * iJf;
   out[1] = mu_E * (q.d7 * du_dx + q.d2 * dv_dx + q.d8 * dw_dx + q.b5 * du_dy + q.b2 * dv_dy + q.b6 * dw_dy +
-                   q.f5 * du_dz + q.f2 * dv_dz + q.f10 * dw_dz) / Jf;
+                   q.f5 * du_dz + q.f2 * dv_dz + q.f10 * dw_dz) * iJf;
   out[2] = mu_E * (q.d9 * du_dx + q.d10 * dv_dx + q.d3 * dw_dx + q.b7 * du_dy + q.b6 * dv_dy + q.b3 * dw_dy +
-                   q.f6 * du_dz + q.f8 * dv_dz + q.f3 * dw_dz) / Jf;
+                   q.f6 * du_dz + q.f8 * dv_dz + q.f3 * dw_dz) * iJf;
   out[3] = mu_E * (0.5 * q.b1 * du2_dy + 0.5 * q.b2 * dv2_dy + 0.5 * q.b3 * dw2_dy + q.b5 * duv_dy + q.b6 * dvw_dy +
-                   q.b7 * duw_dy + CvK * q.b4 * dT_dy / (pr) + 0.5 * q.d1 * du2_dx + 0.5 * q.d2 * dv2_dx +
+                   q.b7 * duw_dy + CvK * q.b4 * dT_dy * ipr + 0.5 * q.d1 * du2_dx + 0.5 * q.d2 * dv2_dx +
                    0.5 * q.d3 * dw2_dx + q.d5 * Uy * dv_dx + q.d6 * Uy * dw_dx + q.d7 * Vy * du_dx +
-                   q.d8 * Vy * dw_dx + q.d9 * Wy * du_dx + q.d10 * Wy * dv_dx + CvK * q.d4 * dT_dx / (pr) +
+                   q.d8 * Vy * dw_dx + q.d9 * Wy * du_dx + q.d10 * Wy * dv_dx + CvK * q.d4 * dT_dx * ipr +
                    0.5 * q.f1 * du2_dz + 0.5 * q.f2 * dv2_dz + 0.5 * q.f3 * dw2_dz + q.f5 * Vy * du_dz +
                    q.f6 * Wy * du_dz + q.f7 * Uy * dv_dz + q.f8 * Wy * dv_dz + q.f9 * Uy * dw_dz +
-                   q.f10 * Vy * dw_dz + CvK * q.f4 * dT_dz / (pr)) / Jf;
+                   q.f10 * Vy * dw_dz + CvK * q.f4 * dT_dz * ipr) * iJf;
 }
 
 // z face k-1/2, Viscous_terms.cpp:714-861, with the typo of :744-746 that
@@ -175,6 +180,7 @@ __device__ __forceinline__ void visc_face_z(double dxi, double det, double dzt, 
                                             const P &iJ, const double mm[9], double Jf, double out[4]) {
   const double inv4XI = 1. / (4 * dxi), inv4ET = 1. / (4 * det), invZT = 1. / (dzt);
   const double CvK = CV * KG;
+  const double iJf = 1.0 / Jf, ipr = 1.0 / pr;
   double U = o.U, V = o.V, W = o.W, T = o.T;
   double du_dx = (ip.U + kI.U - im.U - ikm.U) * inv4XI, dv_dx = (ip.V + kI.V - im.V - ikm.V) * inv4XI,
          dw_dx = (ip.W + kI.W - im.W - ikm.W) * inv4XI;
@@ -199,18 +205,18 @@ __device__ __forceinline__ void visc_face_z(double dxi, double det, double dzt, 
   double Uz = 0.5 * (U + km.U), Vz = 0.5 * (V + km.V), Wz = 0.5 * (W + km.W), Tz = 0.5 * (T + km.T);
   double mu_E = sutherland_mu(mu, Tz);
   out[0] = mu_E * (q.e1 * du_dx + q.e5 * dv_dx + q.e6 * dw_dx + q.f1 * du_dy + q.f5 * dv_dy + q.f6 * dw_dy +
-                   q.c1 * du_dz + q.c5 * dv_dz + q.c7 * dw_dz) / Jf;
+                   q.c1 * du_dz + q.c5 * dv_dz + q.c7 * dw_dz) * iJf;
   out[1] = mu_E * (q.e7 * du_dx + q.e2 * dv_dx + q.e8 * dw_dx + q.f7 * du_dy + q.f2 * dv_dy + q.f8 * dw_dy +
-                   q.c5 * du_dz + q.c2 * dv_dz + q.c6 * dw_dz) / Jf;
+                   q.c5 * du_dz + q.c2 * dv_dz + q.c6 * dw_dz) * iJf;
   out[2] = mu_E * (q.e9 * du_dx + q.e10 * dv_dx + q.e3 * dw_dx + q.f9 * du_dy + q.f10 * dv_dy + q.f3 * dw_dy +
-                   q.c7 * du_dz + q.c6 * dv_dz + q.c3 * dw_dz) / Jf;
+                   q.c7 * du_dz + q.c6 * dv_dz + q.c3 * dw_dz) * iJf;
   out[3] = mu_E * (0.5 * q.c1 * du2_dz + 0.5 * q.c2 * dv2_dz + 0.5 * q.c3 * dw2_dz + q.c5 * duv_dz + q.c6 * dvw_dz +
-                   q.c7 * duw_dz + CvK * q.c4 * dT_dz / (pr) + 0.5 * q.e1 * du2_dx + 0.5 * q.e2 * dv2_dx +
+                   q.c7 * duw_dz + CvK * q.c4 * dT_dz * ipr + 0.5 * q.e1 * du2_dx + 0.5 * q.e2 * dv2_dx +
                    0.5 * q.e3 * dw2_dx + q.e5 * Uz * dv_dx + q.e6 * Uz * dw_dx + q.e7 * Vz * du_dx +
-                   q.e8 * Vz * dw_dx + q.e9 * Wz * du_dx + q.e10 * Wz * dv_dx + CvK * q.e4 * dT_dx / (pr) +
+                   q.e8 * Vz * dw_dx + q.e9 * Wz * du_dx + q.e10 * Wz * dv_dx + CvK * q.e4 * dT_dx * ipr +
                    0.5 * q.f1 * du2_dy + 0.5 * q.f2 * dv2_dy + 0.5 * q.f3 * dw2_dy + q.f5 * Uz * dv_dy +
                    q.f6 * Uz * dw_dy + q.f7 * Vz * du_dy + q.f8 * Vz * dw_dy + q.f9 * Wz * du_dy +
-                   q.f10 * Wz * dv_dy + CvK * q.f4 * dT_dy / (pr)) / Jf;
+                   q.f10 * Wz * dv_dy + CvK * q.f4 * dT_dy * ipr) * iJf;
 }
 
 }  // namespace cgli

@@ -50,7 +50,7 @@ EXPORTS = [
     "cgli_cnn_param_count", "cgli_cnn_create", "cgli_cnn_destroy", "cgli_cnn_last_error", "cgli_cnn_set_params",
     "cgli_cnn_get_params", "cgli_cnn_set_scales", "cgli_cnn_forward_host", "cgli_cnn_loss_grad_host",
     "cgli_cnn_reserve_levels", "cgli_cnn_levels", "cgli_cnn_push_level_host", "cgli_cnn_push_level",
-    "cgli_cnn_pair_loss", "cgli_cnn_train", "cgli_set_learned_guess",
+    "cgli_cnn_pair_loss", "cgli_cnn_train", "cgli_set_learned_guess", "cgli_step_norms",
 ]
 
 _lib = None
@@ -109,6 +109,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cgli_cnn_pair_loss.argtypes = [P, LL, FP]
     L.cgli_cnn_train.argtypes = [P, ctypes.c_int, F, ctypes.c_ulonglong, LL, LL, FP]
     L.cgli_set_learned_guess.argtypes = [P, P]
+    L.cgli_step_norms.argtypes = [P, P, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     L.cgli_update_norms_noalloc.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P, DP, P]
     L.cgli_event_record.argtypes = [P, ctypes.c_int]
     L.cgli_event_elapsed.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
@@ -283,6 +284,16 @@ class Solver:
         """0: previous time level (reference); 1: second-order extrapolation;
         2: extrapolation plus the learned correction (set_learned_guess)."""
         self._rc(self.L.cgli_set_predictor(self.h, mode))
+
+    def step_norms(self) -> np.ndarray:
+        """(iterations, 5) norms of every inner iteration of the last step."""
+        buf = np.zeros((64, 5))
+        n = ctypes.c_int()
+        self._rc(self.L.cgli_step_norms(self.h, buf.ctypes.data, 64, ctypes.byref(n)))
+        if n.value > 64:
+            buf = np.zeros((n.value, 5))
+            self._rc(self.L.cgli_step_norms(self.h, buf.ctypes.data, n.value, ctypes.byref(n)))
+        return buf[:n.value].copy()
 
     def set_learned_guess(self, net) -> None:
         """Attach a cgli_fu_flow_b200.cnn.Network (None detaches)."""

@@ -123,6 +123,10 @@ int cgli_set_force(cgli_ctx *ctx, double force);
  * runs exactly that many), then the time-level shift (Q^(n-2) is kept too).
  * Returns the iteration count and the final norms. */
 int cgli_step(cgli_ctx *ctx, int fixed_iters, double drop, int cap, int *iters, double er[5]);
+/* The five norms of every inner iteration of the last cgli_step, iteration
+ * by iteration (norms[5*i + v]); copies min(iterations, max_iters) rows and
+ * returns the iteration count in *iters. */
+int cgli_step_norms(cgli_ctx *ctx, double *norms, int max_iters, int *iters);
 /* Initial guess of each step's inner iteration.  0: Q^(n+1,0) = Q^n, as
  * main.cpp:364-386 leaves it; 1: second-order extrapolation
  * 3Q^n - 3Q^(n-1) + Q^(n-2) (2Q^n - Q^(n-1) for the first step after

@@ -188,12 +188,17 @@ def test_training_on_solver_levels_and_ab_against_extrapolation():
     assert loss1 < 0.7 * loss0
     B.set_learned_guess(net)
     B.set_predictor(2)
-    it_a, it_b, held_cnn, held_ext = [], [], [], []
+    it_a, it_b, held_cnn, held_ext, saved = [], [], [], [], []
     for k in range(12):
         na, _ = A.step(None, 1e-3, 30)
         nb, _ = B.step(None, 1e-3, 30)
         it_a.append(na)
         it_b.append(nb)
+        # iterations the learned guess needs to reach the accuracy (all five
+        # update norms) that extrapolation reached at its last iteration
+        ea, eb = A.step_norms(), B.step_norms()
+        reach = np.nonzero(np.all(eb <= ea[-1] * (1 + 1e-12), axis=1))[0]
+        saved.append(len(ea) - (reach[0] + 1) if reach.size else 0)
         net.push_level(A)
         p = net.levels - 4
         held_cnn.append(net.pair_loss(p))
@@ -204,4 +209,6 @@ def test_training_on_solver_levels_and_ab_against_extrapolation():
         held_ext.append(float(np.mean(r * r)))
     print("held-out guess MSE (normalised): learned", np.mean(held_cnn), "extrapolation", np.mean(held_ext))
     print("inner iterations: extrapolation", it_a, "learned", it_b)
+    print("iterations saved at equal update norms:", saved)
     assert np.mean(held_cnn) < 0.9 * np.mean(held_ext)
+    assert sum(saved) >= 0
