@@ -2,11 +2,20 @@
 
 A step is one physical time step of the dual-time scheme on the
 256 x 192 x 192 channel (the plain-FP64-at-scale workload): inner LU-SGS
-iterations until every one of the five update norms has dropped by 1e-3
-relative to the step's first iteration (capped at 30), then the time-level
-shift and the driving-force update.  All state stays resident on the GPU for
-`value`; `e2e` repeats the measurement through the C ABI with the step's
-inputs copied from pinned host memory and its result copied back every step.
+iterations until every one of the five update norms, divided by its running
+maximum over the run (the reference's rule), is below 1e-3 (capped at 30),
+then the time-level shift and the driving-force update.  All state stays
+resident on the GPU for `value` (plain FP64, the reference's algorithm, from
+the seeded field); `e2e` repeats the measurement through the C ABI with the
+step's inputs copied from pinned host memory and its result copied back
+every step.
+
+`arms` compares, from one common point of a run (after `--collect` steps
+with second-order extrapolation in mixed precision, whose converged levels
+train the learned initial guess with Adam on the GPU), the same number of
+steps in: plain FP64 (previous-level guess), mixed precision with
+extrapolation, and mixed precision with the learned guess, with each mixed
+arm's state error against the FP64 arm.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -51,6 +60,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-iters", type=int, default=2, help="reference inner iterations in the CPU sample")
+    ap.add_argument("--arms", default="all", choices=["all", "none"])
+    ap.add_argument("--collect", type=int, default=40, help="steps whose levels train the learned guess")
+    ap.add_argument("--train-steps", type=int, default=300)
+    ap.add_argument("--lr", type=float, default=1e-3)
     return ap.parse_args()
 
 
@@ -173,6 +186,7 @@ def run_gpu(a, dist: Dist) -> dict | None:
     if not a.no_e2e:
         e2e = run_e2e(a, ch, prec, dist)
     sol.close()
+    arms = run_arms(a, ch, dist) if a.arms == "all" else None
     if dist.rank != 0:
         return None
     from cgli_fu_flow_b200 import roofline
@@ -203,6 +217,86 @@ def run_gpu(a, dist: Dist) -> dict | None:
     }
     if e2e:
         out["e2e"] = e2e
+    if arms:
+        out["arms"] = arms
+    return out
+
+
+def _timed_steps(sol, a, dist):
+    iters = []
+    dist.barrier()
+    sol.event(0)
+    for _ in range(a.steps):
+        it, _ = sol.step(None, a.drop, a.cap)
+        iters.append(it)
+    sol.event(1)
+    ms = dist.max(sol.elapsed_ms(0, 1))
+    return ms, iters
+
+
+def run_arms(a, ch, dist) -> dict:
+    """FP64 / mixed + extrapolation / mixed + learned guess from one point of
+    a run (module docstring)."""
+    from cgli_fu_flow_b200.cnn import (CNN_FLOP_PER_CELL, CNN_TC_FLOP_PER_CELL, Network, init_params,
+                                       physical_levels, scales_from_levels)
+    from cgli_fu_flow_b200.solver import FP64, MIXED, Solver
+    base = Solver(ch, MIXED)
+    base.init(ch.initial_conserved())
+    base.set_predictor(1)
+    net = Network(ch.nx, ch.ny, ch.nz)
+    net.reserve_levels(a.collect)
+    net.set_params(init_params(0))
+    host = []
+    t0 = time.perf_counter()
+    for k in range(a.collect):
+        base.step(None, a.drop, a.cap)
+        net.push_level(base)
+        if k >= a.collect - 6:
+            host.append(physical_levels(base, np.float32))
+    collect_s = time.perf_counter() - t0
+    net.set_scales(*scales_from_levels(host))
+    del host
+    npairs = net.levels - 3
+    t0 = time.perf_counter()
+    loss = net.train(a.train_steps, a.lr, 20261203, 0, npairs)
+    train_s = time.perf_counter() - t0
+    held = float(np.mean([net.pair_loss(p) for p in range(max(0, npairs - 4), npairs)]))
+    out = {"common_point": f"after {a.collect} steps from the seeded field (mixed precision, extrapolated guess)",
+           "learned_guess": {"training_pairs": npairs, "adam_steps": a.train_steps, "lr": a.lr,
+                             "final_mean_loss": round(loss, 5), "last_pairs_loss": round(held, 5),
+                             "collect_s": round(collect_s, 2), "train_s": round(train_s, 2),
+                             "loss_unit": "mean squared extrapolation correction / its RMS (1.0 = extrapolation)"}}
+    sols = {}
+    for name, prec, pred in (("fp64", FP64, 0), ("mixed_extrapolation", MIXED, 1), ("mixed_learned", MIXED, 2)):
+        s = Solver(ch, prec)
+        s.copy_state_from(base)
+        if pred == 2:
+            s.set_learned_guess(net)
+        s.set_predictor(pred)
+        for _ in range(a.warmup):
+            s.step(None, a.drop, a.cap)
+        ms, iters = _timed_steps(s, a, dist)
+        value = dist.sum(float(ch.cells) * a.steps) / (ms / 1e3) / 1e6
+        out[name] = {"value": round(value, 3), "unit": "Mcell-steps/s", "ms_per_step": round(ms / a.steps, 3),
+                     "mean_inner_iterations": round(float(np.mean(iters)), 2), "inner_iterations": iters,
+                     "precision": "fp64" if prec == FP64 else "mixed", "predictor": ["previous level", "extrapolation",
+                                                                                     "learned"][pred]}
+        if pred == 2:
+            inf_ms = net.time_inference(s, 3)
+            tf = ch.cells * CNN_TC_FLOP_PER_CELL / (inf_ms / 1e3) / 1e12
+            out[name]["inference"] = {"ms": round(inf_ms, 3), "tensor_tflops": round(tf, 1),
+                                      "real_tflops": round(ch.cells * CNN_FLOP_PER_CELL / (inf_ms / 1e3) / 1e12, 1)}
+        sols[name] = s
+    sl = (slice(None), slice(3, ch.nx + 3), slice(2, ch.ny + 2), slice(2, ch.nz + 2))
+    ref = sols["fp64"].q()[sl]
+    for name in ("mixed_extrapolation", "mixed_learned"):
+        q = sols[name].q()[sl]
+        errs = [float(np.linalg.norm(q[v] - ref[v]) / np.linalg.norm(ref[v])) for v in range(5)]
+        out[name]["state_rel_l2_vs_fp64"] = max(errs)
+    for s in sols.values():
+        s.close()
+    base.close()
+    net.close()
     return out
 
 

@@ -102,6 +102,12 @@ class Network:
         a = np.ascontiguousarray(q, dtype=np.float32)
         self._rc(self.L.cgli_cnn_push_level_host(self.h, a.ctypes.data))
 
+    def time_inference(self, solver, reps: int = 3) -> float:
+        """Mean device ms of one inference on the solver's current levels."""
+        ms = ctypes.c_float()
+        self._rc(self.L.cgli_cnn_time_inference(self.h, solver.h, reps, ctypes.byref(ms)))
+        return float(ms.value)
+
     def pair_loss(self, pair: int) -> float:
         loss = ctypes.c_float()
         self._rc(self.L.cgli_cnn_pair_loss(self.h, pair, ctypes.byref(loss)))
@@ -113,12 +119,18 @@ class Network:
         return float(loss.value)
 
 
-def physical_levels(solver) -> np.ndarray:
+def physical_levels(solver, dtype=np.float64) -> np.ndarray:
     """Q = U*J of the solver's current level on the interior, (5, nx, ny, nz)."""
     ch = solver.ch
     sl = np.s_[3:ch.nx + 3, 2:ch.ny + 2, 2:ch.nz + 2]
     J = solver.get("J")[sl]
-    return np.stack([solver.get(f"U{v}")[sl] * J for v in range(1, 6)])
+    return np.stack([(solver.get(f"U{v}")[sl] * J).astype(dtype) for v in range(1, 6)])
+
+
+# real multiply-adds per cell of one inference (15->32, 3 x 32->32, 32->5,
+# 27 taps) and the ones the tensor cores execute (every layer padded to 32x32)
+CNN_FLOP_PER_CELL = 2 * 27 * (15 * 32 + 3 * 32 * 32 + 32 * 5)
+CNN_TC_FLOP_PER_CELL = 2 * 27 * 32 * 32 * 5
 
 
 def scales_from_levels(levels: list[np.ndarray]):

@@ -435,6 +435,28 @@ int cgli_set_state(cgli_ctx *c, const double *const U_[5], const double *const U
   return CGLI_OK;
 }
 
+int cgli_copy_state(cgli_ctx *dst, const cgli_ctx *src) {
+  int rc = check(dst); if (rc) return rc;
+  if (!src || !src->have_state) return fail(CGLI_ESTATE, "source context has no state");
+  if (src->p.nx != dst->p.nx || src->p.ny != dst->p.ny || src->p.nz != dst->p.nz)
+    return fail(CGLI_EINVAL, "contexts of different grids");
+  CUDA_TRY(cudaStreamSynchronize(src->stream));
+  size_t n = (size_t)dst->d.X * dst->d.Y * dst->d.Z * sizeof(double);
+  for (int v = 0; v < 5; v++) {
+    CUDA_TRY(cudaMemcpyAsync(dst->d.U_[v], src->d.U_[v], n, cudaMemcpyDeviceToDevice, dst->stream));
+    CUDA_TRY(cudaMemcpyAsync(dst->d.U[v], src->d.U[v], n, cudaMemcpyDeviceToDevice, dst->stream));
+    CUDA_TRY(cudaMemcpyAsync(dst->d.Uq[v], src->d.Uq[v], n, cudaMemcpyDeviceToDevice, dst->stream));
+    CUDA_TRY(cudaMemcpyAsync(dst->d.Uqq[v], src->d.Uqq[v], n, cudaMemcpyDeviceToDevice, dst->stream));
+  }
+  dst->p.force = src->p.force;
+  CUDA_TRY(cudaMemcpyAsync(dst->d.scal, &dst->p.force, sizeof(double), cudaMemcpyHostToDevice, dst->stream));
+  CUDA_TRY(cudaStreamSynchronize(dst->stream));
+  for (int v = 0; v < 5; v++) dst->Emax[v] = src->Emax[v];
+  dst->history = src->history;
+  dst->have_state = true;
+  return CGLI_OK;
+}
+
 int cgli_get_state(cgli_ctx *c, double *const U_[5]) {
   int rc = check(c); if (rc) return rc;
   if (!U_) return fail(CGLI_EINVAL, "null argument");
@@ -567,6 +589,14 @@ int cgli_cnn_push_level(cgli_cnn *n, cgli_ctx *c) {
     return fail(CGLI_EINVAL, "network grid differs from the context's grid");
   if (!c->have_state) return fail(CGLI_ESTATE, "state not set (cgli_set_state)");
   return cgli::cnn_store_level(n, c->d, c->stream);
+}
+
+int cgli_cnn_time_inference(cgli_cnn *n, cgli_ctx *c, int reps, float *ms) {
+  int rc = check(c); if (rc) return rc;
+  if (!n || !ms || reps <= 0) return fail(CGLI_EINVAL, "bad argument");
+  if (!cgli::cnn_matches(n, c->p.nx, c->p.ny, c->p.nz)) return fail(CGLI_EINVAL, "network grid differs from the context's grid");
+  if (!c->have_state) return fail(CGLI_ESTATE, "state not set (cgli_set_state)");
+  return cgli::cnn_time_inference(n, c->d, c->stream, reps, ms);
 }
 
 int cgli_step(cgli_ctx *c, int fixed_iters, double drop, int cap, int *iters, double er[5]) {

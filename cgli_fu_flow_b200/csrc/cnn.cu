@@ -1196,6 +1196,29 @@ const char *cgli_cnn_last_error(void) { return g_cnn_err.c_str(); }
 }  // extern "C"
 
 namespace cgli {
+// device time of the network's inference on the context's levels (packing
+// and the five layers, not the update of U_), mean over reps
+int cnn_time_inference(cgli_cnn *n, const Dev &d, cudaStream_t s, int reps, float *ms) {
+  cudaEvent_t e0, e1;
+  CC(cudaEventCreate(&e0));
+  CC(cudaEventCreate(&e1));
+  const unsigned nb = (unsigned)((n->cells + 255) / 256);
+  CC(cudaEventRecord(e0, s));
+  for (int r = 0; r < reps; r++) {
+    k_pack_state<<<nb, 256, 0, s>>>(d, n->act[0], n->sc);
+    launch_halo(n, n->act[0], s);
+    forward(n, false, s);
+  }
+  CC(cudaEventRecord(e1, s));
+  CC(cudaEventSynchronize(e1));
+  float t = 0.f;
+  CC(cudaEventElapsedTime(&t, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms = t / reps;
+  return check_status(n, s);
+}
+
 // stores the context's current level (U = Q^n after cgli_end_step) as physical Q
 int cnn_store_level(cgli_cnn *n, const Dev &d, cudaStream_t s) {
   if (n->levels.empty()) return cfail(CGLI_ESTATE, "no level storage (cgli_cnn_reserve_levels)");

@@ -15,5 +15,7 @@ cudaError_t cnn_predict(cgli_cnn *n, const Dev &d, cudaStream_t s);
 // appends the context's current level U (Q^n after the time-level shift) as
 // physical Q to the network's stored levels
 int cnn_store_level(cgli_cnn *n, const Dev &d, cudaStream_t s);
+// mean device time of `reps` inferences on the context's levels
+int cnn_time_inference(cgli_cnn *n, const Dev &d, cudaStream_t s, int reps, float *ms);
 
 }  // namespace cgli

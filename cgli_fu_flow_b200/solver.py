@@ -51,6 +51,7 @@ EXPORTS = [
     "cgli_cnn_get_params", "cgli_cnn_set_scales", "cgli_cnn_forward_host", "cgli_cnn_loss_grad_host",
     "cgli_cnn_reserve_levels", "cgli_cnn_levels", "cgli_cnn_push_level_host", "cgli_cnn_push_level",
     "cgli_cnn_pair_loss", "cgli_cnn_train", "cgli_set_learned_guess", "cgli_step_norms",
+    "cgli_copy_state", "cgli_cnn_time_inference",
 ]
 
 _lib = None
@@ -110,6 +111,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cgli_cnn_train.argtypes = [P, ctypes.c_int, F, ctypes.c_ulonglong, LL, LL, FP]
     L.cgli_set_learned_guess.argtypes = [P, P]
     L.cgli_step_norms.argtypes = [P, P, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    L.cgli_copy_state.argtypes = [P, P]
+    L.cgli_cnn_time_inference.argtypes = [P, P, ctypes.c_int, FP]
     L.cgli_update_norms_noalloc.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P, DP, P]
     L.cgli_event_record.argtypes = [P, ctypes.c_int]
     L.cgli_event_elapsed.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
@@ -284,6 +287,13 @@ class Solver:
         """0: previous time level (reference); 1: second-order extrapolation;
         2: extrapolation plus the learned correction (set_learned_guess)."""
         self._rc(self.L.cgli_set_predictor(self.h, mode))
+
+    def copy_state_from(self, other: "Solver") -> None:
+        """Continue `other`'s run from its current point (levels, force and
+        its controller, norm maxima, history)."""
+        self._rc(self.L.cgli_copy_state(self.h, other.h))
+        self.force = other.force
+        self.ctrl = dict(other.ctrl)
 
     def step_norms(self) -> np.ndarray:
         """(iterations, 5) norms of every inner iteration of the last step."""

@@ -84,6 +84,11 @@ int cgli_set_state(cgli_ctx *ctx, const double *const U_[5], const double *const
                    const double *const Uq[5]);
 /* Reads back Q^(n+1,m) (5 arrays). */
 int cgli_get_state(cgli_ctx *ctx, double *const U_[5]);
+/* Copies the time levels (U_, U, Uq, Q^(n-2)), the driving force, the
+ * running maxima of the norms and the step history of `src` into `dst`
+ * (device to device; same grid, any precision), so that several contexts
+ * continue one run from the same point. */
+int cgli_copy_state(cgli_ctx *dst, const cgli_ctx *src);
 
 /* ---- the reference routines, one entry point each, acting on the device state */
 /* main.cpp:167-200: periodic 3-plane halo of U_ in x */
@@ -170,6 +175,9 @@ int cgli_cnn_pair_loss(cgli_cnn *cnn, long long pair, float *loss);
  * from [first_pair, first_pair + npairs); mean training loss */
 int cgli_cnn_train(cgli_cnn *cnn, int steps, float lr, unsigned long long seed, long long first_pair,
                    long long npairs, float *mean_loss);
+/* device time (ms, mean over reps) of the network's inference on the
+ * context's current levels: input packing and the five layers */
+int cgli_cnn_time_inference(cgli_cnn *cnn, cgli_ctx *ctx, int reps, float *ms);
 /* use the network for predictor mode 2 (null detaches it) */
 int cgli_set_learned_guess(cgli_ctx *ctx, cgli_cnn *cnn);
 

@@ -190,3 +190,50 @@ def test_extrapolated_predictor_matches_oracle(lib):
     qg, qo = g.q()[sl], o.q()[sl]
     for v in range(5):
         assert rel_l2(qg[v], qo[v]) <= STEP_TOL, v
+
+
+MIXED_TOL = 1e-6
+
+
+def test_mixed_precision_hundred_steps_within_1e6_of_fp64_oracle(lib):
+    """FP32 sweeps and split Jacobians, FP64 residual, filter-free update:
+    after 100 physical steps x 10 inner iterations the state differs from the
+    FP64 CPU oracle by at most 1e-6 (relative L2, every variable)."""
+    from cgli_fu_flow_b200.solver import Solver, MIXED
+    from oracle.oracle import Oracle
+    ch = Channel(16, 24, 16)
+    g = Solver(ch, MIXED)
+    g.init()
+    o = Oracle(ch)
+    o.init()
+    for _ in range(100):
+        g.step(10)
+        o.step(10)
+    reg = regions(ch)
+    sl = (slice(None),) + reg["cell"]
+    qg, qo = g.q()[sl], o.q()[sl]
+    errs = [rel_l2(qg[v], qo[v]) for v in range(5)]
+    print("mixed vs FP64 oracle after 100 steps, relative L2 per variable:", errs)
+    assert max(errs) <= MIXED_TOL
+
+
+def test_copy_state_continues_the_same_run(lib):
+    """Two contexts continued from one point by cgli_copy_state produce the
+    same states as the original context (bit for bit: same kernels, same
+    order)."""
+    from cgli_fu_flow_b200.solver import Solver
+    ch = Channel(10, 12, 8)
+    a = Solver(ch)
+    a.init()
+    a.set_predictor(1)
+    for _ in range(3):
+        a.step(None, 1e-2, 20)
+    b = Solver(ch)
+    b.copy_state_from(a)
+    b.set_predictor(1)
+    for _ in range(2):
+        ia, _ = a.step(None, 1e-2, 20)
+        ib, _ = b.step(None, 1e-2, 20)
+        assert ia == ib
+    sl = (slice(None),) + regions(ch)["cell"]
+    assert np.array_equal(a.q()[sl], b.q()[sl])
