@@ -276,7 +276,7 @@ int cgli_create(const cgli_params *p, cgli_ctx **out) {
   }
 #undef F
   if (rc == CGLI_OK) rc = alloc(c, 16 * sizeof(double), (void **)&d.scal);
-  if (rc == CGLI_OK) rc = alloc(c, 16 * sizeof(double), (void **)&c->d_out);
+  if (rc == CGLI_OK) rc = alloc(c, (8 + 296) * sizeof(double), (void **)&c->d_out);
   if (rc == CGLI_OK) rc = alloc(c, 16 * sizeof(int), (void **)&d.status);
   c->update_blocks = p->nx * p->ny;
   const int nti = (p->nx + cgli::SWEEP_TI - 1) / cgli::SWEEP_TI, ntj = (p->ny + cgli::SWEEP_TJ - 1) / cgli::SWEEP_TJ;

@@ -71,7 +71,8 @@ void launch_viscous(const Dev &d, cudaStream_t s);
 void launch_dts(const Dev &d, cudaStream_t s, int update_blocks_x);
 // reduces d.partial (nblocks x 5) into out[5] = sqrt(sum) * scale
 void launch_norms(const Dev &d, cudaStream_t s, int nblocks, double scale, double *out);
-// bulk mass flux (Driven_force.cpp:38-62) into out[0]
+// bulk mass flux (Driven_force.cpp:38-62) into out[0]; out holds 8 + 296
+// doubles (per-block partial sums at out + 8)
 void launch_bulk_flux(const Dev &d, cudaStream_t s, double *out);
 // time-level shift over planes 2..ie+1 (main.cpp:364-386)
 void launch_end_step(const Dev &d, cudaStream_t s);

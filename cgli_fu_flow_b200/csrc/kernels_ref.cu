@@ -464,20 +464,33 @@ __global__ void k_norms(const double *partial, int nblocks, double scale, double
 
 // bulk mass flux, Driven_force.cpp:38-62: sum over interior cells of
 // (U2_*J)/J / Jsum with Jsum the column volume sum at (i,k) = (3,3)
-__global__ void k_bulk_flux(Dev d, double *out) {
+// bulk mass flux of Driven_force.cpp:38-62: sum over the interior of
+// (rho u / J... as written) / Jsum, divided by Nx Nz; a grid-wide two-stage
+// reduction in a fixed order (per-block partials, then one block)
+__global__ void k_bulk_partial(Dev d, double *part) {
   double acc[5] = {0, 0, 0, 0, 0};
-  double Jsum = 0;
-  for (int j = 2; j <= d.ny + 1; j++) Jsum = Jsum + 1. / d.J[ix(d, 3, j, 3)];
-  long long n = (long long)d.nx * d.ny * d.nz;
-  for (long long t = threadIdx.x; t < n; t += blockDim.x) {
+  const long long n = (long long)d.nx * d.ny * d.nz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     int k = (int)(t % d.nz), j = (int)((t / d.nz) % d.ny), i = (int)(t / ((long long)d.nz * d.ny));
     long long c = ix(d, i + 3, j + 2, k + 2);
-    acc[0] += (d.U_[1][c] * d.J[c]) * 1. / d.J[c] / Jsum;
+    acc[0] += (d.U_[1][c] * d.J[c]) * 1. / d.J[c];
   }
   __shared__ double tot[5];
   block_sum5(acc, tot);
   __syncthreads();
-  if (threadIdx.x == 0) out[0] = tot[0] / d.nx / d.nz;
+  if (threadIdx.x == 0) part[blockIdx.x] = tot[0];
+}
+__global__ void k_bulk_final(Dev d, const double *part, int nblk, double *out) {
+  double acc[5] = {0, 0, 0, 0, 0};
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) acc[0] += part[b];
+  __shared__ double tot[5];
+  block_sum5(acc, tot);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double Jsum = 0;
+    for (int j = 2; j <= d.ny + 1; j++) Jsum = Jsum + 1. / d.J[ix(d, 3, j, 3)];
+    out[0] = tot[0] / Jsum / d.nx / d.nz;
+  }
 }
 
 // main.cpp:364-386 over planes 2..ie+1, all rows; Q^(n-2) is kept as well
@@ -515,7 +528,10 @@ void launch_norms(const Dev &d, cudaStream_t s, int nblocks, double scale, doubl
   k_norms<<<1, 1024, 0, s>>>(d.partial, nblocks, scale, out);
 }
 void launch_bulk_flux(const Dev &d, cudaStream_t s, double *out) {
-  k_bulk_flux<<<1, 1024, 0, s>>>(d, out);
+  // the per-block partials go to out[8 ..]: the caller's scratch holds 8 + 296 doubles
+  constexpr int kBlocks = 296;
+  k_bulk_partial<<<kBlocks, 256, 0, s>>>(d, out + 8);
+  k_bulk_final<<<1, 256, 0, s>>>(d, out + 8, kBlocks, out);
 }
 void launch_end_step(const Dev &d, cudaStream_t s) {
   long long n = (long long)(d.nx + 2) * d.di;

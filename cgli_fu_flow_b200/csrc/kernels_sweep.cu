@@ -199,6 +199,34 @@ __global__ void __launch_bounds__(TI *TJ) k_sweep(Dev d, SweepArgs a) {
   T carry_z[5] = {0, 0, 0, 0, 0};
   double acc[5] = {0, 0, 0, 0, 0};
 
+  // hand-over values of the next two steps, loaded ahead: a neighbouring
+  // tile runs just far enough ahead for its value to exist when needed, so
+  // a load issued then would wait one L2 round trip per step; loaded two
+  // steps early it is usually there (a sentinel falls back to the bounded
+  // poll)
+  auto kl_of = [&](int step) {
+    const int r = BACKWARD ? step - (TI - 1 - il) - (TJ - 1 - jl) : step - il - jl;
+    return (inside && r >= 0 && r < Nz) ? (BACKWARD ? Nz - 1 - r : r) : -1;
+  };
+  const T *xsrc = xb + ((long long)tile_pa * TJ + jl) * Nz * 5;
+  const T *ysrc = yb + ((long long)tile_pb * TI + il) * Nz * 5;
+  const bool pre_x = recv_x, pre_y = recv_y && !wall_y;
+  T px0[5], px1[5], py0[5], py1[5];
+  auto preload = [&](int step, T *px, T *py) {
+    const int k2 = kl_of(step);
+#pragma unroll
+    for (int v = 0; v < 5; v++) { px[v] = (T)0; py[v] = (T)0; }
+    if (k2 < 0) return;
+    if (pre_x)
+#pragma unroll
+      for (int v = 0; v < 5; v++) px[v] = ld_gpu(xsrc + (long long)k2 * 5 + v);
+    if (pre_y)
+#pragma unroll
+      for (int v = 0; v < 5; v++) py[v] = ld_gpu(ysrc + (long long)k2 * 5 + v);
+  };
+  preload(0, px0, py0);
+  preload(1, px1, py1);
+
   Cell<T> cur, nxt;
   fetch_cell<TI, TJ, Met, BACKWARD, T>(d, a, s_et, il, jl, j, 0, S, tile_base, inside, halo_edge, cur);
 
@@ -219,14 +247,20 @@ __global__ void __launch_bounds__(TI *TJ) k_sweep(Dev d, SweepArgs a) {
 #pragma unroll
         for (int v = 0; v < 5; v++) tx[v] = sx[pbuf][sil][jl][v];
       } else {
-        recv5<T>(xb + (((long long)tile_pa * TJ + jl) * Nz + kl) * 5, tx, d.status, a.spin_limit);
+        bool ok = true;
+#pragma unroll
+        for (int v = 0; v < 5; v++) { tx[v] = px0[v]; ok = ok && !is_sentinel(px0[v]); }
+        if (!ok) recv5<T>(xsrc + (long long)kl * 5, tx, d.status, a.spin_limit);
       }
       if (!recv_y) {
         const int sjl = BACKWARD ? jl + 1 : jl - 1;
 #pragma unroll
         for (int v = 0; v < 5; v++) ty[v] = sy[pbuf][il][sjl][v];
       } else if (!wall_y) {
-        recv5<T>(yb + (((long long)tile_pb * TI + il) * Nz + kl) * 5, ty, d.status, a.spin_limit);
+        bool ok = true;
+#pragma unroll
+        for (int v = 0; v < 5; v++) { ty[v] = py0[v]; ok = ok && !is_sentinel(py0[v]); }
+        if (!ok) recv5<T>(ysrc + (long long)kl * 5, ty, d.status, a.spin_limit);
       } else {
 #pragma unroll
         for (int v = 0; v < 5; v++) ty[v] = 0;  // wall ghost row: dQ = 0 there
@@ -320,6 +354,11 @@ __global__ void __launch_bounds__(TI *TJ) k_sweep(Dev d, SweepArgs a) {
             for (int v = 0; v < 5; v++) SweepPtrs<T>::hb(a)[v][h] = n[v];
         }
       }
+    }
+    if (pre_x || pre_y) {
+#pragma unroll
+      for (int v = 0; v < 5; v++) { px0[v] = px1[v]; py0[v] = py1[v]; }
+      if (s + 2 < S) preload(s + 2, px1, py1);
     }
     cur = nxt;
     __syncthreads();
