@@ -61,8 +61,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-iters", type=int, default=2, help="reference inner iterations in the CPU sample")
     ap.add_argument("--arms", default="all", choices=["all", "none"])
-    ap.add_argument("--collect", type=int, default=40, help="steps whose levels train the learned guess")
-    ap.add_argument("--train-steps", type=int, default=300)
+    ap.add_argument("--collect", type=int, default=48, help="steps before the common point of the arms")
+    ap.add_argument("--skip", type=int, default=16, help="first steps (initial transient) not used for training")
+    ap.add_argument("--train-steps", type=int, default=600)
     ap.add_argument("--lr", type=float, default=1e-3)
     return ap.parse_args()
 
@@ -244,26 +245,33 @@ def run_arms(a, ch, dist) -> dict:
     base.init(ch.initial_conserved())
     base.set_predictor(1)
     net = Network(ch.nx, ch.ny, ch.nz)
-    net.reserve_levels(a.collect)
+    net.reserve_levels(a.collect - a.skip)
     net.set_params(init_params(0))
-    host = []
+    # scales from the first and the last quadruple of the training levels
+    quads = sorted({a.skip, max(a.skip, a.collect - 4)})
+    keep = {k for q in quads for k in range(q, q + 4)}
+    host = {}
     t0 = time.perf_counter()
     for k in range(a.collect):
         base.step(None, a.drop, a.cap)
-        net.push_level(base)
-        if k >= a.collect - 6:
-            host.append(physical_levels(base, np.float32))
+        if k >= a.skip:
+            net.push_level(base)
+            if k in keep:
+                host[k] = physical_levels(base, np.float32)
     collect_s = time.perf_counter() - t0
-    net.set_scales(*scales_from_levels(host))
+    sc = [scales_from_levels([host[k] for k in range(q, q + 4)]) for q in quads]
+    net.set_scales(*[np.mean([x[i] for x in sc], axis=0) for i in range(3)])
     del host
     npairs = net.levels - 3
+    ntrain = max(1, npairs - 4)       # the last four pairs are held out
     t0 = time.perf_counter()
-    loss = net.train(a.train_steps, a.lr, 20261203, 0, npairs)
+    loss = net.train(a.train_steps, a.lr, 20261203, 0, ntrain)
     train_s = time.perf_counter() - t0
-    held = float(np.mean([net.pair_loss(p) for p in range(max(0, npairs - 4), npairs)]))
+    held = float(np.mean([net.pair_loss(p) for p in range(ntrain, npairs)]))
     out = {"common_point": f"after {a.collect} steps from the seeded field (mixed precision, extrapolated guess)",
-           "learned_guess": {"training_pairs": npairs, "adam_steps": a.train_steps, "lr": a.lr,
-                             "final_mean_loss": round(loss, 5), "last_pairs_loss": round(held, 5),
+           "learned_guess": {"training_pairs": ntrain, "training_steps_of_run": [a.skip, a.collect],
+                             "adam_steps": a.train_steps, "lr": a.lr,
+                             "final_mean_loss": round(loss, 5), "held_out_loss_last_4_pairs": round(held, 5),
                              "collect_s": round(collect_s, 2), "train_s": round(train_s, 2),
                              "loss_unit": "mean squared extrapolation correction / its RMS (1.0 = extrapolation)"}}
     sols = {}

@@ -204,4 +204,7 @@ WORKLOADS = {
     "c2": (256, 192, 192),
     "c3": (384, 256, 256),
     "c4": (256, 256, 128),
+    # profiling case: the channel at 160 x 128 x 128 cells (sweep data of one
+    # pass ~0.4 GB, larger than L2; ~3 GB on the device)
+    "p1": (160, 128, 128),
 }

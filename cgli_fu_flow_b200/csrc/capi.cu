@@ -296,11 +296,13 @@ int cgli_create(const cgli_params *p, cgli_ctx **out) {
         if (rc == CGLI_OK) rc = alloc(c, nsk * es, (void **)&a.mrf[v]);
         if (rc == CGLI_OK) rc = alloc(c, plane * es, (void **)&a.halo_ff[v]);
         if (rc == CGLI_OK) rc = alloc(c, plane * es, (void **)&a.halo_bf[v]);
+        if (rc == CGLI_OK) rc = alloc(c, plane * es, (void **)&a.hxpf[v]);
       } else {
         if (rc == CGLI_OK) rc = alloc(c, nsk * es, (void **)&a.dq[v]);
         if (rc == CGLI_OK) rc = alloc(c, nsk * es, (void **)&a.mrs[v]);
         if (rc == CGLI_OK) rc = alloc(c, plane * es, (void **)&a.halo_f[v]);
         if (rc == CGLI_OK) rc = alloc(c, plane * es, (void **)&a.halo_b[v]);
+        if (rc == CGLI_OK) rc = alloc(c, plane * es, (void **)&a.hxp[v]);
       }
     }
     for (int v = 0; v < cgli::REC_N; v++) {

@@ -27,6 +27,10 @@ struct SweepArgs {
   // (backward) and the records of planes 2 / ie+1
   double *halo_f[5], *halo_b[5], *hrec_f[REC_N], *hrec_b[REC_N];
   float *halo_ff[5], *halo_bf[5], *hrecf_f[REC_N], *hrecf_b[REC_N];
+  // the halo neighbour's product A.dQ of the current pass per (j, k), formed
+  // before the pass from the halo record and the lagged dQ
+  double *hxp[5];
+  float *hxpf[5];
   double *xbuf, *ybuf;            // products handed between tiles
   float *xbuff, *ybuff;
   unsigned int *ticket;           // tile ticket counter

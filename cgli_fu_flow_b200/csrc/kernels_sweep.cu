@@ -49,6 +49,7 @@ template <> struct SweepPtrs<double> {
   __device__ __forceinline__ static double *const *hrec(const SweepArgs &a, bool b) { return b ? a.hrec_b : a.hrec_f; }
   __device__ __forceinline__ static double *xb(const SweepArgs &a) { return a.xbuf; }
   __device__ __forceinline__ static double *yb(const SweepArgs &a) { return a.ybuf; }
+  __device__ __forceinline__ static double *const *hxp(const SweepArgs &a) { return a.hxp; }
 };
 template <> struct SweepPtrs<float> {
   __device__ __forceinline__ static float *const *dq(const SweepArgs &a) { return a.dqf; }
@@ -59,6 +60,7 @@ template <> struct SweepPtrs<float> {
   __device__ __forceinline__ static float *const *hrec(const SweepArgs &a, bool b) { return b ? a.hrecf_b : a.hrecf_f; }
   __device__ __forceinline__ static float *xb(const SweepArgs &a) { return a.xbuff; }
   __device__ __forceinline__ static float *yb(const SweepArgs &a) { return a.ybuff; }
+  __device__ __forceinline__ static float *const *hxp(const SweepArgs &a) { return a.hxpf; }
 };
 
 // face-direction metrics of a cell: general 3-D arrays, or a grid uniform in
@@ -140,22 +142,38 @@ __device__ __forceinline__ void fetch_cell(const Dev &d, const SweepArgs &a, con
 #pragma unroll
   for (int v = 0; v < 5; v++) x.mr[v] = BACKWARD ? SweepPtrs<T>::dq(a)[v][slot] : SweepPtrs<T>::mr(a)[v][slot];
   if (halo_edge) {
-    // periodic lagged halo: the x neighbour is plane 2 (forward) or ie+1
-    // (backward), a copy of plane ie / 3 made by the Q halo exchange; its
-    // record and the lagged dQ are kept per (j, k)
+    // periodic lagged halo: the x neighbour's product, formed before the
+    // pass (k_halo_products)
     const int kl = BACKWARD ? d.nz - 1 - rel : rel;
     const long long h = (long long)j * d.dj + 2 + kl;
-    T rn[REC_N], mm[9];
 #pragma unroll
-    for (int v = 0; v < REC_N; v++) rn[v] = SweepPtrs<T>::hrec(a, BACKWARD)[v][h];
-    Met::template dirs<T>(d, et, h + (BACKWARD ? (long long)(d.nx + 3) : 2LL) * d.di, jl, mm);
-    Split<T> An = split_from_record<T>(rn, 0, mm[0], mm[1], mm[2]);
-    T nh[5];
-#pragma unroll
-    for (int v = 0; v < 5; v++) nh[v] = BACKWARD ? SweepPtrs<T>::hb(a)[v][h] : SweepPtrs<T>::hf(a)[v][h];
-    if (BACKWARD) upper_terms<T>(An, nh, x.hx); else lower_terms<T>(An, nh, x.hx);
+    for (int v = 0; v < 5; v++) x.hx[v] = SweepPtrs<T>::hxp(a)[v][h];
     x.has_hx = true;
   }
+}
+
+// The x neighbour of the slab's first plane (forward) / last plane
+// (backward) is the periodic halo plane 2 / ie+1, a copy of plane ie / 3 made
+// by the Q halo exchange; its record and the lagged dQ are kept per (j, k).
+// Its product A+.dQ (forward) / A-.dQ (backward) is formed here once per
+// pass for every (j, k), off the wavefront's critical path.
+template <class Met, bool BACKWARD, typename T>
+__global__ void k_halo_products(Dev d, SweepArgs a) {
+  const int k = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 2 + blockIdx.y;
+  if (k > d.nz + 1) return;
+  const long long h = (long long)j * d.dj + k;
+  T rn[REC_N], mm[9];
+#pragma unroll
+  for (int v = 0; v < REC_N; v++) rn[v] = SweepPtrs<T>::hrec(a, BACKWARD)[v][h];
+  Met::template dirs<T>(d, a.etdytab, h + (BACKWARD ? (long long)(d.nx + 3) : 2LL) * d.di, j, mm);
+  Split<T> An = split_from_record<T>(rn, 0, mm[0], mm[1], mm[2]);
+  T nh[5], o[5];
+#pragma unroll
+  for (int v = 0; v < 5; v++) nh[v] = BACKWARD ? SweepPtrs<T>::hb(a)[v][h] : SweepPtrs<T>::hf(a)[v][h];
+  if (BACKWARD) upper_terms<T>(An, nh, o); else lower_terms<T>(An, nh, o);
+#pragma unroll
+  for (int v = 0; v < 5; v++) SweepPtrs<T>::hxp(a)[v][h] = o[v];
 }
 
 template <int TI, int TJ, class Met, bool BACKWARD, typename T>
@@ -396,8 +414,14 @@ static void run_sweeps(const Dev &d, const SweepArgs &a, cudaStream_t s) {
       cudaMemsetAsync(a.ticket, 0, sizeof(unsigned int), s);
       cudaMemsetAsync(xb, 0xff, xbytes, s);
       cudaMemsetAsync(yb, 0xff, ybytes, s);
-      if (pass == 0) k_sweep<TI, TJ, Met, false, T><<<ntiles, TI * TJ, 0, s>>>(d, f);
-      else k_sweep<TI, TJ, Met, true, T><<<ntiles, TI * TJ, 0, s>>>(d, b);
+      const dim3 hg((d.nz + 63) / 64, d.ny);
+      if (pass == 0) {
+        k_halo_products<Met, false, T><<<hg, 64, 0, s>>>(d, f);
+        k_sweep<TI, TJ, Met, false, T><<<ntiles, TI * TJ, 0, s>>>(d, f);
+      } else {
+        k_halo_products<Met, true, T><<<hg, 64, 0, s>>>(d, b);
+        k_sweep<TI, TJ, Met, true, T><<<ntiles, TI * TJ, 0, s>>>(d, b);
+      }
     }
   }
 }
@@ -413,8 +437,14 @@ static void run_one_pass(const Dev &d, const SweepArgs &a, cudaStream_t s, bool 
   cudaMemsetAsync(a.ticket, 0, sizeof(unsigned int), s);
   cudaMemsetAsync(xb, 0xff, xbytes, s);
   cudaMemsetAsync(yb, 0xff, ybytes, s);
-  if (!backward) k_sweep<TI, TJ, Met, false, T><<<ntiles, TI * TJ, 0, s>>>(d, b);
-  else k_sweep<TI, TJ, Met, true, T><<<ntiles, TI * TJ, 0, s>>>(d, b);
+  const dim3 hg((d.nz + 63) / 64, d.ny);
+  if (!backward) {
+    k_halo_products<Met, false, T><<<hg, 64, 0, s>>>(d, b);
+    k_sweep<TI, TJ, Met, false, T><<<ntiles, TI * TJ, 0, s>>>(d, b);
+  } else {
+    k_halo_products<Met, true, T><<<hg, 64, 0, s>>>(d, b);
+    k_sweep<TI, TJ, Met, true, T><<<ntiles, TI * TJ, 0, s>>>(d, b);
+  }
 }
 
 void launch_sweep_pass(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed, bool backward, bool final_pass) {

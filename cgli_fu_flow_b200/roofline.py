@@ -24,7 +24,7 @@ SWEEP_BYTES_PER_CELL = {"fp64": 25 * 8, "mixed": 25 * 4}
 # forward and backward averaged), on the 160x128x128 channel; traffic grows
 # with the cell count, so it is scaled to the benchmark grid.  See
 # profiles/k_sweep_channel_160x128x128.md.
-MEASURED_TRAFFIC_PER_CELL = {"fp64": None, "mixed": None}
+MEASURED_TRAFFIC_PER_CELL = {"fp64": (219.0 + 214.0) / 2, "mixed": None}
 
 
 def hbm_peak() -> tuple[float, str]:
