@@ -155,7 +155,7 @@ class Clocks:
 # ------------------------------------------------------------ GPU arm
 def run_gpu(a, dist: Dist) -> dict | None:
     from cgli_fu_flow_b200.solver import Solver, FP64, MIXED
-    ch = C.Channel(*C.WORKLOADS[a.workload])
+    ch = C.workload(a.workload)
     prec = FP64 if a.precision == "fp64" else MIXED
     sol = Solver(ch, prec)
     q0 = ch.initial_conserved()
@@ -372,7 +372,7 @@ def cpu_reference_sample(ch, iters: int, warm: int = 1) -> dict:
 def run_reference(a, dist: Dist) -> dict | None:
     if dist.rank != 0:
         return None
-    ch = C.Channel(*C.WORKLOADS[a.workload])
+    ch = C.workload(a.workload)
     lib = os.path.join(HERE, "oracle", "_ref", ch.name, "libref.so")
     if not os.path.exists(lib):
         return {"impl": "reference", "unavailable": f"reference build {lib} missing (build() compiles it where the "
@@ -415,7 +415,7 @@ def main():
         else:
             out = run_gpu(a, dist)
             if out is not None and not a.no_cpu_baseline and dist.world == 1:
-                ch = C.Channel(*C.WORKLOADS[a.workload])
+                ch = C.workload(a.workload)
                 lib = os.path.join(HERE, "oracle", "_ref", ch.name, "libref.so")
                 if os.path.exists(lib):
                     smp = cpu_reference_sample(ch, a.cpu_iters)

@@ -258,6 +258,7 @@ int cgli_create(const cgli_params *p, cgli_ctx **out) {
   d.dj = d.Z; d.di = (long long)d.Y * d.Z;
   d.dxi = p->dxi; d.det = p->det; d.dzt = p->dzt; d.dt = p->dt; d.e = p->e;
   d.mu = p->mu; d.pr = p->pr; d.twl = p->twall_lo; d.twh = p->twall_hi;
+  d.curved_walls = p->curved_walls ? 1 : 0;
   int rc = CGLI_OK;
 #define F(x) if (rc == CGLI_OK) rc = field(c, &(x))
   for (int v = 0; v < 5; v++) {
@@ -399,11 +400,26 @@ int cgli_get_array(cgli_ctx *c, const char *name, double *host) {
   return CGLI_OK;
 }
 
+static int upload_metrics(cgli_ctx *c, const cgli::MetricSet &M);
+
 int cgli_channel_metrics(cgli_ctx *c, double high, double stretch) {
   int rc = check(c); if (rc) return rc;
   if (!(high > 0 && stretch > 0)) return fail(CGLI_EINVAL, "high and stretch must be positive");
   cgli::MetricSet M;
   cgli::channel_metrics(c->p.nx, c->p.ny, c->p.nz, c->p.det, high, stretch, M);
+  return upload_metrics(c, M);
+}
+
+int cgli_wavy_channel_metrics(cgli_ctx *c, double high, double stretch, double amplitude) {
+  int rc = check(c); if (rc) return rc;
+  if (!(high > 0 && stretch > 0) || !(fabs(amplitude) < 0.5 * high))
+    return fail(CGLI_EINVAL, "need high, stretch > 0 and |amplitude| < high / 2");
+  cgli::MetricSet M;
+  cgli::wavy_metrics(c->p.nx, c->p.ny, c->p.nz, c->p.dxi, c->p.det, high, stretch, amplitude, M);
+  return upload_metrics(c, M);
+}
+
+static int upload_metrics(cgli_ctx *c, const cgli::MetricSet &M) {
   size_t n = (size_t)c->d.X * c->d.Y * c->d.Z;
   CUDA_TRY(cudaMemcpyAsync(c->d.J, M.J.data(), n * 8, cudaMemcpyHostToDevice, c->stream));
   for (int v = 0; v < 9; v++) CUDA_TRY(cudaMemcpyAsync(c->d.m[v], M.m[v].data(), n * 8, cudaMemcpyHostToDevice, c->stream));
@@ -638,12 +654,28 @@ int cgli_step(cgli_ctx *c, int fixed_iters, double drop, int cap, int *iters, do
   return rc;
 }
 
+static int copy_metric(const cgli::MetricSet &M, const char *name, double *out);
+
 int cgli_channel_metrics_host(int nx, int ny, int nz, double det, double high, double stretch,
                               const char *name, double *out) {
   if (!name || !out || nx < 1 || ny < 1 || nz < 1 || !(det > 0 && high > 0 && stretch > 0))
     return fail(CGLI_EINVAL, "bad argument");
   cgli::MetricSet M;
   cgli::channel_metrics(nx, ny, nz, det, high, stretch, M);
+  return copy_metric(M, name, out);
+}
+
+int cgli_wavy_channel_metrics_host(int nx, int ny, int nz, double dxi, double det, double high, double stretch,
+                                   double amplitude, const char *name, double *out) {
+  if (!name || !out || nx < 1 || ny < 1 || nz < 1 || !(dxi > 0 && det > 0 && high > 0 && stretch > 0) ||
+      !(fabs(amplitude) < 0.5 * high))
+    return fail(CGLI_EINVAL, "bad argument");
+  cgli::MetricSet M;
+  cgli::wavy_metrics(nx, ny, nz, dxi, det, high, stretch, amplitude, M);
+  return copy_metric(M, name, out);
+}
+
+static int copy_metric(const cgli::MetricSet &M, const char *name, double *out) {
   const std::vector<double> *src = nullptr;
   if (!strcmp(name, "J")) src = &M.J;
   const char *fs[3] = {"J_u", "J_v", "J_w"};

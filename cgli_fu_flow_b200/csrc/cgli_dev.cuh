@@ -22,6 +22,7 @@ struct Dev {
   int X, Y, Z;            // X_np, Y_m, Z_m
   long long di, dj;       // strides of i and j (k stride is 1)
   double dxi, det, dzt, dt, e, mu, pr, twl, twh;
+  int curved_walls;       // wall-face pressure force with eta_x, eta_z terms
   double *U_[5], *U[5], *Uq[5];
   double *Uqq[5];         // Q^(n-2)/J for the extrapolated initial guess
   double *J, *m[9];

@@ -9,6 +9,7 @@ struct MetricSet {
 };
 
 void channel_metrics(int nx, int ny, int nz, double det, double high, double g, MetricSet &M);
+void wavy_metrics(int nx, int ny, int nz, double dxi, double det, double high, double g, double amp, MetricSet &M);
 bool hyperplane(int nx, int ny, int nz, int *Nijk, long nijk_len, int *ijk, long ijk_len);
 
 }  // namespace cgli

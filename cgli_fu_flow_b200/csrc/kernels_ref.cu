@@ -110,6 +110,11 @@ __global__ void k_flux_y(Dev d) {
   if (j == 1 || j == jn) {
     F[0] = 0; F[1] = 0; F[3] = 0; F[4] = 0;
     F[2] = 0.5 * (ety * pp - 1. * fav3) / Jf;
+    if (d.curved_walls) {
+      // a curved wall also carries the x and z pressure force
+      F[1] = 0.5 * (d.mf[1][3][f] * pp) / Jf;
+      F[3] = 0.5 * (d.mf[1][5][f] * pp) / Jf;
+    }
   }
   for (int v = 0; v < 5; v++) d.inF[1][v][f] = F[v];
 }

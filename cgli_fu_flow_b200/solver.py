@@ -36,7 +36,7 @@ class Params(ctypes.Structure):
                 ("dt", ctypes.c_double), ("e", ctypes.c_double),
                 ("mu", ctypes.c_double), ("pr", ctypes.c_double),
                 ("twall_lo", ctypes.c_double), ("twall_hi", ctypes.c_double),
-                ("force", ctypes.c_double), ("precision", ctypes.c_int)]
+                ("force", ctypes.c_double), ("precision", ctypes.c_int), ("curved_walls", ctypes.c_int)]
 
 
 EXPORTS = [
@@ -51,7 +51,7 @@ EXPORTS = [
     "cgli_cnn_get_params", "cgli_cnn_set_scales", "cgli_cnn_forward_host", "cgli_cnn_loss_grad_host",
     "cgli_cnn_reserve_levels", "cgli_cnn_levels", "cgli_cnn_push_level_host", "cgli_cnn_push_level",
     "cgli_cnn_pair_loss", "cgli_cnn_train", "cgli_set_learned_guess", "cgli_step_norms",
-    "cgli_copy_state", "cgli_cnn_time_inference",
+    "cgli_copy_state", "cgli_cnn_time_inference", "cgli_wavy_channel_metrics", "cgli_wavy_channel_metrics_host",
 ]
 
 _lib = None
@@ -117,6 +117,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cgli_event_record.argtypes = [P, ctypes.c_int]
     L.cgli_event_elapsed.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
     L.cgli_channel_metrics_host.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, D, D, D, ctypes.c_char_p, P]
+    L.cgli_wavy_channel_metrics.argtypes = [P, D, D, D]
+    L.cgli_wavy_channel_metrics_host.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, D, D, D, D, D,
+                                                 ctypes.c_char_p, P]
     _lib = L
     return L
 
@@ -161,13 +164,17 @@ class Solver:
         self.shape = ch.shape
         self.n = int(np.prod(self.shape))
         p = Params(ch.nx, ch.ny, ch.nz, ch.dxi, ch.det, ch.dzt, ch.dt,
-                   C.PRECOND_EPS if e is None else e, C.MU0, C.PR, C.T0, C.T0, ch.force_lam, precision)
+                   C.PRECOND_EPS if e is None else e, C.MU0, C.PR, C.T0, C.T0, ch.force_lam, precision,
+                   int(ch.wavy))
         h = ctypes.c_void_p()
         self._rc(self.L.cgli_create(ctypes.byref(p), ctypes.byref(h)))
         self.h = h
         self.force = ch.force_lam
         self.ctrl: dict = {}
-        self._rc(self.L.cgli_channel_metrics(self.h, ch.high, C.STRETCH))
+        if ch.wavy:
+            self._rc(self.L.cgli_wavy_channel_metrics(self.h, ch.high, C.STRETCH, ch.amplitude))
+        else:
+            self._rc(self.L.cgli_channel_metrics(self.h, ch.high, C.STRETCH))
 
     def _rc(self, rc: int) -> None:
         if rc != 0:
@@ -340,12 +347,21 @@ def hyperplane_lists(nx: int, ny: int, nz: int):
     return nijk, ijk
 
 
+METRIC_NAMES = ["J", "J_u", "J_v", "J_w"] + [m + s for m in ("xidx", "xidy", "xidz", "etdx", "etdy", "etdz",
+                                                               "ztdx", "ztdy", "ztdz") for s in ("", "_u", "_v", "_w")]
+
+
 def channel_metric_host(ch: C.Channel, name: str) -> np.ndarray:
-    """One metric array from the library's host-side generator (no GPU)."""
+    """One metric array from the library's host-side generator (no GPU):
+    the reference's channel metrics, or the wavy-wall ones for ch.wavy."""
     L = load_library()
     out = np.empty(ch.shape)
-    rc = L.cgli_channel_metrics_host(ch.nx, ch.ny, ch.nz, ch.det, ch.high, C.STRETCH, name.encode(),
-                                     out.ctypes.data)
+    if ch.wavy:
+        rc = L.cgli_wavy_channel_metrics_host(ch.nx, ch.ny, ch.nz, ch.dxi, ch.det, ch.high, C.STRETCH, ch.amplitude,
+                                              name.encode(), out.ctypes.data)
+    else:
+        rc = L.cgli_channel_metrics_host(ch.nx, ch.ny, ch.nz, ch.det, ch.high, C.STRETCH, name.encode(),
+                                         out.ctypes.data)
     if rc:
         raise CgliError(rc, L.cgli_last_error().decode())
     return out

@@ -48,6 +48,10 @@ typedef struct cgli_params {
   double twall_lo, twall_hi; /* wall temperatures (Y_boundary_condition.cpp:139,166) */
   double force;            /* uniform x body force (replaces Dual_time_stepping.cpp:831) */
   int precision;           /* CGLI_FP64 or CGLI_MIXED */
+  int curved_walls;        /* 0: the wall-face flux of Flux_Y.cpp:400-408 (flat walls);
+                            * 1: plus the x and z components of the wall pressure
+                            * force, 0.5 (eta_x, eta_z) (p_L + p_R) / J_v, which
+                            * flat walls do not have (identical for flat walls) */
 } cgli_params;
 
 typedef struct cgli_ctx cgli_ctx;
@@ -77,6 +81,17 @@ int cgli_channel_metrics(cgli_ctx *ctx, double high, double stretch);
  * Nx x Ny x Nz slab into `out` (X_np*Y_m*Z_m doubles). */
 int cgli_channel_metrics_host(int nx, int ny, int nz, double det, double high, double stretch,
                               const char *name, double *out);
+/* Curvilinear metrics of a channel with a wavy lower wall (no reference
+ * code: the workload that exercises every metric term).  Mapping x = xi,
+ * z = zeta, y = yw(x) + (high - yw(x)) Y0(eta) / high with the tanh
+ * clustering Y0 of cgli_channel_metrics and yw(x) = amplitude sin(4 pi x /
+ * Lx), Lx = Nx * deltaXI; J = 1 / y_eta, etdx = -y_xi / y_eta,
+ * etdy = 1 / y_eta, xidx = ztdz = 1, other terms zero, at the cell and face
+ * positions and with the ghost rules of the channel generator.
+ * |amplitude| < high / 2. */
+int cgli_wavy_channel_metrics(cgli_ctx *ctx, double high, double stretch, double amplitude);
+int cgli_wavy_channel_metrics_host(int nx, int ny, int nz, double dxi, double det, double high, double stretch,
+                                   double amplitude, const char *name, double *out);
 
 /* Sets Q^(n+1,m) (U_), Q^n (U) and Q^(n-1) (Uq), 5 arrays each, in the
  * reference layout (Initial_condition.cpp:111-236 and main.cpp:127-141). */

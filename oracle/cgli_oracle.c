@@ -44,6 +44,7 @@ typedef struct {
   double mu, pr;           /* mu_L, Pr_L */
   double twall_lo, twall_hi;
   double force;            /* uniform x body force replacing Dual_time_stepping.cpp:831 */
+  int curved_walls;        /* 1: wall-face momentum flux with the eta_x, eta_z pressure terms */
 } or_params;
 
 typedef struct {
@@ -483,6 +484,12 @@ void or_flux_y(or_state *s) {
         if (j == 1 || j == jn) {
           F[0] = 0; F[1] = 0; F[3] = 0; F[4] = 0;
           F[2] = 0.5 * (mf[4][f] * pp - 1. * Fav3) / s->Jf[1][f];
+          /* Flux_Y.cpp:400-408 assumes flat walls (eta_x = eta_z = 0): a
+           * curved wall also carries the x and z pressure force */
+          if (s->p.curved_walls) {
+            F[1] = 0.5 * (mf[3][f] * pp) / s->Jf[1][f];
+            F[3] = 0.5 * (mf[5][f] * pp) / s->Jf[1][f];
+          }
         }
         for (int v = 0; v < 5; v++) s->inF[1][v][f] = F[v];
       }

@@ -30,7 +30,7 @@ class _Params(ctypes.Structure):
                 ("dt", ctypes.c_double), ("e", ctypes.c_double),
                 ("mu", ctypes.c_double), ("pr", ctypes.c_double),
                 ("twall_lo", ctypes.c_double), ("twall_hi", ctypes.c_double),
-                ("force", ctypes.c_double)]
+                ("force", ctypes.c_double), ("curved_walls", ctypes.c_int)]
 
 
 _lib = None
@@ -59,21 +59,33 @@ def _load():
     return _lib
 
 
+def load_wavy_metrics(array, ch) -> None:
+    """Overwrites the 40 metric arrays with the wavy-wall workload's (the
+    workload definition, generated once on the host and fed to the oracle,
+    the reference build and the GPU path alike)."""
+    from cgli_fu_flow_b200.solver import METRIC_NAMES, channel_metric_host
+    for name in METRIC_NAMES:
+        array(name)[...] = channel_metric_host(ch, name)
+
+
 class Oracle:
     """CPU restatement of one slab of the reference solver for one workload."""
 
-    def __init__(self, ch, e: float | None = None):
+    def __init__(self, ch, e: float | None = None, curved_walls: bool | None = None):
         from cgli_fu_flow_b200 import channel as C
         self.C = C
         self.ch = ch
         self.L = _load()
         p = _Params(ch.nx, ch.ny, ch.nz, ch.dxi, ch.det, ch.dzt, ch.dt,
-                    C.PRECOND_EPS if e is None else e, C.MU0, C.PR, C.T0, C.T0, ch.force_lam)
+                    C.PRECOND_EPS if e is None else e, C.MU0, C.PR, C.T0, C.T0, ch.force_lam,
+                    int(ch.wavy if curved_walls is None else curved_walls))
         self.s = self.L.or_create(ctypes.byref(p))
         self.shape = ch.shape
         self.force = ch.force_lam
         self.ctrl = {}
         self.L.or_metrics(self.s, ch.high, C.STRETCH)
+        if ch.wavy:
+            load_wavy_metrics(self.array, ch)
 
     def __del__(self):
         if getattr(self, "s", None):

@@ -152,7 +152,8 @@ long ref_check_hyperplanes() {
 
 /* main.cpp:87-141: allocation, metrics, hyperplanes, initial condition read
  * from a restart file in the layout of Initial_condition.cpp:136-221 */
-int ref_init(const char *initial_path, double deltaT, double e) {
+/* arrays, hyperplane lists and the reference's metrics */
+int ref_setup(double deltaT, double e) {
   X_np = X_out / 3 + 6;
   if (!allocated) {
     for (int v = 0; v < 5; v++) {
@@ -178,6 +179,11 @@ int ref_init(const char *initial_path, double deltaT, double e) {
   Jacobian_v(MYID, A.Jv, mv[0], mv[1], mv[2], mv[3], mv[4], mv[5], mv[6], mv[7], mv[8],
              A.J, m[0], m[1], m[2], m[3], m[4], m[5], m[6], m[7], m[8]);
   Jacobian_w(MYID, A.Jw, mw[0], mw[1], mw[2], mw[3], mw[4], mw[5], mw[6], mw[7], mw[8]);
+  return 0;
+}
+
+/* the initial field through the reference's restart reader (uses J) */
+int ref_load(const char *initial_path) {
   int sw = 0;
   if (initial_path && initial_path[0]) {
     strncpy(cgli_stub_initial_path, initial_path, sizeof(cgli_stub_initial_path) - 1);
@@ -192,6 +198,11 @@ int ref_init(const char *initial_path, double deltaT, double e) {
       for (int k = 2; k < nzz; k++)
         for (int v = 0; v < 5; v++) A.U_[v][i][j][k] = A.U[v][i][j][k];
   return 0;
+}
+
+int ref_init(const char *initial_path, double deltaT, double e) {
+  ref_setup(deltaT, e);
+  return ref_load(initial_path);
 }
 
 void ref_set_force(double f) { cgli_ref_force = f; }

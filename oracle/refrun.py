@@ -32,6 +32,8 @@ class RefSolver:
         L.ref_array.restype = ctypes.POINTER(ctypes.c_double)
         L.ref_array.argtypes = [ctypes.c_char_p]
         L.ref_init.argtypes = [ctypes.c_char_p, ctypes.c_double, ctypes.c_double]
+        L.ref_setup.argtypes = [ctypes.c_double, ctypes.c_double]
+        L.ref_load.argtypes = [ctypes.c_char_p]
         L.ref_set_force.argtypes = [ctypes.c_double]
         L.ref_bulk_flux.restype = ctypes.c_double
         L.ref_check_hyperplanes.restype = ctypes.c_long
@@ -57,7 +59,11 @@ class RefSolver:
         with tempfile.TemporaryDirectory() as td:
             path = os.path.join(td, "initial.bin")
             ch.write_restart(path, q_n, q_nm1)
-            self.lib.ref_init(path.encode(), ch.dt, _c().PRECOND_EPS)
+            self.lib.ref_setup(ch.dt, _c().PRECOND_EPS)
+            if ch.wavy:
+                from .oracle import load_wavy_metrics
+                load_wavy_metrics(self.array, ch)
+            self.lib.ref_load(path.encode())
         self.lib.ref_set_force(self.force)
 
     def array(self, name: str) -> np.ndarray:
