@@ -65,6 +65,9 @@ def parse():
     ap.add_argument("--skip", type=int, default=16, help="first steps (initial transient) not used for training")
     ap.add_argument("--train-steps", type=int, default=600)
     ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--profile-check", type=int, default=0, metavar="STEPS",
+                    help="instead of timing: run FP64 and mixed STEPS steps each and compare the mean streamwise "
+                         "velocity profiles over x, z and the steps (the configs[2] criterion, 0.5 %%)")
     return ap.parse_args()
 
 
@@ -406,9 +409,45 @@ def run_reference(a, dist: Dist) -> dict | None:
                     "d2h_bytes_per_step": 0}}
 
 
+def run_profile_check(a) -> dict:
+    """Mean streamwise velocity profile of mixed precision against FP64 on
+    the same workload (each from the seeded field, same stopping rule), and
+    the final states' relative L2 difference."""
+    from cgli_fu_flow_b200.solver import FP64, MIXED, Solver
+    ch = C.workload(a.workload)
+    prof, q, iters, secs = {}, {}, {}, {}
+    for name, prec in (("fp64", FP64), ("mixed", MIXED)):
+        g = Solver(ch, prec)
+        g.init()
+        it = []
+        t0 = time.perf_counter()
+        for _ in range(a.profile_check):
+            n, _ = g.step(None, a.drop, a.cap)
+            it.append(n)
+            g.accumulate_statistics()
+        secs[name] = time.perf_counter() - t0
+        prof[name] = g.mean_profiles()["U"]
+        sl = (slice(None), slice(3, ch.nx + 3), slice(2, ch.ny + 2), slice(2, ch.nz + 2))
+        q[name] = g.q()[sl]
+        iters[name] = float(np.mean(it))
+        g.close()
+    diff = float(np.abs(prof["mixed"] - prof["fp64"]).max() / ch.u_b)
+    rel = [float(np.linalg.norm(q["mixed"][v] - q["fp64"][v]) / np.linalg.norm(q["fp64"][v])) for v in range(5)]
+    return {"check": "mean streamwise velocity profile over x, z and steps: mixed vs FP64",
+            "workload": f"channel {ch.nx}x{ch.ny}x{ch.nz}", "steps": a.profile_check,
+            "max_profile_difference_over_u_b": diff, "criterion": 0.005, "passed": diff <= 0.005,
+            "state_rel_l2_mixed_vs_fp64": rel, "mean_inner_iterations": iters, "wall_s": secs,
+            "profile_fp64": [round(float(x), 6) for x in prof["fp64"]]}
+
+
 def main():
     a = parse()
     dist = Dist()
+    if a.profile_check:
+        if dist.rank == 0:
+            print(json.dumps(run_profile_check(a)), flush=True)
+        dist.close()
+        return
     try:
         if a.impl == "reference":
             out = run_reference(a, dist)

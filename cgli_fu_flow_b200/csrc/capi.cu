@@ -65,6 +65,8 @@ struct cgli_ctx {
   int predictor = 0;                  // 0 previous level, 1 extrapolation, 2 learned
   cgli_cnn *cnn = nullptr;            // learned initial guess (not owned)
   std::vector<double> step_norms;     // the five norms of every inner iteration of the last step
+  double *stats = nullptr;            // [11][nx][ny] running sums (allocated on first use)
+  long long stat_samples = 0;
   cgli::FilterBufs fb;                // allocated on first use of the filter
   bool have_filter = false, have_ypoint = false;
 };
@@ -159,9 +161,13 @@ int check(cgli_ctx *c) {
   return CGLI_OK;
 }
 
+int check_channel_metrics(cgli_ctx *c);
+
 int need_ready(cgli_ctx *c) {
   if (!c->have_metrics) return fail(CGLI_ESTATE, "metrics not set (cgli_channel_metrics / cgli_set_array)");
   if (!c->have_state) return fail(CGLI_ESTATE, "state not set (cgli_set_state)");
+  // quantities derived from the metrics (1/J, the channel tables), once per change
+  if (!c->metrics_checked) { int rc = check_channel_metrics(c); if (rc) return rc; }
   return CGLI_OK;
 }
 
@@ -225,6 +231,8 @@ int check_channel_metrics(cgli_ctx *c) {
     CUDA_TRY(cudaMemcpy((void *)c->sw.etdytab, et.data(), sizeof(double) * d.Y, cudaMemcpyHostToDevice));
   }
   c->sw.channel_metrics = ok ? 1 : 0;
+  cgli::launch_inverse_j(d, c->stream);
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
   c->metrics_checked = true;
   drop_graph(c);
   return CGLI_OK;
@@ -270,6 +278,7 @@ int cgli_create(const cgli_params *p, cgli_ctx **out) {
     for (int f = 0; f < 3; f++) F(d.vflux[f][v]);
   }
   F(d.J);
+  F(d.iJ);
   for (int v = 0; v < 9; v++) F(d.m[v]);
   for (int f = 0; f < 3; f++) {
     F(d.Jf[f]);
@@ -589,6 +598,41 @@ int cgli_step_norms(cgli_ctx *c, double *norms, int max_iters, int *iters) {
   const int n = (int)(c->step_norms.size() / 5);
   *iters = n;
   std::copy(c->step_norms.begin(), c->step_norms.begin() + 5 * std::min(n, max_iters), norms);
+  return CGLI_OK;
+}
+
+int cgli_statistics_accumulate(cgli_ctx *c) {
+  int rc = check(c); if (rc) return rc;
+  rc = need_ready(c); if (rc) return rc;
+  const size_t bytes = (size_t)11 * c->p.nx * c->p.ny * sizeof(double);
+  if (!c->stats) { rc = alloc(c, bytes, (void **)&c->stats); if (rc) return rc; }
+  cgli::launch_statistics(c->d, c->stream, c->stats);
+  rc = last_launch("statistics"); if (rc) return rc;
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->stat_samples++;
+  return CGLI_OK;
+}
+
+int cgli_statistics_get(cgli_ctx *c, double *sums, long long *samples) {
+  int rc = check(c); if (rc) return rc;
+  if (!sums || !samples) return fail(CGLI_EINVAL, "null argument");
+  const size_t bytes = (size_t)11 * c->p.nx * c->p.ny * sizeof(double);
+  if (!c->stats) memset(sums, 0, bytes);
+  else {
+    CUDA_TRY(cudaMemcpyAsync(sums, c->stats, bytes, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+  }
+  *samples = c->stat_samples;
+  return CGLI_OK;
+}
+
+int cgli_statistics_reset(cgli_ctx *c) {
+  int rc = check(c); if (rc) return rc;
+  if (c->stats) {
+    CUDA_TRY(cudaMemsetAsync(c->stats, 0, (size_t)11 * c->p.nx * c->p.ny * sizeof(double), c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+  }
+  c->stat_samples = 0;
   return CGLI_OK;
 }
 

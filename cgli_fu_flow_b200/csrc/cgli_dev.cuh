@@ -26,6 +26,7 @@ struct Dev {
   double *U_[5], *U[5], *Uq[5];
   double *Uqq[5];         // Q^(n-2)/J for the extrapolated initial guess
   double *J, *m[9];
+  double *iJ;             // 1/J per cell (0 where J = 0), formed when the metrics change
   double *Jf[3], *mf[3][9];
   double *inF[3][5], *vF[4];
   double *MR[5], *NL[5], *NR[5];
@@ -70,14 +71,14 @@ __device__ __forceinline__ double m2(const double *u, const double *J, long long
 }
 
 // One side of a face for all five variables: the weight
-// t = 1 / sum(c_p / J_p) is computed once and applied to each variable's
-// sum(c_p u_p) (the reference's m5L/m5R/m3L/m3R/m2 expressions, same
-// evaluation order).
+// t = 1 / sum(c_p / J_p) (c_p / J_p as c_p times the cell's stored 1/J) is
+// computed once and applied to each variable's sum(c_p u_p) (the reference's
+// m5L/m5R/m3L/m3R/m2 expressions, same evaluation order).
 template <int N>
 __device__ __forceinline__ void muscl_side(const Dev &d, const long long (&o)[N], const double (&c)[N], double out[5]) {
-  double s = c[0] / d.J[o[0]];
+  double s = c[0] * d.iJ[o[0]];
 #pragma unroll
-  for (int p = 1; p < N; p++) s += c[p] / d.J[o[p]];
+  for (int p = 1; p < N; p++) s += c[p] * d.iJ[o[p]];
   const double t = 1. / s;
 #pragma unroll
   for (int v = 0; v < 5; v++) {

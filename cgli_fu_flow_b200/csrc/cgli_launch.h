@@ -62,6 +62,11 @@ void launch_sweep_pass(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mi
 // residual assembly writing MR and the first sweep's lagged halo planes
 void launch_residual_fast(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed);
 
+// adds the per-(i, j) sums over k of Statistic.cpp:120-160 to sums
+// [11][nx][ny] (U, V, W, T, UU, VV, WW, TT, UV, UT, VT)
+void launch_statistics(const Dev &d, cudaStream_t s, double *sums);
+// d.iJ = 1/J on every cell (0 where J = 0)
+void launch_inverse_j(const Dev &d, cudaStream_t s);
 void launch_halo_bc(const Dev &d, cudaStream_t s);
 void launch_halo_x(const Dev &d, cudaStream_t s);
 void launch_bc_y(const Dev &d, cudaStream_t s);

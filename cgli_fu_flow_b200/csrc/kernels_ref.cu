@@ -532,6 +532,14 @@ void launch_predict(const Dev &d, cudaStream_t s, int order) {
 void launch_norms(const Dev &d, cudaStream_t s, int nblocks, double scale, double *out) {
   k_norms<<<1, 1024, 0, s>>>(d.partial, nblocks, scale, out);
 }
+__global__ void k_inverse_j(Dev d, long long n) {
+  const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (c < n) d.iJ[c] = d.J[c] != 0.0 ? 1.0 / d.J[c] : 0.0;
+}
+void launch_inverse_j(const Dev &d, cudaStream_t s) {
+  const long long n = (long long)d.X * d.Y * d.Z;
+  k_inverse_j<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(d, n);
+}
 void launch_bulk_flux(const Dev &d, cudaStream_t s, double *out) {
   // the per-block partials go to out[8 ..]: the caller's scratch holds 8 + 296 doubles
   constexpr int kBlocks = 296;

@@ -52,6 +52,7 @@ EXPORTS = [
     "cgli_cnn_reserve_levels", "cgli_cnn_levels", "cgli_cnn_push_level_host", "cgli_cnn_push_level",
     "cgli_cnn_pair_loss", "cgli_cnn_train", "cgli_set_learned_guess", "cgli_step_norms",
     "cgli_copy_state", "cgli_cnn_time_inference", "cgli_wavy_channel_metrics", "cgli_wavy_channel_metrics_host",
+    "cgli_statistics_accumulate", "cgli_statistics_get", "cgli_statistics_reset",
 ]
 
 _lib = None
@@ -112,6 +113,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cgli_set_learned_guess.argtypes = [P, P]
     L.cgli_step_norms.argtypes = [P, P, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     L.cgli_copy_state.argtypes = [P, P]
+    L.cgli_statistics_accumulate.argtypes = [P]
+    L.cgli_statistics_get.argtypes = [P, P, ctypes.POINTER(ctypes.c_longlong)]
+    L.cgli_statistics_reset.argtypes = [P]
     L.cgli_cnn_time_inference.argtypes = [P, P, ctypes.c_int, FP]
     L.cgli_update_norms_noalloc.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P, DP, P]
     L.cgli_event_record.argtypes = [P, ctypes.c_int]
@@ -294,6 +298,29 @@ class Solver:
         """0: previous time level (reference); 1: second-order extrapolation;
         2: extrapolation plus the learned correction (set_learned_guess)."""
         self._rc(self.L.cgli_set_predictor(self.h, mode))
+
+    STATS = ("U", "V", "W", "T", "UU", "VV", "WW", "TT", "UV", "UT", "VT")
+
+    def accumulate_statistics(self) -> None:
+        """Adds the current level to the running sums (Statistic.cpp:120-160)."""
+        self._rc(self.L.cgli_statistics_accumulate(self.h))
+
+    def statistics(self) -> tuple[np.ndarray, int]:
+        """The running sums (11, Nx, Ny) and the number of accumulated steps."""
+        out = np.zeros((11, self.ch.nx, self.ch.ny))
+        n = ctypes.c_longlong()
+        self._rc(self.L.cgli_statistics_get(self.h, out.ctypes.data, ctypes.byref(n)))
+        return out, int(n.value)
+
+    def reset_statistics(self) -> None:
+        self._rc(self.L.cgli_statistics_reset(self.h))
+
+    def mean_profiles(self) -> dict:
+        """Means over x, z and the accumulated steps, per wall-normal cell:
+        the reference's (i, j) means (sums / (steps Nz)) averaged over i."""
+        sums, n = self.statistics()
+        m = sums.mean(axis=1) / (max(n, 1) * self.ch.nz)
+        return dict(zip(self.STATS, m))
 
     def copy_state_from(self, other: "Solver") -> None:
         """Continue `other`'s run from its current point (levels, force and

@@ -196,6 +196,16 @@ int cgli_cnn_time_inference(cgli_cnn *cnn, cgli_ctx *ctx, int reps, float *ms);
 /* use the network for predictor mode 2 (null detaches it) */
 int cgli_set_learned_guess(cgli_ctx *ctx, cgli_cnn *cnn);
 
+/* ---- running statistics (replaces the accumulation of Statistic.cpp:120-160).
+ * Each call adds, for every interior (i, j), the sums over k of U, V, W, T,
+ * UU, VV, WW, TT, UV, UT, VT of the current U_ (call after each cgli_step);
+ * cgli_statistics_get copies the sums [11][Nx][Ny] (quantity-major, i then j)
+ * and the number of accumulated calls; the reference's means are the sums
+ * divided by calls * Nz (Statistic.cpp:162-190). */
+int cgli_statistics_accumulate(cgli_ctx *ctx);
+int cgli_statistics_get(cgli_ctx *ctx, double *sums, long long *samples);
+int cgli_statistics_reset(cgli_ctx *ctx);
+
 /* ---- high-order filter sensor (replaces Filter(myid, Roe_criterion, E_high,
  * E_low, U1_..U5_, Y_point, EpX, EpY, EpZ, J), Filter.cpp:12-1720, prototype
  * main.h:948-974).  Reads U_ as stored (ghost planes included, like the

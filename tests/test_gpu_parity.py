@@ -281,3 +281,44 @@ def test_wavy_wall_specified_amplitude_first_step(lib):
     sl = (slice(None),) + regions(ch)["cell"]
     qg, qo = g.q()[sl], o.q()[sl]
     assert max(rel_l2(qg[v], qo[v]) for v in range(5)) <= 1e-12
+
+
+def test_statistics_match_restatement(lib):
+    """Running sums of Statistic.cpp:120-160 over three steps against the
+    numpy restatement applied to the same converged levels."""
+    from cgli_fu_flow_b200.solver import Solver
+    from oracle.stats_oracle import sums
+    ch = Channel(10, 12, 8)
+    g = Solver(ch)
+    g.init()
+    J = g.get("J")
+    want = np.zeros((11, ch.nx, ch.ny))
+    for _ in range(3):
+        g.step(6)
+        g.accumulate_statistics()
+        want += sums(g.q(), J, ch.nx, ch.ny, ch.nz)
+    got, n = g.statistics()
+    assert n == 3
+    assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max()
+    g.reset_statistics()
+    assert g.statistics()[1] == 0 and not g.statistics()[0].any()
+
+
+def test_mixed_mean_velocity_profile_within_half_percent(lib):
+    """The configs[2] criterion on a small channel: the mean streamwise
+    velocity profile over x, z and the steps of the mixed path agrees with
+    the FP64 path's within 0.5 % (max over the wall-normal cells, relative to
+    the bulk velocity)."""
+    from cgli_fu_flow_b200.solver import Solver, MIXED
+    ch = Channel(16, 24, 32)
+    prof = []
+    for prec in (0, MIXED):
+        g = Solver(ch, prec)
+        g.init()
+        for _ in range(30):
+            g.step(None, 1e-3, 30)
+            g.accumulate_statistics()
+        prof.append(g.mean_profiles()["U"])
+    diff = np.abs(prof[1] - prof[0]).max() / ch.u_b
+    print("mean U profile, mixed vs FP64, max difference / U_b:", diff)
+    assert diff <= 5e-3
