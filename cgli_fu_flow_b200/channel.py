@@ -195,17 +195,18 @@ class Channel:
         vv = u * u + v * v + w * w
         return np.stack([rho, rho * u, rho * v, rho * w, p / (GAMMA - 1) + 0.5 * rho * vv])
 
-    def write_restart(self, path: str, q_n: np.ndarray, q_nm1: np.ndarray, ranks: int = 3) -> None:
-        """Writes the reference restart layout for a run presented as rank 1
-        of `ranks` equal x-slabs: 10 fields [U1..U5 at n, U1..U5 at n-1],
-        each of ranks*Nx x Ny x Nz doubles, this slab at x-offset Nx."""
+    def write_restart(self, path: str, q_n: np.ndarray, q_nm1: np.ndarray, ranks: int = 3, rank: int = 1) -> None:
+        """Writes the reference restart layout for a run presented as rank
+        `rank` of `ranks` equal x-slabs: 10 fields [U1..U5 at n, U1..U5 at
+        n-1], each of ranks*Nx x Ny x Nz doubles, this slab at x-offset
+        rank*Nx."""
         nx, ny, nz = self.nx, self.ny, self.nz
         field = ranks * nx * ny * nz * 8
         with open(path, "wb") as fh:
-            fh.truncate(10 * field)          # sparse: only this slab's third is written
+            fh.truncate(10 * field)          # sparse: only this slab's part is written
             for f in range(10):
                 q = q_n if f < 5 else q_nm1
-                fh.seek(f * field + nx * ny * nz * 8)
+                fh.seek(f * field + rank * nx * ny * nz * 8)
                 fh.write(np.ascontiguousarray(q[f % 5], dtype=np.float64).tobytes())
 
 

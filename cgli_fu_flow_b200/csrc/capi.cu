@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdint>
+#include <sys/types.h>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -482,6 +484,141 @@ int cgli_copy_state(cgli_ctx *dst, const cgli_ctx *src) {
   dst->history = src->history;
   dst->have_state = true;
   return CGLI_OK;
+}
+
+// ---------------------------------------------------------------- restart
+// Field f (0..4: Q^n = U*J, 5..9: Q^(n-1) = Uq*J) of the slab occupies
+// [x_offset, x_offset + Nx) of a global x extent, k fastest: the MPI-IO
+// layout of Output.cpp:187-284 / Initial_condition.cpp:111-236.
+static int restart_io(cgli_ctx *c, const char *path, int global_nx, int x_offset, bool write) {
+  const int nx = c->p.nx, ny = c->p.ny, nz = c->p.nz;
+  if (!path) return fail(CGLI_EINVAL, "null path");
+  if (global_nx < nx || x_offset < 0 || x_offset + nx > global_nx)
+    return fail(CGLI_EINVAL, "slab [x_offset, x_offset + Nx) must lie in [0, global_nx)");
+  const cgli::Dev &d = c->d;
+  const size_t n = (size_t)d.X * d.Y * d.Z, cells = (size_t)nx * ny * nz;
+  std::vector<double> J(n), a(n), buf(cells);
+  CUDA_TRY(cudaMemcpy(J.data(), d.J, n * 8, cudaMemcpyDeviceToHost));
+  FILE *f = write ? fopen(path, "r+b") : fopen(path, "rb");
+  if (!f && write) f = fopen(path, "w+b");
+  if (!f) return fail(CGLI_EINVAL, std::string("cannot open ") + path);
+  std::vector<double> U[10];
+  if (!write) {
+    // Initial_condition.cpp:56-103: the quiescent state on every row of the
+    // interior planes, as Q/J (x ghost planes stay zero)
+    const double T = 298.0592, P = 101300, rho = P / T / cgli::RG, vel = 0, VV = 0;
+    const double q[5] = {rho, rho * vel, rho * vel, rho * vel, P / (cgli::KG - 1) + 0.5 * rho * VV};
+    for (int f2 = 0; f2 < 10; f2++) {
+      U[f2].assign(n, 0.0);
+      for (int i = 3; i <= nx + 2; i++)
+        for (int j = 0; j < d.Y; j++)
+          for (int k = 0; k < d.Z; k++) {
+            const size_t cc = cgli::ix(d, i, j, k);
+            U[f2][cc] = q[f2 % 5] / J[cc];
+          }
+    }
+  }
+  int rc = CGLI_OK;
+  for (int fld = 0; fld < 10 && rc == CGLI_OK; fld++) {
+    const long long off = ((long long)fld * global_nx + x_offset) * (long long)ny * nz * 8;
+    if (fseeko(f, (off_t)off, SEEK_SET)) { rc = fail(CGLI_EINVAL, "seek failed"); break; }
+    if (write) {
+      double *src = fld < 5 ? d.U[fld] : d.Uq[fld - 5];
+      if (cudaMemcpy(a.data(), src, n * 8, cudaMemcpyDeviceToHost) != cudaSuccess) { rc = fail(CGLI_ECUDA, "copy"); break; }
+      for (int i = 0; i < nx; i++)
+        for (int j = 0; j < ny; j++)
+          for (int k = 0; k < nz; k++) {
+            const size_t cc = cgli::ix(d, i + 3, j + 2, k + 2);
+            buf[((size_t)i * ny + j) * nz + k] = a[cc] * J[cc];
+          }
+      if (fwrite(buf.data(), 8, cells, f) != cells) rc = fail(CGLI_EINVAL, std::string("short write to ") + path);
+    } else {
+      if (fread(buf.data(), 8, cells, f) != cells) { rc = fail(CGLI_EINVAL, std::string("short read from ") + path); break; }
+      // Initial_condition.cpp:186-221
+      for (int i = 0; i < nx; i++)
+        for (int j = 0; j < ny; j++)
+          for (int k = 0; k < nz; k++) {
+            const size_t cc = cgli::ix(d, i + 3, j + 2, k + 2);
+            U[fld][cc] = buf[((size_t)i * ny + j) * nz + k] / J[cc];
+          }
+    }
+  }
+  if (fclose(f) && rc == CGLI_OK && write) rc = fail(CGLI_EINVAL, std::string("close failed: ") + path);
+  if (rc || write) return rc;
+  const double *Un[5], *U0[5], *Uq[5];
+  for (int v = 0; v < 5; v++) { Un[v] = U[v].data(); U0[v] = U[v].data(); Uq[v] = U[v + 5].data(); }
+  return cgli_set_state(c, Un, U0, Uq);   // U_ = U (main.cpp:127-141), Q^(n-2) = Q^(n-1)
+}
+
+int cgli_write_restart(cgli_ctx *c, const char *path, int global_nx, int x_offset) {
+  int rc = check(c); if (rc) return rc;
+  rc = need_ready(c); if (rc) return rc;
+  return restart_io(c, path, global_nx, x_offset, true);
+}
+
+int cgli_read_restart(cgli_ctx *c, const char *path, int global_nx, int x_offset) {
+  int rc = check(c); if (rc) return rc;
+  if (!c->have_metrics) return fail(CGLI_ESTATE, "metrics not set (the reader divides by J)");
+  return restart_io(c, path, global_nx, x_offset, false);
+}
+
+// sidecar of what the reference's file has no room for: the raw device
+// levels U_, U, Uq, Uqq (Q/J, ghost cells included, so the lagged ghost
+// values survive), the driving force, the norm maxima and the step history
+struct HistoryHeader {
+  char magic[8];
+  int32_t nx, ny, nz, history;
+  double force, emax[5];
+};
+
+int cgli_write_history(cgli_ctx *c, const char *path) {
+  int rc = check(c); if (rc) return rc;
+  rc = need_ready(c); if (rc) return rc;
+  if (!path) return fail(CGLI_EINVAL, "null path");
+  const cgli::Dev &d = c->d;
+  const size_t n = (size_t)d.X * d.Y * d.Z;
+  HistoryHeader h{};
+  memcpy(h.magic, "CGLIHST2", 8);
+  h.nx = c->p.nx; h.ny = c->p.ny; h.nz = c->p.nz; h.history = c->history; h.force = c->p.force;
+  for (int v = 0; v < 5; v++) h.emax[v] = c->Emax[v];
+  std::vector<double> a(n);
+  FILE *f = fopen(path, "wb");
+  if (!f) return fail(CGLI_EINVAL, std::string("cannot open ") + path);
+  bool ok = fwrite(&h, sizeof h, 1, f) == 1;
+  double *const *lv[4] = {d.U_, d.U, d.Uq, d.Uqq};
+  for (int l = 0; l < 4 && ok; l++)
+    for (int v = 0; v < 5 && ok; v++) {
+      ok = cudaMemcpy(a.data(), lv[l][v], n * 8, cudaMemcpyDeviceToHost) == cudaSuccess;
+      if (ok) ok = fwrite(a.data(), 8, n, f) == n;
+    }
+  if (fclose(f)) ok = false;
+  return ok ? CGLI_OK : fail(CGLI_EINVAL, std::string("write failed: ") + path);
+}
+
+int cgli_read_history(cgli_ctx *c, const char *path) {
+  int rc = check(c); if (rc) return rc;
+  rc = need_ready(c); if (rc) return rc;
+  if (!path) return fail(CGLI_EINVAL, "null path");
+  const cgli::Dev &d = c->d;
+  const size_t n = (size_t)d.X * d.Y * d.Z;
+  FILE *f = fopen(path, "rb");
+  if (!f) return fail(CGLI_EINVAL, std::string("cannot open ") + path);
+  HistoryHeader h{};
+  bool ok = fread(&h, sizeof h, 1, f) == 1 && !memcmp(h.magic, "CGLIHST2", 8) && h.nx == c->p.nx &&
+            h.ny == c->p.ny && h.nz == c->p.nz;
+  if (!ok) { fclose(f); return fail(CGLI_EINVAL, std::string("not a history file of this grid: ") + path); }
+  std::vector<double> a(n);
+  double *const *lv[4] = {d.U_, d.U, d.Uq, d.Uqq};
+  for (int l = 0; l < 4 && ok; l++)
+    for (int v = 0; v < 5 && ok; v++) {
+      ok = fread(a.data(), 8, n, f) == n;
+      if (ok) ok = cudaMemcpy(lv[l][v], a.data(), n * 8, cudaMemcpyHostToDevice) == cudaSuccess;
+    }
+  fclose(f);
+  if (!ok) return fail(CGLI_EINVAL, std::string("short read from ") + path);
+  c->history = h.history;
+  for (int v = 0; v < 5; v++) c->Emax[v] = h.emax[v];
+  return cgli_set_force(c, h.force);
 }
 
 int cgli_get_state(cgli_ctx *c, double *const U_[5]) {

@@ -53,6 +53,7 @@ EXPORTS = [
     "cgli_cnn_pair_loss", "cgli_cnn_train", "cgli_set_learned_guess", "cgli_step_norms",
     "cgli_copy_state", "cgli_cnn_time_inference", "cgli_wavy_channel_metrics", "cgli_wavy_channel_metrics_host",
     "cgli_statistics_accumulate", "cgli_statistics_get", "cgli_statistics_reset",
+    "cgli_write_restart", "cgli_read_restart", "cgli_write_history", "cgli_read_history",
 ]
 
 _lib = None
@@ -116,6 +117,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cgli_statistics_accumulate.argtypes = [P]
     L.cgli_statistics_get.argtypes = [P, P, ctypes.POINTER(ctypes.c_longlong)]
     L.cgli_statistics_reset.argtypes = [P]
+    L.cgli_write_restart.argtypes = [P, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
+    L.cgli_read_restart.argtypes = [P, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
+    L.cgli_write_history.argtypes = [P, ctypes.c_char_p]
+    L.cgli_read_history.argtypes = [P, ctypes.c_char_p]
     L.cgli_cnn_time_inference.argtypes = [P, P, ctypes.c_int, FP]
     L.cgli_update_norms_noalloc.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P, DP, P]
     L.cgli_event_record.argtypes = [P, ctypes.c_int]
@@ -298,6 +303,26 @@ class Solver:
         """0: previous time level (reference); 1: second-order extrapolation;
         2: extrapolation plus the learned correction (set_learned_guess)."""
         self._rc(self.L.cgli_set_predictor(self.h, mode))
+
+    def write_restart(self, path: str, global_nx: int | None = None, x_offset: int = 0,
+                      history: bool = True) -> None:
+        """The reference's LES%05d.bin layout (this slab of a global_nx-plane
+        file); with history, also `path + '.history'` (Q^(n-2), force, norm
+        maxima, step count)."""
+        self._rc(self.L.cgli_write_restart(self.h, path.encode(), global_nx or self.ch.nx, x_offset))
+        if history:
+            self._rc(self.L.cgli_write_history(self.h, (path + ".history").encode()))
+
+    def read_restart(self, path: str, global_nx: int | None = None, x_offset: int = 0,
+                     history: bool = True, ctrl: dict | None = None) -> None:
+        self._rc(self.L.cgli_read_restart(self.h, path.encode(), global_nx or self.ch.nx, x_offset))
+        if history:
+            self._rc(self.L.cgli_read_history(self.h, (path + ".history").encode()))
+            import struct
+            with open(path + ".history", "rb") as fh:
+                self.force = struct.unpack("<8s4i6d", fh.read(72))[5]
+        if ctrl is not None:
+            self.ctrl = dict(ctrl)
 
     STATS = ("U", "V", "W", "T", "UU", "VV", "WW", "TT", "UV", "UT", "VT")
 

@@ -99,6 +99,25 @@ int cgli_set_state(cgli_ctx *ctx, const double *const U_[5], const double *const
                    const double *const Uq[5]);
 /* Reads back Q^(n+1,m) (5 arrays). */
 int cgli_get_state(cgli_ctx *ctx, double *const U_[5]);
+/* ---- restart files in the reference's format.  cgli_write_restart writes
+ * Q^n = U*J and Q^(n-1) = Uq*J of this slab into `path` as Output.cpp:187-284
+ * lays out LES%05d.bin: ten fields, each spanning a global x extent of
+ * global_nx planes, this slab at planes [x_offset, x_offset + Nx), k fastest
+ * (single GPU: global_nx = Nx, x_offset = 0; one slab of a multi-slab file
+ * otherwise, the file is not truncated).  cgli_read_restart reads such a file
+ * as Initial_condition.cpp:56-236 does (quiescent state on the interior
+ * planes, then the slab's cells as Q/J; U_ = U) and acts as cgli_set_state.
+ * The metrics must be set first.  cgli_write_history / cgli_read_history keep
+ * what the reference format has no room for (no counterpart in the
+ * reference): the raw levels U_, U, Uq and Q^(n-2)/J with their ghost cells,
+ * the driving force, the running maxima of the norms and the step history;
+ * reading the sidecar after the file continues the run bit for bit (the
+ * file alone loses the lagged ghost values and the rounding of Q = U*J). */
+int cgli_write_restart(cgli_ctx *ctx, const char *path, int global_nx, int x_offset);
+int cgli_read_restart(cgli_ctx *ctx, const char *path, int global_nx, int x_offset);
+int cgli_write_history(cgli_ctx *ctx, const char *path);
+int cgli_read_history(cgli_ctx *ctx, const char *path);
+
 /* Copies the time levels (U_, U, Uq, Q^(n-2)), the driving force, the
  * running maxima of the norms and the step history of `src` into `dst`
  * (device to device; same grid, any precision), so that several contexts

@@ -66,6 +66,17 @@ class RefSolver:
             self.lib.ref_load(path.encode())
         self.lib.ref_set_force(self.force)
 
+    def load(self, path: str) -> None:
+        """Set-up, then the initial field read from a restart file written
+        elsewhere (the reference's own reader, Initial_condition.cpp:111-236)."""
+        ch = self.ch
+        self.lib.ref_setup(ch.dt, _c().PRECOND_EPS)
+        if ch.wavy:
+            from .oracle import load_wavy_metrics
+            load_wavy_metrics(self.array, ch)
+        self.lib.ref_load(path.encode())
+        self.lib.ref_set_force(self.force)
+
     def array(self, name: str) -> np.ndarray:
         """A live view of one reference array, shape (X_np, Y_m, Z_m)."""
         p = self.lib.ref_array(name.encode())
