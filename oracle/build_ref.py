@@ -44,7 +44,7 @@ SOURCES = [
     "Initial_condition.cpp", "X_boundary_condition.cpp", "Y_boundary_condition.cpp",
     "Z_boundary_condition.cpp", "Flux_X.cpp", "Flux_Y.cpp", "Flux_Z.cpp",
     "Viscous_terms.cpp", "Dual_time_stepping.cpp", "Driven_force.cpp", "Hyperplane.cpp",
-    "Filter.cpp",
+    "Filter.cpp", "DPLUSGS.cpp",
 ]
 
 PATCHES = {
@@ -56,6 +56,16 @@ PATCHES = {
                                  ("T = 298.0592;", "T = CGLI_TWALL_HI;", 1)],
     "Dual_time_stepping.cpp": [("f = -(rho-1.1842)*9.81;", "f = cgli_ref_force;", 1),
                                ("void Dual_time_stepping", "extern double cgli_ref_force;\nvoid Dual_time_stepping", 1)],
+    # DPLUSGS.cpp reads the constant f of prm.h (included in its body); the
+    # harness gives it the same driving force as Dual_time_stepping.  Its
+    # relaxation loop never assigns j_ and k_ (ijk.h declares them, the
+    # OpenMP clause makes them private and uninitialised), so the upper y / z
+    # terms would read NL at indeterminate rows; the loop header sets them to
+    # j+1 and k+1, the neighbours whose state the same terms use.
+    "DPLUSGS.cpp": [("for (k = 2, _k = 1; k < nzz; k++, _k++) {",
+                     "for (k = 2, _k = 1, j_ = j + 1, k_ = 3; k < nzz; k++, _k++, k_++) {", 2),("+f/J[i][j][k];", "+cgli_ref_force/J[i][j][k];", 1),
+                    ("+f*u/J[i][j][k];", "+cgli_ref_force*u/J[i][j][k];", 1),
+                    ("void DPLUSGS", "extern double cgli_ref_force;\nvoid DPLUSGS", 1)],
     "Flux_Y.cpp": [("deltaP*XIx;", "deltaP*ETx;", 1), ("deltaP*XIy;", "deltaP*ETy;", 1),
                    ("deltaP*XIz;", "deltaP*ETz;", 1)],
     "Flux_Z.cpp": [("deltaP*XIx;", "deltaP*ZTx;", 1), ("deltaP*XIy;", "deltaP*ZTy;", 1),

@@ -1052,6 +1052,148 @@ void or_update(or_state *s, double *er) {
   er[3] = sqrt(e4) * DN; er[4] = sqrt(e5) * DN;
 }
 
+/* ------------------------------------------------------------------------ */
+/* DP-LUR inner solver: DPLUSGS.cpp (the alternative to the LU-SGS sweeps    */
+/* of Dual_time_stepping, left commented out at main.cpp:268-284)             */
+
+/* one Jacobi relaxation at one cell, DPLUSGS.cpp:560-1118: the lower and
+ * upper neighbours' split Jacobians applied to the previous iterate NL, the
+ * inviscid diagonal of the cell (:1068-1107), NR = D^-1 (MR - LL - UU) */
+static void dplur_cell(or_state *s, int i, int j, int k) {
+  const size_t di = (size_t)s->Y * s->Z, dj = s->Z;
+  size_t c = IX(s, i, j, k), cil = c - di, cjl = c - dj, ckl = c - 1, ciu = c + di, cju = c + dj, cku = c + 1;
+  double **NL = s->NL;
+  const double dXI = s->p.dxi, dET = s->p.det, dZT = s->p.dzt;
+  splitj A = split_at(s, cil, 0), B = split_at(s, cjl, 1), C = split_at(s, ckl, 2);
+  double LL1 = (-A.p11 * NL[0][cil] - A.p12 * NL[1][cil] - A.p13 * NL[2][cil] - A.p14 * NL[3][cil]) / dXI +
+               (-B.p11 * NL[0][cjl] - B.p12 * NL[1][cjl] - B.p13 * NL[2][cjl] - B.p14 * NL[3][cjl]) / dET +
+               (-C.p11 * NL[0][ckl] - C.p12 * NL[1][ckl] - C.p13 * NL[2][ckl] - C.p14 * NL[3][ckl]) / dZT;
+  double LL2 = (-A.p21 * NL[0][cil] - A.p22 * NL[1][cil]) / dXI + (-B.p21 * NL[0][cjl] - B.p22 * NL[1][cjl]) / dET +
+               (-C.p21 * NL[0][ckl] - C.p22 * NL[1][ckl]) / dZT;
+  double LL3 = (-A.p31 * NL[0][cil] - A.p22 * NL[2][cil]) / dXI + (-B.p31 * NL[0][cjl] - B.p22 * NL[2][cjl]) / dET +
+               (-C.p31 * NL[0][ckl] - C.p22 * NL[2][ckl]) / dZT;
+  double LL4 = (-A.p41 * NL[0][cil] - A.p22 * NL[3][cil]) / dXI + (-B.p41 * NL[0][cjl] - B.p22 * NL[3][cjl]) / dET +
+               (-C.p41 * NL[0][ckl] - C.p22 * NL[3][ckl]) / dZT;
+  double LL5 =
+      (-A.p51 * NL[0][cil] - A.p52 * NL[1][cil] - A.p53 * NL[2][cil] - A.p54 * NL[3][cil] - A.p22 * NL[4][cil]) / dXI +
+      (-B.p51 * NL[0][cjl] - B.p52 * NL[1][cjl] - B.p53 * NL[2][cjl] - B.p54 * NL[3][cjl] - B.p22 * NL[4][cjl]) / dET +
+      (-C.p51 * NL[0][ckl] - C.p52 * NL[1][ckl] - C.p53 * NL[2][ckl] - C.p54 * NL[3][ckl] - C.p22 * NL[4][ckl]) / dZT;
+  A = split_at(s, ciu, 0); B = split_at(s, cju, 1); C = split_at(s, cku, 2);
+  double UU1 = (+A.m11 * NL[0][ciu] + A.p12 * NL[1][ciu] + A.p13 * NL[2][ciu] + A.p14 * NL[3][ciu]) / dXI +
+               (+B.m11 * NL[0][cju] + B.p12 * NL[1][cju] + B.p13 * NL[2][cju] + B.p14 * NL[3][cju]) / dET +
+               (+C.m11 * NL[0][cku] + C.p12 * NL[1][cku] + C.p13 * NL[2][cku] + C.p14 * NL[3][cku]) / dZT;
+  double UU2 = (+A.p21 * NL[0][ciu] + A.m22 * NL[1][ciu]) / dXI + (+B.p21 * NL[0][cju] + B.m22 * NL[1][cju]) / dET +
+               (+C.p21 * NL[0][cku] + C.m22 * NL[1][cku]) / dZT;
+  double UU3 = (+A.p31 * NL[0][ciu] + A.m22 * NL[2][ciu]) / dXI + (+B.p31 * NL[0][cju] + B.m22 * NL[2][cju]) / dET +
+               (+C.p31 * NL[0][cku] + C.m22 * NL[2][cku]) / dZT;
+  double UU4 = (+A.p41 * NL[0][ciu] + A.m22 * NL[3][ciu]) / dXI + (+B.p41 * NL[0][cju] + B.m22 * NL[3][cju]) / dET +
+               (+C.p41 * NL[0][cku] + C.m22 * NL[3][cku]) / dZT;
+  double UU5 =
+      (+A.p51 * NL[0][ciu] + A.p52 * NL[1][ciu] + A.p53 * NL[2][ciu] + A.p54 * NL[3][ciu] + A.m22 * NL[4][ciu]) / dXI +
+      (+B.p51 * NL[0][cju] + B.p52 * NL[1][cju] + B.p53 * NL[2][cju] + B.p54 * NL[3][cju] + B.m22 * NL[4][cju]) / dET +
+      (+C.p51 * NL[0][cku] + C.p52 * NL[1][cku] + C.p53 * NL[2][cku] + C.p54 * NL[3][cku] + C.m22 * NL[4][cku]) / dZT;
+  cprim q = cp_at(s, c);
+  diag3 d = diag_at(s, c, &q);
+  double **MR = s->MR, **NR = s->NR;
+  NR[0][c] = d.d11 * (MR[0][c] - LL1 - UU1);
+  NR[1][c] = d.d22 * (MR[1][c] - LL2 - UU2);
+  NR[2][c] = d.d22 * (MR[2][c] - LL3 - UU3);
+  NR[3][c] = d.d22 * (MR[3][c] - LL4 - UU4);
+  NR[4][c] = d.d51 * (MR[0][c] - LL1 - UU1) + d.d22 * (MR[4][c] - LL5 - UU5);
+}
+
+/* four Jacobi relaxations, DPLUSGS.cpp:488-1141; before each one the
+ * periodic 1-plane x halo of NL (NL[2] <- NL[ie], NL[ie+1] <- NL[3], the
+ * self-copies of :510-531), after it NL <- NR on the interior (:1127-1139).
+ * NL starts as D^-1 MR with zero ghost rows, as or_dts_residual leaves it
+ * (:186-478 form the same values: the sponge terms that Dual_time_stepping
+ * adds are zero here). */
+void or_dplur_sweeps(or_state *s) {
+  const int ie = s->p.nx + 2, jn = s->p.ny + 1, kn = s->p.nz + 1;
+  const size_t plane = (size_t)s->Y * s->Z;
+  for (int sweep = 1; sweep <= 4; sweep++) {
+    for (int v = 0; v < 5; v++) {
+      memmove(s->NL[v] + 2 * plane, s->NL[v] + (size_t)ie * plane, plane * sizeof(double));
+      memmove(s->NL[v] + (size_t)(ie + 1) * plane, s->NL[v] + 3 * plane, plane * sizeof(double));
+    }
+    for (int i = 3; i <= ie; i++)
+      for (int j = 2; j <= jn; j++)
+        for (int k = 2; k <= kn; k++) dplur_cell(s, i, j, k);
+    for (int i = 3; i <= ie; i++)
+      for (int j = 2; j <= jn; j++)
+        for (int k = 2; k <= kn; k++) {
+          size_t c = IX(s, i, j, k);
+          for (int v = 0; v < 5; v++) s->NL[v][c] = s->NR[v][c];
+        }
+  }
+}
+
+/* primitive-variable update of DPLUSGS.cpp:1152-1196 (as or_update, but the
+ * first increment is that of the pressure) and its norms, :1203-1221:
+ * er[v] = sqrt(sum of the squared squared increments) / (Nx Ny Nz) */
+void or_dplur_update(or_state *s, double *er) {
+  const int ie = s->p.nx + 2, jn = s->p.ny + 1, kn = s->p.nz + 1;
+  double e1 = 0, e2 = 0, e3 = 0, e4 = 0, e5 = 0;
+  for (int i = 3; i <= ie; i++)
+    for (int j = 2; j <= jn; j++)
+      for (int k = 2; k <= kn; k++) {
+        size_t c = IX(s, i, j, k);
+        const double J = s->J[c];
+        double **q = s->U_, **NR = s->NR;
+        double rhoold = q[0][c] * J;
+        double Uold = q[1][c] / q[0][c];
+        double Vold = q[2][c] / q[0][c];
+        double Wold = q[3][c] / q[0][c];
+        double VVold = Uold * Uold + Vold * Vold + Wold * Wold;
+        double Pold = (q[4][c] * J - 0.5 * rhoold * VVold) * (KG - 1);
+        double Told = Pold / rhoold;
+        double P = Pold + NR[0][c] * J;
+        double U = Uold + NR[1][c] * J;
+        double V = Vold + NR[2][c] * J;
+        double W = Wold + NR[3][c] * J;
+        double T = Told + NR[4][c] * J;
+        double rho = P / T;
+        q[0][c] = rho / J;
+        q[1][c] = rho * U / J;
+        q[2][c] = rho * V / J;
+        q[3][c] = rho * W / J;
+        q[4][c] = (P / (KG - 1) + 0.5 * rho * (U * U + V * V + W * W)) / J;
+        s->res[0][c] = (P - Pold) * (P - Pold);
+        s->res[1][c] = (U - Uold) * (U - Uold);
+        s->res[2][c] = (V - Vold) * (V - Vold);
+        s->res[3][c] = (W - Wold) * (W - Wold);
+        s->res[4][c] = (T - Told) * (T - Told);
+      }
+  /* the sums run in a second pass in the reference's loop order (:1203-1215) */
+  for (int i = 3; i <= ie; i++)
+    for (int j = 2; j <= jn; j++)
+      for (int k = 2; k <= kn; k++) {
+        size_t c = IX(s, i, j, k);
+        e1 = e1 + s->res[0][c] * s->res[0][c];
+        e2 = e2 + s->res[1][c] * s->res[1][c];
+        e3 = e3 + s->res[2][c] * s->res[2][c];
+        e4 = e4 + s->res[3][c] * s->res[3][c];
+        e5 = e5 + s->res[4][c] * s->res[4][c];
+      }
+  double DN = 1. / ((double)s->p.nx * s->p.ny * s->p.nz);
+  er[0] = sqrt(e1) * DN; er[1] = sqrt(e2) * DN; er[2] = sqrt(e3) * DN;
+  er[3] = sqrt(e4) * DN; er[4] = sqrt(e5) * DN;
+}
+
+/* one inner iteration with DPLUSGS in place of Dual_time_stepping */
+void or_dplur_inner_iteration(or_state *s, double *er) {
+  or_halo_x(s);
+  or_bc_y(s);
+  or_bc_z(s);
+  or_flux_x(s);
+  or_flux_y(s);
+  or_flux_z(s);
+  or_viscous(s);
+  or_dts_residual(s);
+  or_dplur_sweeps(s);
+  or_dplur_update(s, er);
+}
+
 /* one inner iteration: main.cpp:167-264 */
 void or_inner_iteration(or_state *s, double *er) {
   or_halo_x(s);

@@ -55,6 +55,9 @@ def _load():
             getattr(L, name).argtypes = [ctypes.c_void_p]
         L.or_update.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.or_inner_iteration.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.or_dplur_sweeps.argtypes = [ctypes.c_void_p]
+        L.or_dplur_update.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.or_dplur_inner_iteration.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -71,8 +74,12 @@ def load_wavy_metrics(array, ch) -> None:
 class Oracle:
     """CPU restatement of one slab of the reference solver for one workload."""
 
-    def __init__(self, ch, e: float | None = None, curved_walls: bool | None = None):
+    def __init__(self, ch, e: float | None = None, curved_walls: bool | None = None, inner_solver: str = "lusgs"):
+        """inner_solver: "lusgs" (Dual_time_stepping) or "dplur" (DPLUSGS)."""
         from cgli_fu_flow_b200 import channel as C
+        if inner_solver not in ("lusgs", "dplur"):
+            raise ValueError(inner_solver)
+        self.inner_solver = inner_solver
         self.C = C
         self.ch = ch
         self.L = _load()
@@ -123,7 +130,8 @@ class Oracle:
 
     def inner_iteration(self) -> np.ndarray:
         er = np.zeros(5)
-        self.L.or_inner_iteration(self.s, er.ctypes.data)
+        fn = self.L.or_dplur_inner_iteration if self.inner_solver == "dplur" else self.L.or_inner_iteration
+        fn(self.s, er.ctypes.data)
         return er
 
     def bulk_flux(self) -> float:

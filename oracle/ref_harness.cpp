@@ -67,6 +67,13 @@ void Dual_time_stepping(int, double, double, double *, double *, double *, doubl
                         A3, A3, A3, A3,
                         A3, A3, A3, A3, A3, A3, A3, A3, A3, A3, A3, A3, A3, A3, A3,
                         A3, A3, A3, A3, A3, A3, A3);
+void DPLUSGS(int, double, double *, double *, double *, double *, double *, double,
+             A3, A3, A3, A3, A3, A3, A3, A3, A3, A3, A3, A3, A3, A3, A3,
+             A3, A3, A3, A3, A3, A3, A3, A3, A3, A3,
+             A3, A3, A3, A3, A3, A3, A3, A3, A3, A3, A3, A3, A3, A3, A3,
+             A3, A3, A3, A3,
+             A3, A3, A3, A3, A3, A3, A3, A3, A3, A3, A3, A3, A3, A3, A3,
+             A3, A3, A3, A3, A3);
 void Driven_force(int, A3, A3);
 void Hyperplane(int, int (*)[2], int (*)[3]);
 void Filter(int, double, double, double, A3, A3, A3, A3, A3, A3, A3, A3, A3, A3);
@@ -315,6 +322,33 @@ void ref_inner_iteration(double *er) {
   ref_flux_z();
   ref_viscous();
   ref_dts(er);
+}
+
+/* DPLUSGS.cpp in place of Dual_time_stepping (the call main.cpp:268-284
+ * leaves commented out): residual, four Jacobi relaxations, update */
+void ref_dplusgs(double *er) {
+  A3 *q = A.U_, *u = A.U, *uq = A.Uq, *m = A.m;
+  DPLUSGS(MYID, g_dt, &er[0], &er[1], &er[2], &er[3], &er[4], g_e,
+          q[0], q[1], q[2], q[3], q[4], u[0], u[1], u[2], u[3], u[4],
+          uq[0], uq[1], uq[2], uq[3], uq[4],
+          A.J, m[0], m[1], m[2], m[3], m[4], m[5], m[6], m[7], m[8],
+          A.inFx[0], A.inFx[1], A.inFx[2], A.inFx[3], A.inFx[4],
+          A.inFy[0], A.inFy[1], A.inFy[2], A.inFy[3], A.inFy[4],
+          A.inFz[0], A.inFz[1], A.inFz[2], A.inFz[3], A.inFz[4],
+          A.vF[0], A.vF[1], A.vF[2], A.vF[3],
+          A.MR[0], A.MR[1], A.MR[2], A.MR[3], A.MR[4],
+          A.NR[0], A.NR[1], A.NR[2], A.NR[3], A.NR[4],
+          A.NL[0], A.NL[1], A.NL[2], A.NL[3], A.NL[4],
+          A.Res[0], A.Res[1], A.Res[2], A.Res[3], A.Res[4]);
+}
+
+void ref_inner_iteration_dplusgs(double *er) {
+  ref_halo_bc();
+  ref_flux_x();
+  ref_flux_y();
+  ref_flux_z();
+  ref_viscous();
+  ref_dplusgs(er);
 }
 
 /* bulk mass flux with the weighting of Driven_force.cpp:38-62, over the

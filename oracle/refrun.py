@@ -19,7 +19,12 @@ from . import build_ref
 class RefSolver:
     """One reference process (rank 1 of 3, periodic x) for one workload."""
 
-    def __init__(self, ch, threads: int = 0, build: bool = True):
+    def __init__(self, ch, threads: int = 0, build: bool = True, inner_solver: str = "lusgs"):
+        """inner_solver: "lusgs" (Dual_time_stepping, the reference's default)
+        or "dplur" (DPLUSGS.cpp, the call main.cpp:268-284 leaves commented)."""
+        if inner_solver not in ("lusgs", "dplur"):
+            raise ValueError(inner_solver)
+        self.inner_solver = inner_solver
         params = dict(nx=ch.nx, ny=ch.ny, nz=ch.nz, dxi=ch.dxi, det=ch.det, dzt=ch.dzt,
                       high=ch.high, mu=_c().MU0, pr=_c().PR, stretch=_c().STRETCH,
                       twall_lo=_c().T0, twall_hi=_c().T0)
@@ -91,7 +96,10 @@ class RefSolver:
 
     def inner_iteration(self) -> np.ndarray:
         er = (ctypes.c_double * 5)()
-        self.lib.ref_inner_iteration(er)
+        if self.inner_solver == "dplur":
+            self.lib.ref_inner_iteration_dplusgs(er)
+        else:
+            self.lib.ref_inner_iteration(er)
         return np.array(er[:])
 
     def end_step(self, update_force: bool = True) -> None:

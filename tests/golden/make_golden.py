@@ -11,9 +11,12 @@ The oracle must reproduce every hash bit for bit; the GPU path is compared
 with the stored state within tolerance.
 
 It also records the reference's filter sensor (Filter.cpp) on the seeded
-field at five thresholds (filter_<workload>.npz).
+field at five thresholds (filter_<workload>.npz), and the DP-LUR inner
+solver of DPLUSGS.cpp run in place of Dual_time_stepping (dplur_<workload>:
+the first iteration's MR / NR / U_ hashes, three steps' norms, forces and
+final state).
 
-Usage:  python tests/golden/make_golden.py [--filter] [nx ny nz]
+Usage:  python tests/golden/make_golden.py [--filter | --dplur] [nx ny nz]
 """
 from __future__ import annotations
 
@@ -140,10 +143,44 @@ def main_filter(nx=8, ny=12, nz=8):
     print("wrote", base + ".npz")
 
 
+def main_dplur(nx=8, ny=12, nz=8):
+    """DPLUSGS.cpp (with the loop-index fix of oracle/build_ref.py) in place of
+    Dual_time_stepping: one inner iteration's arrays, then three steps of
+    ITERS inner iterations with the driving-force update."""
+    import ctypes
+    ch = Channel(nx, ny, nz)
+    reg = regions(ch)
+    r = RefSolver(ch, threads=1, inner_solver="dplur")
+    r.init()
+    er = (ctypes.c_double * 5)()
+    r.lib.ref_inner_iteration_dplusgs(er)
+    out = {"workload": ch.name, "cells": [nx, ny, nz], "steps": STEPS, "iters_per_step": ITERS,
+           "first": {n: digest(r.array(n)[reg["cell"]]) for n in STAGES["dts"]},
+           "first_norms": [3.0 * x for x in er[:]]}
+    r2 = RefSolver(ch, threads=1, build=False, inner_solver="dplur")
+    r2.init()
+    forces, norms = [r2.force], []
+    for _ in range(STEPS):
+        _, e = r2.step(ITERS)
+        norms.append([3.0 * x for x in e])
+        forces.append(r2.force)
+    out["step_norms"] = norms
+    out["forces"] = forces
+    q = r2.q()[(slice(None),) + reg["cell"]]
+    out["final_state"] = digest(q)
+    base = os.path.join(HERE, "dplur_" + ch.name)
+    np.savez_compressed(base + ".npz", q=q)
+    with open(base + ".json", "w") as fh:
+        json.dump(out, fh, indent=1)
+    print("wrote", base + ".json", base + ".npz")
+
+
 if __name__ == "__main__":
     argv = sys.argv[1:]
     which = main
     if argv and argv[0] == "--filter":
         which, argv = main_filter, argv[1:]
+    elif argv and argv[0] == "--dplur":
+        which, argv = main_dplur, argv[1:]
     args = [int(a) for a in argv[0:3]] or [8, 12, 8]
     which(*args)
