@@ -5,6 +5,7 @@
 
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <sys/types.h>
 #include <cstdio>
 #include <cstring>
@@ -65,6 +66,7 @@ struct cgli_ctx {
   double Emax[5] = {0, 0, 0, 0, 0};   // running maximum of the norms over the run
   int history = 0;                    // completed steps since the state was set
   int predictor = 0;                  // 0 previous level, 1 extrapolation, 2 learned
+  int inner_solver = CGLI_LUSGS;      // CGLI_LUSGS or CGLI_DPLUR
   cgli_cnn *cnn = nullptr;            // learned initial guess (not owned)
   std::vector<double> step_norms;     // the five norms of every inner iteration of the last step
   double *stats = nullptr;            // [11][nx][ny] running sums (allocated on first use)
@@ -291,6 +293,12 @@ int cgli_create(const cgli_params *p, cgli_ctx **out) {
   if (rc == CGLI_OK) rc = alloc(c, (8 + 296) * sizeof(double), (void **)&c->d_out);
   if (rc == CGLI_OK) rc = alloc(c, 16 * sizeof(int), (void **)&d.status);
   c->update_blocks = p->nx * p->ny;
+  // relaxation tile shape of the DP-LUR solver (tuning; defaults 6 rows, 32 planes)
+  if (const char *ev = getenv("CGLI_DPLUR_TILE_ROWS")) cgli::dplur_tile_rows = atoi(ev) == 14 ? 14 : 6;
+  if (const char *ev = getenv("CGLI_DPLUR_CHUNK")) {
+    int v = atoi(ev);
+    if (v >= 2 && v <= 4096) cgli::dplur_chunk = v;
+  }
   const int nti = (p->nx + cgli::SWEEP_TI - 1) / cgli::SWEEP_TI, ntj = (p->ny + cgli::SWEEP_TJ - 1) / cgli::SWEEP_TJ;
   c->sweep_tiles = nti * ntj;
   size_t nblk = (size_t)std::max(c->update_blocks, c->sweep_tiles);
@@ -660,6 +668,27 @@ int cgli_dual_time_stepping(cgli_ctx *c, double er[5]) {
   return read_norms(c, er, c->update_blocks);
 }
 
+int cgli_dplusgs(cgli_ctx *c, double er[5]) {
+  int rc = check(c); if (rc) return rc;
+  rc = need_ready(c); if (rc) return rc;
+  if (!er) return fail(CGLI_EINVAL, "null er");
+  if (c->p.precision != CGLI_FP64) return fail(CGLI_EINVAL, "DP-LUR needs precision CGLI_FP64");
+  cgli::launch_dplur(c->d, c->stream);
+  rc = last_launch("dplusgs"); if (rc) return rc;
+  return read_norms(c, er, c->update_blocks);
+}
+
+int cgli_set_inner_solver(cgli_ctx *c, int solver) {
+  int rc = check(c); if (rc) return rc;
+  if (solver != CGLI_LUSGS && solver != CGLI_DPLUR)
+    return fail(CGLI_EINVAL, "inner solver must be CGLI_LUSGS or CGLI_DPLUR");
+  if (solver == CGLI_DPLUR && c->p.precision != CGLI_FP64)
+    return fail(CGLI_EINVAL, "DP-LUR needs precision CGLI_FP64");
+  if (solver != c->inner_solver) drop_graph(c);
+  c->inner_solver = solver;
+  return CGLI_OK;
+}
+
 int cgli_inner_iteration(cgli_ctx *c, double er[5]) {
   int rc = check(c); if (rc) return rc;
   rc = need_ready(c); if (rc) return rc;
@@ -667,10 +696,12 @@ int cgli_inner_iteration(cgli_ctx *c, double er[5]) {
   if (!c->metrics_checked) {
     rc = check_channel_metrics(c); if (rc) return rc;
   }
+  const bool dplur = c->inner_solver == CGLI_DPLUR;
   if (!c->iter_graph) {
     cudaGraph_t g;
     CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    cgli::launch_fused_iteration(c->d, c->sw, c->stream, c->p.precision);
+    if (dplur) cgli::launch_dplur_iteration(c->d, c->stream);
+    else cgli::launch_fused_iteration(c->d, c->sw, c->stream, c->p.precision);
     cudaError_t e = cudaStreamEndCapture(c->stream, &g);
     if (e != cudaSuccess) return fail(CGLI_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
     e = cudaGraphInstantiate(&c->iter_graph, g, 0);
@@ -678,7 +709,7 @@ int cgli_inner_iteration(cgli_ctx *c, double er[5]) {
     if (e != cudaSuccess) return fail(CGLI_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
   }
   CUDA_TRY(cudaGraphLaunch(c->iter_graph, c->stream));
-  return read_norms(c, er, c->sweep_tiles);
+  return read_norms(c, er, dplur ? c->update_blocks : c->sweep_tiles);
 }
 
 int cgli_driven_force(cgli_ctx *c, double *bulk_flux) {

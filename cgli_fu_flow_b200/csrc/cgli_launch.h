@@ -59,6 +59,20 @@ void sweep_tile_order(int nti, int ntj, std::vector<int> &order);
 void launch_sweeps(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed);
 // one pass (forward / backward, final with the update) of the sweeps
 void launch_sweep_pass(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed, bool backward, bool final_pass);
+// Dual_time_stepping.cpp:737-922 residual on the natural layout: MR and
+// NL = NR = D^-1 MR on the interior cells
+void launch_dts_residual(const Dev &d, cudaStream_t s);
+// DP-LUR inner solver of DPLUSGS.cpp (kernels_dplur.cu): residual, four
+// Jacobi relaxations (final result in NR), update with per-block partial
+// sums of the squared squared increments in d.partial (nx * ny blocks)
+void launch_dplur(const Dev &d, cudaStream_t s);
+// one relaxation NR -> NL (from_nr) or NL -> NR
+void launch_dplur_relax(const Dev &d, cudaStream_t s, bool from_nr);
+// halo, boundaries, fluxes, viscous terms, then launch_dplur
+void launch_dplur_iteration(const Dev &d, cudaStream_t s);
+// relaxation tile rows (6 or 14) and x planes per CTA
+extern int dplur_tile_rows;
+extern int dplur_chunk;
 // residual assembly writing MR and the first sweep's lagged halo planes
 void launch_residual_fast(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed);
 

@@ -433,6 +433,10 @@ void launch_viscous(const Dev &d, cudaStream_t s) {
   k_viscous_faces<<<cellgrid(d.nz + 1, d.ny + 1, d.nx + 1, 64), 64, 0, s>>>(d);
   k_viscous_div<<<cellgrid(d.nz, d.ny, d.nx, 64), 64, 0, s>>>(d);
 }
+void launch_dts_residual(const Dev &d, cudaStream_t s) {
+  k_dts_residual<<<cellgrid(d.nz, d.ny, d.nx, 64), 64, 0, s>>>(d);
+}
+
 void launch_dts(const Dev &d, cudaStream_t s, int update_blocks_x) {
   k_dts_residual<<<cellgrid(d.nz, d.ny, d.nx, 64), 64, 0, s>>>(d);
   int ie = d.nx + 2, jn = d.ny + 1, kn = d.nz + 1;

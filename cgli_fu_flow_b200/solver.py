@@ -54,7 +54,10 @@ EXPORTS = [
     "cgli_copy_state", "cgli_cnn_time_inference", "cgli_wavy_channel_metrics", "cgli_wavy_channel_metrics_host",
     "cgli_statistics_accumulate", "cgli_statistics_get", "cgli_statistics_reset",
     "cgli_write_restart", "cgli_read_restart", "cgli_write_history", "cgli_read_history",
+    "cgli_dplusgs", "cgli_set_inner_solver",
 ]
+
+INNER_SOLVERS = {"lusgs": 0, "dplur": 1}
 
 _lib = None
 
@@ -261,6 +264,19 @@ class Solver:
         er = (ctypes.c_double * 5)()
         self._rc(self.L.cgli_dual_time_stepping(self.h, er))
         return np.array(er[:])
+
+    def dplusgs(self) -> np.ndarray:
+        """DPLUSGS.cpp in place of dual_time_stepping (reads the same inF / vF)."""
+        er = (ctypes.c_double * 5)()
+        self._rc(self.L.cgli_dplusgs(self.h, er))
+        return np.array(er[:])
+
+    def set_inner_solver(self, name: str) -> None:
+        """"lusgs" (Dual_time_stepping's sweeps, the default) or "dplur"
+        (DPLUSGS's Jacobi relaxations; double precision only)."""
+        if name not in INNER_SOLVERS:
+            raise ValueError(name)
+        self._rc(self.L.cgli_set_inner_solver(self.h, INNER_SOLVERS[name]))
 
     def inner_iteration(self) -> np.ndarray:
         er = (ctypes.c_double * 5)()

@@ -143,9 +143,25 @@ int cgli_viscous_terms(cgli_ctx *ctx);
  * filled by the three flux entry points and cgli_viscous_terms. */
 int cgli_dual_time_stepping(cgli_ctx *ctx, double er[5]);
 
+/* DPLUSGS.cpp:18-1240, the DP-LUR alternative to Dual_time_stepping that
+ * main.cpp:268-284 leaves commented out: the same residual, four Jacobi
+ * relaxations of the same split-Jacobian operator (inviscid diagonal), the
+ * update of U_, five norms er[v] = sqrt(sum of r_v^2)/(Nx Ny Nz) with r the
+ * squared increments of p, u, v, w, T (the reference divides by its global
+ * X_out).  Needs precision CGLI_FP64. */
+int cgli_dplusgs(cgli_ctx *ctx, double er[5]);
+
+#define CGLI_LUSGS 0          /* inner solver: Dual_time_stepping's LU-SGS sweeps */
+#define CGLI_DPLUR 1          /* inner solver: DPLUSGS's Jacobi relaxations */
+/* Inner solver of cgli_inner_iteration and cgli_step: the reference's
+ * Dual_time_stepping call (main.cpp:245-262, the default) or its commented
+ * DPLUSGS call (main.cpp:268-284).  CGLI_DPLUR needs precision CGLI_FP64. */
+int cgli_set_inner_solver(cgli_ctx *ctx, int solver);
+
 /* One complete inner iteration (main.cpp:167-264) through the fused fast
- * path: halo + boundaries, one residual kernel (fluxes, viscous terms,
- * dual-time residual), the wavefront sweeps and the update. */
+ * path: halo + boundaries, fluxes, viscous terms, the dual-time residual,
+ * then the wavefront sweeps and the update (CGLI_LUSGS) or the relaxations
+ * and the update (CGLI_DPLUR). */
 int cgli_inner_iteration(cgli_ctx *ctx, double er[5]);
 
 /* Driven_force.cpp:14-74: bulk mass flux (volume-weighted mean of rho*u) */

@@ -112,3 +112,134 @@ def test_dplur_oracle_matches_reference_wavy_grid():
         r.step(4)
         o.step(4)
         assert np.array_equal(r.q()[sl], o.q()[sl])
+
+
+# ------------------------------------------------------------------ GPU
+# Tolerances as for the LU-SGS path: the relaxation kernel evaluates the
+# same expressions with reciprocals and fused multiply-adds, so one call
+# agrees to ~1e-13 of each array's scale; whole steps by relative L2 per
+# conserved variable.
+
+STAGE_TOL = 1e-12
+STEP_TOL = 1e-10
+
+
+def _rel_max(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def _rel_l2(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def _pair(ch, **kw):
+    from cgli_fu_flow_b200 import build
+    from cgli_fu_flow_b200.solver import Solver
+    from oracle.oracle import Oracle
+    build.build()
+    g = Solver(ch)
+    g.init()
+    o = Oracle(ch, inner_solver="dplur", **kw)
+    o.init()
+    return g, o
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dims", [(8, 12, 8), (40, 36, 62)])
+def test_dplusgs_entry_matches_oracle(dims):
+    """cgli_dplusgs after the granular residual entry points: the relaxed
+    increment NR, the updated state and the norms.  The second grid has
+    ragged relaxation tiles in j and k and two x chunks."""
+    ch = Channel(*dims)
+    g, o = _pair(ch)
+    for fn in ("halo_x", "y_boundary_condition", "z_boundary_condition", "flux_x", "flux_y", "flux_z",
+               "viscous_terms"):
+        getattr(g, fn)()
+    for n in ("halo_x", "bc_y", "bc_z", "flux_x", "flux_y", "flux_z", "viscous", "dts_residual", "dplur_sweeps"):
+        o.call(n)
+    er_o = np.zeros(5)
+    o.L.or_dplur_update(o.s, er_o.ctypes.data)
+    er_g = g.dplusgs()
+    reg = _regions(ch)["cell"]
+    for v in range(1, 6):
+        assert _rel_max(g.get(f"NR{v}")[reg], o.array(f"NR{v}")[reg]) <= STAGE_TOL, v
+        assert _rel_max(g.get(f"U{v}_")[reg], o.array(f"U{v}_")[reg]) <= STAGE_TOL, v
+    np.testing.assert_allclose(er_g, er_o, rtol=1e-9)
+
+
+@pytest.mark.gpu
+def test_dplur_steps_match_reference_fixture():
+    """Three steps of ten inner iterations through cgli_step with the DP-LUR
+    solver against the reference's DPLUSGS.cpp final state."""
+    g0 = _fixture()
+    ch = Channel(*g0["cells"])
+    g, _ = _pair(ch)
+    g.set_inner_solver("dplur")
+    for _ in range(g0["steps"]):
+        it, _er = g.step(g0["iters_per_step"])
+        assert it == g0["iters_per_step"]
+    ref = np.load(os.path.join(GOLDEN, "dplur_channel_8x12x8.npz"))["q"]
+    q = g.q()[(slice(None),) + _regions(ch)["cell"]]
+    for v in range(5):
+        assert _rel_l2(q[v], ref[v]) <= STEP_TOL, v
+
+
+@pytest.mark.gpu
+def test_dplur_twenty_steps_match_oracle():
+    """Twenty steps on a grid with several relaxation tiles and x chunks,
+    with the stopping rule of main.cpp:287-304 deciding the iteration
+    counts on both sides."""
+    ch = Channel(34, 20, 40)
+    g, o = _pair(ch)
+    g.set_inner_solver("dplur")
+    for s in range(20):
+        it_g, _ = g.step(None, drop=1e-2, cap=12)
+        it_o, _ = o.step(None, drop=1e-2, cap=12)
+        assert it_g == it_o, s
+    sl = (slice(None),) + _regions(ch)["cell"]
+    for v in range(5):
+        assert _rel_l2(g.q()[sl][v], o.q()[sl][v]) <= STEP_TOL, v
+
+
+@pytest.mark.gpu
+def test_dplur_wavy_wall_matches_oracle():
+    """General metrics (every metric term live): five steps."""
+    ch = Channel(16, 16, 32, wavy=True, wave=0.01)
+    g, o = _pair(ch)
+    g.set_inner_solver("dplur")
+    for _ in range(5):
+        g.step(6)
+        o.step(6)
+    sl = (slice(None),) + _regions(ch)["cell"]
+    for v in range(5):
+        assert _rel_l2(g.q()[sl][v], o.q()[sl][v]) <= STEP_TOL, v
+
+
+@pytest.mark.gpu
+def test_inner_solver_switch_and_errors():
+    """Switching back to LU-SGS gives the LU-SGS result again; DP-LUR is
+    refused in mixed precision and an unknown solver is refused."""
+    from cgli_fu_flow_b200 import build
+    from cgli_fu_flow_b200.solver import CgliError, Solver
+    from oracle.oracle import Oracle
+    build.build()
+    ch = Channel(8, 12, 8)
+    g = Solver(ch)
+    g.init()
+    g.set_inner_solver("dplur")
+    g.set_inner_solver("lusgs")
+    o = Oracle(ch)
+    o.init()
+    g.step(5)
+    o.step(5)
+    sl = (slice(None),) + _regions(ch)["cell"]
+    assert _rel_l2(g.q()[sl][0], o.q()[sl][0]) <= STEP_TOL
+    with pytest.raises(CgliError):
+        g._rc(g.L.cgli_set_inner_solver(g.h, 7))
+    m = Solver(ch, 1)
+    m.init()
+    with pytest.raises(CgliError):
+        m.set_inner_solver("dplur")
+    er = (__import__("ctypes").c_double * 5)()
+    with pytest.raises(CgliError):
+        m._rc(m.L.cgli_dplusgs(m.h, er))
