@@ -14,8 +14,10 @@ every step.
 with second-order extrapolation in mixed precision, whose converged levels
 train the learned initial guess with Adam on the GPU), the same number of
 steps in: plain FP64 (previous-level guess), mixed precision with
-extrapolation, and mixed precision with the learned guess, with each mixed
-arm's state error against the FP64 arm.
+extrapolation, mixed precision with the learned guess, and plain FP64 with
+the DP-LUR inner solver of DPLUSGS.cpp in place of the LU-SGS sweeps (its
+stopping norms are those of DPLUSGS.cpp, squared increments with the
+pressure first), with each arm's state error against the FP64 arm.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -278,12 +280,15 @@ def run_arms(a, ch, dist) -> dict:
                              "collect_s": round(collect_s, 2), "train_s": round(train_s, 2),
                              "loss_unit": "mean squared extrapolation correction / its RMS (1.0 = extrapolation)"}}
     sols = {}
-    for name, prec, pred in (("fp64", FP64, 0), ("mixed_extrapolation", MIXED, 1), ("mixed_learned", MIXED, 2)):
+    for name, prec, pred in (("fp64", FP64, 0), ("mixed_extrapolation", MIXED, 1), ("mixed_learned", MIXED, 2),
+                             ("fp64_dplur", FP64, 0)):
         s = Solver(ch, prec)
         s.copy_state_from(base)
         if pred == 2:
             s.set_learned_guess(net)
         s.set_predictor(pred)
+        if name == "fp64_dplur":
+            s.set_inner_solver("dplur")
         for _ in range(a.warmup):
             s.step(None, a.drop, a.cap)
         ms, iters = _timed_steps(s, a, dist)
@@ -291,7 +296,9 @@ def run_arms(a, ch, dist) -> dict:
         out[name] = {"value": round(value, 3), "unit": "Mcell-steps/s", "ms_per_step": round(ms / a.steps, 3),
                      "mean_inner_iterations": round(float(np.mean(iters)), 2), "inner_iterations": iters,
                      "precision": "fp64" if prec == FP64 else "mixed", "predictor": ["previous level", "extrapolation",
-                                                                                     "learned"][pred]}
+                                                                                     "learned"][pred],
+                     "inner_solver": "DP-LUR (DPLUSGS.cpp: 4 Jacobi relaxations; norms of squared "
+                                     "p, u, v, w, T increments)" if name == "fp64_dplur" else "LU-SGS"}
         if pred == 2:
             inf_ms = net.time_inference(s, 3)
             tf = ch.cells * CNN_TC_FLOP_PER_CELL / (inf_ms / 1e3) / 1e12
@@ -300,7 +307,7 @@ def run_arms(a, ch, dist) -> dict:
         sols[name] = s
     sl = (slice(None), slice(3, ch.nx + 3), slice(2, ch.ny + 2), slice(2, ch.nz + 2))
     ref = sols["fp64"].q()[sl]
-    for name in ("mixed_extrapolation", "mixed_learned"):
+    for name in ("mixed_extrapolation", "mixed_learned", "fp64_dplur"):
         q = sols[name].q()[sl]
         errs = [float(np.linalg.norm(q[v] - ref[v]) / np.linalg.norm(ref[v])) for v in range(5)]
         out[name]["state_rel_l2_vs_fp64"] = max(errs)

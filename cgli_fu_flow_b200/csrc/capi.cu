@@ -673,7 +673,7 @@ int cgli_dplusgs(cgli_ctx *c, double er[5]) {
   rc = need_ready(c); if (rc) return rc;
   if (!er) return fail(CGLI_EINVAL, "null er");
   if (c->p.precision != CGLI_FP64) return fail(CGLI_EINVAL, "DP-LUR needs precision CGLI_FP64");
-  cgli::launch_dplur(c->d, c->stream);
+  cgli::launch_dplur(c->d, c->sw, c->stream);
   rc = last_launch("dplusgs"); if (rc) return rc;
   return read_norms(c, er, c->update_blocks);
 }
@@ -700,7 +700,7 @@ int cgli_inner_iteration(cgli_ctx *c, double er[5]) {
   if (!c->iter_graph) {
     cudaGraph_t g;
     CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    if (dplur) cgli::launch_dplur_iteration(c->d, c->stream);
+    if (dplur) cgli::launch_dplur_iteration(c->d, c->sw, c->stream);
     else cgli::launch_fused_iteration(c->d, c->sw, c->stream, c->p.precision);
     cudaError_t e = cudaStreamEndCapture(c->stream, &g);
     if (e != cudaSuccess) return fail(CGLI_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));

@@ -64,12 +64,13 @@ void launch_sweep_pass(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mi
 void launch_dts_residual(const Dev &d, cudaStream_t s);
 // DP-LUR inner solver of DPLUSGS.cpp (kernels_dplur.cu): residual, four
 // Jacobi relaxations (final result in NR), update with per-block partial
-// sums of the squared squared increments in d.partial (nx * ny blocks)
-void launch_dplur(const Dev &d, cudaStream_t s);
+// sums of the squared squared increments in d.partial (nx * ny blocks).
+// Reads the per-j metric tables of sw when sw.channel_metrics is set.
+void launch_dplur(const Dev &d, const SweepArgs &sw, cudaStream_t s);
 // one relaxation NR -> NL (from_nr) or NL -> NR
-void launch_dplur_relax(const Dev &d, cudaStream_t s, bool from_nr);
+void launch_dplur_relax(const Dev &d, const SweepArgs &sw, cudaStream_t s, bool from_nr);
 // halo, boundaries, fluxes, viscous terms, then launch_dplur
-void launch_dplur_iteration(const Dev &d, cudaStream_t s);
+void launch_dplur_iteration(const Dev &d, const SweepArgs &sw, cudaStream_t s);
 // relaxation tile rows (6 or 14) and x planes per CTA
 extern int dplur_tile_rows;
 extern int dplur_chunk;
