@@ -73,6 +73,19 @@ class Channel:
     # the flat upper wall (the curvilinear workload); False: the flat channel
     wavy: bool = False
     wave: float = 0.05
+    # the reference's own configuration instead of the periodic channel: x
+    # open with characteristic inflow / outflow ghost planes
+    # (X_boundary_condition.cpp), sponge layers over the first nx_inlet and
+    # the last nx_outlet cells (Dual_time_stepping.cpp:554-664), walls
+    # isothermal only between them (Y_boundary_condition.cpp:114), and
+    # optionally its buoyancy body force f = -(rho - 1.1842) 9.81
+    # (Dual_time_stepping.cpp:831) in place of the controlled uniform force
+    x_open: bool = False
+    nx_inlet: int = 0
+    nx_outlet: int = 0
+    buoyancy: bool = False
+    twall_lo: float = T0                  # lower / upper wall temperature (K)
+    twall_hi: float = T0
     # derived (filled in __post_init__)
     rho0: float = field(init=False)
     c0: float = field(init=False)
@@ -103,6 +116,8 @@ class Channel:
 
     @property
     def name(self) -> str:
+        if self.x_open:
+            return f"open_{self.nx}x{self.ny}x{self.nz}_{self.nx_inlet}_{self.nx_outlet}"
         return f"{'wavy' if self.wavy else 'channel'}_{self.nx}x{self.ny}x{self.nz}"
 
     @property

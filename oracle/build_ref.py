@@ -54,8 +54,9 @@ PATCHES = {
     "Jacobian_w.cpp": [("double gamma1 = 2.8;", "double gamma1 = CGLI_STRETCH;", 1)],
     "Y_boundary_condition.cpp": [("T = 343.0592;", "T = CGLI_TWALL_LO;", 1),
                                  ("T = 298.0592;", "T = CGLI_TWALL_HI;", 1)],
-    "Dual_time_stepping.cpp": [("f = -(rho-1.1842)*9.81;", "f = cgli_ref_force;", 1),
-                               ("void Dual_time_stepping", "extern double cgli_ref_force;\nvoid Dual_time_stepping", 1)],
+    "Dual_time_stepping.cpp": [("f = -(rho-1.1842)*9.81;", "f = cgli_ref_buoyancy ? -(rho-1.1842)*9.81 : cgli_ref_force;", 1),
+                               ("void Dual_time_stepping",
+                                "extern double cgli_ref_force;\nextern int cgli_ref_buoyancy;\nvoid Dual_time_stepping", 1)],
     # DPLUSGS.cpp reads the constant f of prm.h (included in its body); the
     # harness gives it the same driving force as Dual_time_stepping.  Its
     # relaxation loop never assigns j_ and k_ (ijk.h declares them, the
@@ -80,10 +81,17 @@ def r17(x: float) -> str:
 
 
 def gen_headers(cfgdir: str, p: dict) -> None:
-    nx3 = 3 * p["nx"]
-    res = f"""/* generated stand-in for Resolution.h: rank 1 of 3 x-slabs */
-#define nx_inlet  0
-#define nx_outlet 0
+    """Periodic slab: rank 1 of 3 equal slabs (X_out = 3 Nx), every routine on
+    its interior-rank path.  x_open: a single rank 0 of 1 (X_out = Nx), the
+    reference's own inflow/outflow configuration with sponge layers."""
+    open_ = bool(p.get("x_open", 0))
+    nslab = 1 if open_ else 3
+    nx3 = nslab * p["nx"]
+    res = f"""/* generated stand-in for Resolution.h: rank {0 if open_ else 1} of {nslab} x-slabs */
+#define nx_inlet  {p.get('nx_inlet', 0) if open_ else 0}
+#define nx_outlet {p.get('nx_outlet', 0) if open_ else 0}
+#define CGLI_NSLAB {nslab}
+#define CGLI_MYID {0 if open_ else 1}
 #define X_out {nx3}
 #define Y_out {p['ny']}
 #define Z_out {p['nz']}
@@ -125,8 +133,8 @@ double psi = 0.001;
 double Cp = Cv*K;
 double lambda_L = mu_L*Cv*K/Pr_L;
 """
-    mpi = """/* generated stand-in for MPI_prm.h: three x-slabs */
-#define np 3
+    mpi = f"""/* generated stand-in for MPI_prm.h: {nslab} x-slab(s) */
+#define np {nslab}
 int nproc = np;
 int istart, iend, icount, r_nbr, l_nbr, lastp, iroot;
 int itag, isrc, idest, istart1, icount1,icount2, istart2, iend1, iend2;
@@ -167,7 +175,8 @@ def compile_one(fname: str, outdir: str, cfgdir: str) -> str:
 
 def build(params: dict, name: str | None = None, jobs: int = 8) -> str:
     """Builds (if needed) and returns the path of libref.so for `params`
-    (keys nx, ny, nz, dxi, det, dzt, high, mu, pr, stretch, twall_lo, twall_hi)."""
+    (keys nx, ny, nz, dxi, det, dzt, high, mu, pr, stretch, twall_lo, twall_hi,
+    and for the open configuration x_open, nx_inlet, nx_outlet)."""
     if not os.path.isdir(REF_SRC):
         raise FileNotFoundError(f"reference sources not found at {REF_SRC}")
     name = name or f"channel_{params['nx']}x{params['ny']}x{params['nz']}"

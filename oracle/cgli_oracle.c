@@ -20,9 +20,16 @@
  * and Nz+2).  Face arrays keep the reference's shifted indexing: the x-face
  * i+1/2 of cell (i,j,k) is stored at [i][j-1][k-1], the y-face j+1/2 at
  * [i-1][j][k-1], the z-face k+1/2 at [i-1][j-1][k] (Dual_time_stepping.cpp:
- * 810-828).  The x-direction is periodic: the reference's slab decomposition
- * collapses to one slab whose halos wrap around (main.cpp:167-200 and
- * Dual_time_stepping.cpp:942-976 with the single slab as its own neighbour).
+ * 810-828).  Two x configurations: periodic (x_open = 0), where the
+ * reference's slab decomposition collapses to one slab whose halos wrap
+ * around (main.cpp:167-200 and Dual_time_stepping.cpp:942-976 with the single
+ * slab as its own neighbour: the reference's interior-rank code paths), and
+ * open (x_open = 1), the reference's own inflow/outflow configuration run as
+ * a single rank that is both the first and the last (every myid == 0 and
+ * myid == nproc-1 branch taken): characteristic X boundaries, one-sided
+ * MUSCL stencils at the x ends, no x halo exchange, zero implicit halos,
+ * sponge layers of nx_inlet / nx_outlet cells and, optionally, the
+ * reference's buoyancy body force.
  *
  * Names below that mirror the reference: jn = "ny" (= Ny+1), kn = "nz"
  * (= Nz+1), ie = gend (= Nx+2), nyy = Ny+2, nzz = Nz+2.
@@ -45,6 +52,9 @@ typedef struct {
   double twall_lo, twall_hi;
   double force;            /* uniform x body force replacing Dual_time_stepping.cpp:831 */
   int curved_walls;        /* 1: wall-face momentum flux with the eta_x, eta_z pressure terms */
+  int x_open;              /* 1: inflow/outflow x ends (single rank 0 of 1); 0: periodic slab */
+  int nx_inlet, nx_outlet; /* sponge layers (Resolution.h), open x only */
+  int buoyancy;            /* 1: f = -(rho - 1.1842) 9.81 of Dual_time_stepping.cpp:831 */
 } or_params;
 
 typedef struct {
@@ -58,6 +68,8 @@ typedef struct {
   double *visc[3][4];                      /* face viscous fluxes LL/ML/NL 2..5 */
   double *ML[5], *MRs[5];                  /* MUSCL face states */
   double *res[5];                          /* squared increments of the update */
+  double *spg[5];                          /* sponge terms (the reference's Residual arrays) */
+  double high;                             /* channel height parameter of prm.h (or_metrics) */
 } or_state;
 
 #define IX(s, i, j, k) (((size_t)(i) * (size_t)(s)->Y + (size_t)(j)) * (size_t)(s)->Z + (size_t)(k))
@@ -77,7 +89,7 @@ or_state *or_create(const or_params *p) {
   for (int v = 0; v < 5; v++) {
     s->U_[v] = A(); s->U[v] = A(); s->Uq[v] = A();
     s->MR[v] = A(); s->NL[v] = A(); s->NR[v] = A();
-    s->ML[v] = A(); s->MRs[v] = A(); s->res[v] = A();
+    s->ML[v] = A(); s->MRs[v] = A(); s->res[v] = A(); s->spg[v] = A();
     for (int d = 0; d < 3; d++) s->inF[d][v] = A();
   }
   for (int v = 0; v < 4; v++) {
@@ -98,7 +110,7 @@ void or_destroy(or_state *s) {
   if (!s) return;
   for (int v = 0; v < 5; v++) {
     free(s->U_[v]); free(s->U[v]); free(s->Uq[v]); free(s->MR[v]); free(s->NL[v]);
-    free(s->NR[v]); free(s->ML[v]); free(s->MRs[v]); free(s->res[v]);
+    free(s->NR[v]); free(s->ML[v]); free(s->MRs[v]); free(s->res[v]); free(s->spg[v]);
     for (int d = 0; d < 3; d++) free(s->inF[d][v]);
   }
   for (int v = 0; v < 4; v++) {
@@ -127,6 +139,7 @@ double *or_array(or_state *s, const char *name) {
     snprintf(buf, sizeof buf, "inFy%d", v + 1); if (!strcmp(name, buf)) return s->inF[1][v];
     snprintf(buf, sizeof buf, "inFz%d", v + 1); if (!strcmp(name, buf)) return s->inF[2][v];
     snprintf(buf, sizeof buf, "Residual%d", v + 1); if (!strcmp(name, buf)) return s->res[v];
+    snprintf(buf, sizeof buf, "Sponge%d", v + 1); if (!strcmp(name, buf)) return s->spg[v];
   }
   for (int v = 0; v < 4; v++) {
     snprintf(buf, sizeof buf, "vF%d", v + 2); if (!strcmp(name, buf)) return s->vF[v];
@@ -157,9 +170,12 @@ void or_set_force(or_state *s, double f) { s->p.force = f; }
 
 void or_metrics(or_state *s, double high, double gam) {
   const int ie = s->p.nx + 2, jn = s->p.ny + 1, kn = s->p.nz + 1, nyy = jn + 1, nzz = kn + 1;
+  const int open = s->p.x_open;
   double **m = s->m;
-  /* cell metrics, Jacobian.cpp:61-107 (interior rank: planes 0..gend+3) */
-  for (int i = 0; i <= ie + 3; i++)
+  s->high = high;
+  /* cell metrics, Jacobian.cpp:53-107 (interior rank: planes 0..gend+3;
+   * first and last rank: 3..gend) */
+  for (int i = open ? 3 : 0; i <= (open ? ie : ie + 3); i++)
     for (int j = 2; j <= jn; j++)
       for (int k = 2; k <= kn; k++) {
         size_t c = IX(s, i, j, k);
@@ -175,9 +191,24 @@ void or_metrics(or_state *s, double high, double gam) {
         m[6][c] = 0; m[7][c] = 0; m[8][c] = 1;
         s->J[c] = 1. / (1 * ydet * 1);
       }
-  /* y ghost rows, Jacobian.cpp:169-200, with the copy typos that leave
-   * ztdy = ztdz = ztdx of the neighbour (= 0) in the ghost rows */
-  for (int i = 0; i <= ie + 3; i++)
+  /* x-end planes of the first and last rank, Jacobian.cpp:110-157: copies
+   * of the neighbouring interior plane over j, k = 1..Ny+2 / Nz+2 (its ghost
+   * rows are not set yet), where ztdx is copied three times and ztdy, ztdz
+   * of the end plane stay zero */
+  if (open)
+    for (int side = 0; side < 2; side++) {
+      int ig = side ? ie + 1 : 2, is = side ? ie : 3;
+      for (int j = 1; j <= nyy; j++)
+        for (int k = 1; k <= nzz; k++) {
+          size_t g = IX(s, ig, j, k), c = IX(s, is, j, k);
+          for (int v = 0; v < 7; v++) m[v][g] = m[v][c];
+          s->J[g] = s->J[c];
+        }
+    }
+  /* y ghost rows, Jacobian.cpp:159-200 (planes 0..gend+3, or 2..gend+1 on
+   * an open slab), with the copy typos that leave ztdy = ztdz = ztdx of the
+   * neighbour (= 0) in the ghost rows */
+  for (int i = open ? 2 : 0; i <= (open ? ie + 1 : ie + 3); i++)
     for (int k = 2; k <= kn; k++) {
       for (int side = 0; side < 2; side++) {
         int jg = side ? nyy : 1, js = side ? jn : 2;
@@ -189,8 +220,8 @@ void or_metrics(or_state *s, double high, double gam) {
       s->J[IX(s, i, 1, k)] = s->J[IX(s, i, 2, k)];
       s->J[IX(s, i, nyy, k)] = s->J[IX(s, i, jn, k)];
     }
-  /* z ghost rows, Jacobian.cpp:212-243, same typos */
-  for (int i = 0; i <= ie + 3; i++)
+  /* z ghost rows, Jacobian.cpp:203-243, same typos and plane range */
+  for (int i = open ? 2 : 0; i <= (open ? ie + 1 : ie + 3); i++)
     for (int j = 1; j <= nyy; j++) {
       for (int side = 0; side < 2; side++) {
         int kg = side ? nzz : 1, ks = side ? kn : 2;
@@ -249,7 +280,10 @@ void or_metrics(or_state *s, double high, double gam) {
 void or_initial(or_state *s, const double *q_n, const double *q_nm1) {
   const int ie = s->p.nx + 2, Ny = s->p.ny, Nz = s->p.nz;
   const int nyyy = Ny + 3, nzzz = Nz + 3;
-  for (int i = 3; i <= ie; i++)
+  /* the quiescent field of :56-97 also fills the x-end planes 2 and gend+1
+   * of the first and last rank */
+  const int open = s->p.x_open;
+  for (int i = open ? 2 : 3; i <= (open ? ie + 1 : ie); i++)
     for (int j = 0; j <= nyyy; j++)
       for (int k = 0; k <= nzzz; k++) {
         size_t c = IX(s, i, j, k);
@@ -281,6 +315,7 @@ void or_initial(or_state *s, const double *q_n, const double *q_nm1) {
 /* periodic x halo of Q/J, main.cpp:167-200 with the slab as its own neighbour */
 void or_halo_x(or_state *s) {
   const int ie = s->p.nx + 2;
+  if (s->p.x_open) return;   /* both neighbours are MPI_PROC_NULL */
   size_t plane = (size_t)s->Y * s->Z;
   for (int v = 0; v < 5; v++) {
     memmove(s->U_[v] + (size_t)(ie + 1) * plane, s->U_[v] + (size_t)3 * plane, 3 * plane * sizeof(double));
@@ -288,8 +323,10 @@ void or_halo_x(or_state *s) {
   }
 }
 
-/* no-slip isothermal walls, Y_boundary_condition.cpp:94-182 (the heated
- * section covers every x plane when there is no inlet/outlet sponge) */
+/* walls, Y_boundary_condition.cpp:94-182: zero-gradient copy, then
+ * no-slip isothermal reflection inside the heated section (global plane
+ * i + gstart in (nx_inlet + 2, X_out - nx_outlet + 3), :114; every plane
+ * without sponge layers; the slab is planes 1..Nx of the x extent here) */
 void or_bc_y(or_state *s) {
   const int ie = s->p.nx + 2, jn = s->p.ny + 1, kn = s->p.nz + 1, nyy = jn + 1;
   double **q = s->U_;
@@ -300,6 +337,7 @@ void or_bc_y(or_state *s) {
         q[v][IX(s, i, 1, k)] = q[v][IX(s, i, 2, k)];
         q[v][IX(s, i, nyy, k)] = q[v][IX(s, i, jn, k)];
       }
+    if (!(i > s->p.nx_inlet + 2 && i < s->p.nx - s->p.nx_outlet + 3)) continue;
     for (int k = 2; k <= kn; k++) {
       for (int side = 0; side < 2; side++) {
         int js = side ? jn : 2, jg = side ? nyy : 1;
@@ -322,10 +360,129 @@ void or_bc_y(or_state *s) {
   }
 }
 
+/* characteristic inflow / outflow ghost planes of an open slab,
+ * X_boundary_condition.cpp:73-338: the ghost cell of each interior row takes
+ * one pseudo-time step of deltaT/200 with M (Gamma + 3 dtau/(2 dt) M)^-1
+ * applied to the wave amplitudes (outgoing from the one-sided x
+ * differences, incoming zero) plus the BDF2 time derivative.  side 0:
+ * inlet plane 2 against plane 3; side 1: outlet plane gend+1 against gend. */
+static void bc_x_side(or_state *s, int side) {
+  const int ie = s->p.nx + 2, jn = s->p.ny + 1, kn = s->p.nz + 1;
+  const double K = KG, deltaT = s->p.dt, deltaTau = deltaT / 200., e = s->p.e, dXI = s->p.dxi;
+  const int ig = side ? ie + 1 : 2, ii = side ? ie : 3;
+  double **q = s->U_, **u = s->U, **uq = s->Uq;
+  const double *Jc = s->J;
+  for (int j = 2; j <= jn; j++)
+    for (int k = 2; k <= kn; k++) {
+      size_t c = IX(s, ii, j, k), g = IX(s, ig, j, k);
+      /* the interior neighbour */
+      double rho_ = q[0][c] * Jc[c];
+      double U_ = q[1][c] / q[0][c];
+      double V_ = q[2][c] / q[0][c];
+      double W_ = q[3][c] / q[0][c];
+      double VV_ = U_ * U_ + V_ * V_ + W_ * W_;
+      double P_ = (q[4][c] * Jc[c] - 0.5 * rho_ * VV_) * (K - 1);
+      double T_ = P_ / rho_;
+      (void)VV_;
+      /* the ghost cell */
+      double rho = q[0][g] * Jc[g];
+      double U = q[1][g] / q[0][g];
+      double V = q[2][g] / q[0][g];
+      double W = q[3][g] / q[0][g];
+      double VV = U * U + V * V + W * W;
+      double P = (q[4][g] * Jc[g] - 0.5 * rho * VV) * (K - 1);
+      double C = sqrt(K * P / rho);
+      double T = P / rho;
+      double H = 0.5 * VV + C * C / (K - 1);
+      double beta = MAX(VV / C / C, e);
+      double temp = K * T * (2 * deltaT + 3 * deltaTau) * (2 * deltaT + 3 * beta * deltaTau);
+      double temp2 = (K - 1) * (beta - 1) * deltaT * deltaT;
+      double temp3 = H - H * K - VV + K * (T + VV);
+      double d[5][5];
+      d[0][0] = (2 * deltaT * (-2 * (-(K - 1) * (H - VV) - temp3 * beta) * deltaT + 3 * K * T * beta * deltaTau)) / temp;
+      d[0][1] = (-4 * U * temp2) / temp;
+      d[0][2] = (-4 * V * temp2) / temp;
+      d[0][3] = (-4 * W * temp2) / temp;
+      d[0][4] = (4 * temp2) / temp;
+      d[1][0] = (4 * U * temp3 * (beta - 1) * deltaT * deltaT) / temp;
+      d[1][1] = (2 * deltaT * (2 * K * (T - U * U * (beta - 1)) * deltaT + 2 * U * U * (beta - 1) * deltaT + 3 * K * T * beta * deltaTau)) / temp;
+      d[1][2] = (-4 * U * V * temp2) / temp;
+      d[1][3] = (-4 * U * W * temp2) / temp;
+      d[1][4] = (4 * U * temp2) / temp;
+      d[2][0] = (4 * V * temp3 * (beta - 1) * deltaT * deltaT) / temp;
+      d[2][1] = (-4 * U * V * temp2) / temp;
+      d[2][2] = (2 * deltaT * (2 * K * (T - V * V * (beta - 1)) * deltaT + 2 * V * V * (beta - 1) * deltaT + 3 * K * T * beta * deltaTau)) / temp;
+      d[2][3] = (-4 * V * W * temp2) / temp;
+      d[2][4] = (4 * V * temp2) / temp;
+      d[3][0] = (4 * W * temp3 * (beta - 1) * deltaT * deltaT) / temp;
+      d[3][1] = (-4 * U * W * temp2) / temp;
+      d[3][2] = (-4 * V * W * temp2) / temp;
+      d[3][3] = (2 * deltaT * (2 * K * (T - W * W * (beta - 1)) * deltaT + 2 * W * W * (beta - 1) * deltaT + 3 * K * T * beta * deltaTau)) / temp;
+      d[3][4] = (4 * W * temp2) / temp;
+      d[4][0] = (4 * H * temp3 * (beta - 1) * deltaT * deltaT) / temp;
+      d[4][1] = (-4 * H * U * temp2) / temp;
+      d[4][2] = (-4 * H * V * temp2) / temp;
+      d[4][3] = (-4 * H * W * temp2) / temp;
+      d[4][4] = (2 * deltaT * (2 * H * (K - 1) * (beta - 1) * deltaT + K * T * (2 * deltaT + 3 * beta * deltaTau))) / temp;
+      double U_p = 0.5 * (beta + 1) * U;
+      double C_p = 0.5 * sqrt(U * U * (beta - 1) * (beta - 1) + 4 * beta * C * C);
+      double dp_dx, du_dx, dv_dx, dw_dx, dT_dx, L1, L2, L3, L4, L5;
+      if (!side) {   /* :151-187: L5 leaves through the inlet, L4 from it */
+        dp_dx = (P_ - P) / dXI;
+        du_dx = (U_ - U) / dXI;
+        dv_dx = (V_ - V) / dXI;
+        dw_dx = (W_ - W) / dXI;
+        dT_dx = (T_ - T) / dXI;
+        L5 = (U_p - C_p) * (dp_dx - rho * (U_p + C_p - U) * du_dx);
+        L4 = L5 * (U_p - C_p - U) / (U_p + C_p - U);
+        if (U <= 0) {
+          L1 = U * (dT_dx + 1.0 / rho * dp_dx * (1 - K) / K);
+          L2 = U * dw_dx;
+          L3 = -U * dv_dx;
+        } else {
+          L1 = L2 = L3 = 0;
+        }
+      } else {       /* :292-327 */
+        dp_dx = (P - P_) / dXI;
+        du_dx = (U - U_) / dXI;
+        dv_dx = (V - V_) / dXI;
+        dw_dx = (W - W_) / dXI;
+        dT_dx = (T - T_) / dXI;
+        L4 = (U_p + C_p) * (dp_dx - rho * (U_p - C_p - U) * du_dx);
+        L5 = L4 * (U_p + C_p - U) / (U_p - C_p - U);
+        if (U > 0) {
+          L1 = U * (dT_dx + 1.0 / rho * dp_dx * (1 - K) / K);
+          L2 = U * dw_dx;
+          L3 = -U * dv_dx;
+        } else {
+          L1 = L2 = L3 = 0;
+        }
+      }
+      double KAL[5];
+      KAL[0] = 0.5 / (C_p) * (L4 * (U_p + C_p - U) - L5 * (U_p - C_p - U));
+      KAL[1] = 0.5 / (rho * C_p) * (L4 - L5);
+      KAL[2] = -L3;
+      KAL[3] = L2;
+      KAL[4] = L1 + 1. / rho * (K - 1) / K * KAL[0];
+      for (int v = 0; v < 5; v++)
+        KAL[v] = KAL[v] / Jc[g] + (3 * q[v][g] - 4 * u[v][g] + uq[v][g]) / (2 * deltaT);
+      for (int v = 0; v < 5; v++)
+        q[v][g] = q[v][g] - deltaTau * (d[v][0] * KAL[0] + d[v][1] * KAL[1] + d[v][2] * KAL[2] + d[v][3] * KAL[3] +
+                                        d[v][4] * KAL[4]);
+    }
+}
+
+void or_bc_x(or_state *s) {
+  if (!s->p.x_open) return;   /* interior rank: no-op */
+  bc_x_side(s, 0);
+  bc_x_side(s, 1);
+}
+
 /* periodic z ghosts, Z_boundary_condition.cpp:39-66 (all planes, all rows) */
 void or_bc_z(or_state *s) {
   const int ie = s->p.nx + 2, kn = s->p.nz + 1, nzz = kn + 1, nyyy = s->p.ny + 3;
-  for (int i = 0; i <= ie + 3; i++)
+  const int open = s->p.x_open;   /* :40-44: planes 2..gend+1 on an open slab */
+  for (int i = open ? 2 : 0; i <= (open ? ie + 1 : ie + 3); i++)
     for (int j = 0; j <= nyyy; j++)
       for (int v = 0; v < 5; v++) {
         s->U_[v][IX(s, i, j, 1)] = s->U_[v][IX(s, i, j, kn)];
@@ -417,11 +574,15 @@ static void roe_face(const double L[5], const double Rr[5], double mx, double my
   if (pp_out) *pp_out = iP + P_;
 }
 
-/* x-direction inviscid flux, Flux_X.cpp:96-357 on an interior rank */
+/* x-direction inviscid flux, Flux_X.cpp:96-357.  Interior rank: 5-point
+ * states for i = 2..gend+1.  Open slab: 5-point for i = 4..gend-1 and the
+ * first / last rank's reduced stencils of :139-216 (2-point states on the
+ * end faces, 3-point on the next ones) */
 void or_flux_x(or_state *s) {
   const int ie = s->p.nx + 2, jn = s->p.ny + 1, kn = s->p.nz + 1;
   const size_t di = (size_t)s->Y * s->Z;
-  for (int i = 2; i <= ie + 1; i++)
+  const int open = s->p.x_open;
+  for (int i = open ? 4 : 2; i <= (open ? ie - 1 : ie + 1); i++)
     for (int j = 2; j <= jn; j++)
       for (int k = 2; k <= kn; k++) {
         size_t c = IX(s, i, j, k);
@@ -429,6 +590,21 @@ void or_flux_x(or_state *s) {
         for (int v = 0; v < 5; v++) {
           s->ML[v][fl] = m5L(s->U_[v], s->J, c - 2 * di, c - di, c, c + di, c + 2 * di);
           s->MRs[v][fr] = m5R(s->U_[v], s->J, c - 2 * di, c - di, c, c + di, c + 2 * di);
+        }
+      }
+  if (open)
+    for (int j = 2; j <= jn; j++)
+      for (int k = 2; k <= kn; k++) {
+        size_t a = IX(s, 2, j, k), b = a + di, c = b + di;          /* planes 2, 3, 4 */
+        size_t y = IX(s, ie - 1, j, k), z = y + di, w = z + di;    /* planes ie-1, ie, ie+1 */
+        for (int v = 0; v < 5; v++) {
+          const double *u = s->U_[v];
+          s->ML[v][IX(s, 2, j - 1, k - 1)] = m2(u, s->J, a, b);
+          s->ML[v][IX(s, 3, j - 1, k - 1)] = m3L(u, s->J, a, b, c);
+          s->MRs[v][IX(s, 2, j - 1, k - 1)] = m3R(u, s->J, a, b, c);
+          s->ML[v][IX(s, ie, j - 1, k - 1)] = m3L(u, s->J, y, z, w);
+          s->MRs[v][IX(s, ie - 1, j - 1, k - 1)] = m3R(u, s->J, y, z, w);
+          s->MRs[v][IX(s, ie, j - 1, k - 1)] = m2(u, s->J, z, w);
         }
       }
   double **mf = s->mf[0];
@@ -857,8 +1033,80 @@ static inline splitj split_at(const or_state *s, size_t c, int dir) {
   return a;
 }
 
-/* residual assembly, Dual_time_stepping.cpp:737-922 */
-void or_dts_residual(or_state *s) {
+/* sponge layers, Dual_time_stepping.cpp:327-664: the Residual arrays are
+ * zeroed, then the first nx_inlet and the last nx_outlet interior planes of
+ * the x extent (an open slab is the whole extent) get the absorbing terms.
+ * The inlet profile uses the slab's first global index where the outlet one
+ * uses the plane's (:586 against :644).  The outlet target velocity is the
+ * volume mean of u over plane 3, rows 2..Ny+2 and 2..Nz+2 (:510-532). */
+static void or_sponge(or_state *s) {
+  const int ie = s->p.nx + 2, jn = s->p.ny + 1, kn = s->p.nz + 1, nyy = jn + 1, nzz = kn + 1;
+  const size_t n = or_n(s);
+  for (int v = 0; v < 5; v++) memset(s->spg[v], 0, n * sizeof(double));
+  if (!s->p.x_open) return;
+  const int nxin = s->p.nx_inlet, nxout = s->p.nx_outlet, Xout = s->p.nx, gstart = 0;
+  const double dXI = s->p.dxi, dET = s->p.det, dZT = s->p.dzt, high = s->high, e = s->p.e;
+  double z1 = 0.0;
+  const double DZ = 1. / (high * dZT * s->p.nz);
+  for (int j = 2; j <= nyy; j++)
+    for (int k = 2; k <= nzz; k++) {
+      size_t c = IX(s, 3, j, k);
+      double U = s->U_[1][c] / s->U_[0][c];
+      z1 = z1 + U * dET / s->m[4][c] * dZT;
+    }
+  const double targetU = z1 * DZ;
+  const double U_in_0 = 1.0, Sigma_in_0 = 0.035, U_out_0 = 1.0, Sigma_out_0 = 1.25;
+  for (int side = 0; side < 2; side++) {
+    int i0, i1;
+    if (!side) {
+      if (!(gstart < nxin)) continue;
+      i0 = 3; i1 = (Xout - 1 < nxin) ? ie : nxin - gstart + 2;
+    } else {
+      if (!(Xout - 1 > Xout - nxout - 1)) continue;
+      i0 = (gstart > Xout - nxout - 1) ? 3 : (Xout - nxout) - gstart + 2;
+      i1 = ie;
+    }
+    for (int i = i0; i <= i1; i++)
+      for (int j = 2; j <= jn; j++)
+        for (int k = 2; k <= kn; k++) {
+          size_t c = IX(s, i, j, k), b = c - (size_t)s->Y * s->Z;
+          double **q = s->U_;
+          const double *J = s->J;
+          double rho = q[0][c] * J[c];
+          double u = q[1][c] / q[0][c];
+          double v = q[2][c] / q[0][c];
+          double w = q[3][c] / q[0][c];
+          double VV = u * u + v * v + w * w;
+          double P = (q[4][c] * J[c] - 0.5 * rho * VV) * (KG - 1);
+          double C = KG * P / rho;
+          double beta = MAX(VV / C, e);
+          double C_plan = 0.5 * sqrt(u * u * (beta - 1) * (beta - 1) + 4 * beta * C);
+          double Us, Sig, t2 = 0, t5 = 0;
+          if (!side) {
+            Us = pow((((nxin - gstart - 0.5) * 1.0) / nxin), 3.0) * U_in_0 * C_plan;
+            Sig = Sigma_in_0 * Us / high;
+          } else {
+            /* nx of Resolution.h is X_out + 1 */
+            Us = pow((((i + gstart - 0.5 - ((Xout + 1) - nxout)) * 1.0) / nxout), 3.0) * U_out_0 * C_plan;
+            Sig = Sigma_out_0 * Us / high;
+            t2 = 1.1842 * targetU;
+            t5 = 0.5 * 1.1842 * targetU * targetU;
+          }
+          double **sp = s->spg;
+          sp[0][c] = -Us * (q[0][c] * J[c] - q[0][b] * J[b]) / dXI - Sig * (rho - 1.1842);
+          sp[1][c] = -Us * (q[1][c] * J[c] - q[1][b] * J[b]) / dXI - Sig * (side ? rho * u - t2 : rho * u);
+          sp[2][c] = -Us * (q[2][c] * J[c] - q[2][b] * J[b]) / dXI - Sig * (rho * v);
+          sp[3][c] = -Us * (q[3][c] * J[c] - q[3][b] * J[b]) / dXI - Sig * (rho * w);
+          sp[4][c] = -Us * (q[4][c] * J[c] - q[4][b] * J[b]) / dXI -
+                     Sig * (side ? q[4][c] * J[c] - 253250.0 - t5 : q[4][c] * J[c] - 253250.0);
+        }
+  }
+}
+
+/* residual assembly, Dual_time_stepping.cpp:737-922; with dplusgs, that of
+ * DPLUSGS.cpp:324-478, which has no sponge terms and always the uniform
+ * force */
+static void dts_residual(or_state *s, int dplusgs) {
   const int ie = s->p.nx + 2, jn = s->p.ny + 1, kn = s->p.nz + 1, nyy = jn + 1, nzz = kn + 1;
   const double deltaT = s->p.dt, dXI = s->p.dxi, dET = s->p.det, dZT = s->p.dzt;
   /* ghost rows of NL/NR are zero, :255-323 */
@@ -874,7 +1122,16 @@ void or_dts_residual(or_state *s) {
         s->NL[v][IX(s, i, j, nzz)] = 0; s->NR[v][IX(s, i, j, nzz)] = 0;
       }
   }
-  const double zero = 0.0;   /* the sponge Residual arrays, zero without inlet/outlet */
+  if (s->p.x_open)   /* :204-246: the end planes of the first and last rank */
+    for (int side = 0; side < 2; side++) {
+      int ig = side ? ie + 1 : 2;
+      for (int j = 1; j <= nyy; j++)
+        for (int k = 1; k <= nzz; k++)
+          for (int v = 0; v < 5; v++) { s->NL[v][IX(s, ig, j, k)] = 0; s->NR[v][IX(s, ig, j, k)] = 0; }
+    }
+  or_sponge(s);
+  if (dplusgs)
+    for (int v = 0; v < 5; v++) memset(s->spg[v], 0, or_n(s) * sizeof(double));
   for (int i = 3; i <= ie; i++)
     for (int j = 2; j < nyy; j++)
       for (int k = 2; k < nzz; k++) {
@@ -904,12 +1161,13 @@ void or_dts_residual(or_state *s) {
                     (s->inF[1][n][fy1] - s->inF[1][n][fy0]) / dET +
                     (s->inF[2][n][fz1] - s->inF[2][n][fz0]) / dZT);
         }
-        double f = s->p.force;
-        Rk[0] = zero / J + Rp[0] + Rf[0];
-        Rk[1] = zero / J + Rp[1] + Rf[1] + s->vF[0][c] + f / J;
-        Rk[2] = zero / J + Rp[2] + Rf[2] + s->vF[1][c];
-        Rk[3] = zero / J + Rp[3] + Rf[3] + s->vF[2][c];
-        Rk[4] = zero / J + Rp[4] + Rf[4] + s->vF[3][c] + f * u / J;
+        double f = (s->p.buoyancy && !dplusgs) ? -(rho - 1.1842) * 9.81 : s->p.force;   /* :831 */
+        double **sp = s->spg;
+        Rk[0] = sp[0][c] / J + Rp[0] + Rf[0];
+        Rk[1] = sp[1][c] / J + Rp[1] + Rf[1] + s->vF[0][c] + f / J;
+        Rk[2] = sp[2][c] / J + Rp[2] + Rf[2] + s->vF[1][c];
+        Rk[3] = sp[3][c] / J + Rp[3] + Rf[3] + s->vF[2][c];
+        Rk[4] = sp[4][c] / J + Rp[4] + Rf[4] + s->vF[3][c] + f * u / J;
         double MR1 = (d11 * Rk[0] + d12 * Rk[1] + d13 * Rk[2] + d14 * Rk[3] + d15 * Rk[4]);
         double MR2 = (d21 * Rk[0] + d22 * Rk[1] + d23 * Rk[2] + d24 * Rk[3] + d25 * Rk[4]);
         double MR3 = (d31 * Rk[0] + d32 * Rk[1] + d33 * Rk[2] + d34 * Rk[3] + d35 * Rk[4]);
@@ -925,6 +1183,9 @@ void or_dts_residual(or_state *s) {
       }
   (void)dXI; (void)dET; (void)dZT;
 }
+
+void or_dts_residual(or_state *s) { dts_residual(s, 0); }
+void or_dplur_residual(or_state *s) { dts_residual(s, 1); }
 
 /* forward sweep at one cell, Dual_time_stepping.cpp:1017-1293 */
 static void forward_cell(or_state *s, int i, int j, int k) {
@@ -990,7 +1251,7 @@ void or_sweeps(or_state *s) {
   const int ie = s->p.nx + 2, jn = s->p.ny + 1, kn = s->p.nz + 1;
   const size_t plane = (size_t)s->Y * s->Z;
   for (int sweep = 1; sweep <= 2; sweep++) {
-    for (int v = 0; v < 5; v++) {
+    for (int v = 0; v < 5 && !s->p.x_open; v++) {   /* open: the end planes stay zero */
       memmove(s->NL[v] + 2 * plane, s->NL[v] + (size_t)ie * plane, plane * sizeof(double));
       memmove(s->NR[v] + (size_t)(ie + 1) * plane, s->NR[v] + 3 * plane, plane * sizeof(double));
     }
@@ -1112,7 +1373,7 @@ void or_dplur_sweeps(or_state *s) {
   const int ie = s->p.nx + 2, jn = s->p.ny + 1, kn = s->p.nz + 1;
   const size_t plane = (size_t)s->Y * s->Z;
   for (int sweep = 1; sweep <= 4; sweep++) {
-    for (int v = 0; v < 5; v++) {
+    for (int v = 0; v < 5 && !s->p.x_open; v++) {   /* open: the end planes stay zero */
       memmove(s->NL[v] + 2 * plane, s->NL[v] + (size_t)ie * plane, plane * sizeof(double));
       memmove(s->NL[v] + (size_t)(ie + 1) * plane, s->NL[v] + 3 * plane, plane * sizeof(double));
     }
@@ -1184,12 +1445,13 @@ void or_dplur_update(or_state *s, double *er) {
 void or_dplur_inner_iteration(or_state *s, double *er) {
   or_halo_x(s);
   or_bc_y(s);
+  or_bc_x(s);
   or_bc_z(s);
   or_flux_x(s);
   or_flux_y(s);
   or_flux_z(s);
   or_viscous(s);
-  or_dts_residual(s);
+  or_dplur_residual(s);
   or_dplur_sweeps(s);
   or_dplur_update(s, er);
 }
@@ -1198,6 +1460,7 @@ void or_dplur_inner_iteration(or_state *s, double *er) {
 void or_inner_iteration(or_state *s, double *er) {
   or_halo_x(s);
   or_bc_y(s);
+  or_bc_x(s);
   or_bc_z(s);
   or_flux_x(s);
   or_flux_y(s);

@@ -30,7 +30,9 @@ class _Params(ctypes.Structure):
                 ("dt", ctypes.c_double), ("e", ctypes.c_double),
                 ("mu", ctypes.c_double), ("pr", ctypes.c_double),
                 ("twall_lo", ctypes.c_double), ("twall_hi", ctypes.c_double),
-                ("force", ctypes.c_double), ("curved_walls", ctypes.c_int)]
+                ("force", ctypes.c_double), ("curved_walls", ctypes.c_int),
+                ("x_open", ctypes.c_int), ("nx_inlet", ctypes.c_int), ("nx_outlet", ctypes.c_int),
+                ("buoyancy", ctypes.c_int)]
 
 
 _lib = None
@@ -50,8 +52,8 @@ def _load():
         L.or_set_force.argtypes = [ctypes.c_void_p, ctypes.c_double]
         L.or_bulk_flux.restype = ctypes.c_double
         L.or_bulk_flux.argtypes = [ctypes.c_void_p]
-        for name in ("or_halo_x", "or_bc_y", "or_bc_z", "or_flux_x", "or_flux_y", "or_flux_z",
-                     "or_viscous", "or_dts_residual", "or_sweeps", "or_end_step"):
+        for name in ("or_halo_x", "or_bc_y", "or_bc_x", "or_bc_z", "or_flux_x", "or_flux_y", "or_flux_z",
+                     "or_viscous", "or_dts_residual", "or_dplur_residual", "or_sweeps", "or_end_step"):
             getattr(L, name).argtypes = [ctypes.c_void_p]
         L.or_update.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.or_inner_iteration.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
@@ -84,8 +86,9 @@ class Oracle:
         self.ch = ch
         self.L = _load()
         p = _Params(ch.nx, ch.ny, ch.nz, ch.dxi, ch.det, ch.dzt, ch.dt,
-                    C.PRECOND_EPS if e is None else e, C.MU0, C.PR, C.T0, C.T0, ch.force_lam,
-                    int(ch.wavy if curved_walls is None else curved_walls))
+                    C.PRECOND_EPS if e is None else e, C.MU0, C.PR, ch.twall_lo, ch.twall_hi, ch.force_lam,
+                    int(ch.wavy if curved_walls is None else curved_walls),
+                    int(ch.x_open), ch.nx_inlet, ch.nx_outlet, int(ch.buoyancy))
         self.s = self.L.or_create(ctypes.byref(p))
         self.shape = ch.shape
         self.force = ch.force_lam

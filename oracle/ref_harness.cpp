@@ -11,9 +11,12 @@
  *
  * The grid sizes are compile-time constants of the generated Resolution.h,
  * exactly as in the reference; one library is built per configuration.
- * The run is a single process that the MPI stub presents as rank 1 of 3,
- * which makes every routine take its interior path and turns the x halos
- * into periodic self-copies (see mpi_stub/mpi.h).
+ * The run is a single process.  For the periodic channel the MPI stub
+ * presents it as rank 1 of 3 (CGLI_MYID 1, CGLI_NSLAB 3), which makes every
+ * routine take its interior path and turns the x halos into periodic
+ * self-copies (see mpi_stub/mpi.h); for the open (inflow/outflow)
+ * configuration as rank 0 of 1, which takes every first- and last-rank
+ * branch.
  */
 #include <mpi.h>
 #include <omp.h>
@@ -24,11 +27,13 @@
 
 #include "Resolution.h"
 
-int cgli_stub_rank = 1;
-int cgli_stub_size = 3;
+int cgli_stub_rank = CGLI_MYID;
+int cgli_stub_size = CGLI_NSLAB;
 char cgli_stub_initial_path[4096];
-/* value the patched body-force line of Dual_time_stepping.cpp:831 reads */
+/* values the patched body-force line of Dual_time_stepping.cpp:831 reads:
+ * the reference's buoyancy when cgli_ref_buoyancy, else the uniform force */
 double cgli_ref_force = 0.0;
+int cgli_ref_buoyancy = 0;
 int X_np;
 
 typedef double (*A3)[Y_m][Z_m];
@@ -80,7 +85,7 @@ void Filter(int, double, double, double, A3, A3, A3, A3, A3, A3, A3, A3, A3, A3)
 
 namespace {
 
-const int MYID = 1;
+const int MYID = CGLI_MYID;
 
 struct Arrays {
   A3 U_[5], U[5], Uq[5];
@@ -98,7 +103,7 @@ Arrays A;
 bool allocated = false;
 double g_dt = 0.0, g_e = 1e-4;
 
-int gend1() { return (X_out / 3) + 2; } /* gend[1] of Mpi_division.h for nproc=3 */
+int gend1() { return (X_out / CGLI_NSLAB) + 2; } /* gend[MYID] of Mpi_division.h */
 
 A3 alloc3() {
   /* value-initialised, unlike Array.h:7-186 (patch P10) */
@@ -112,8 +117,8 @@ struct Named { const char *name; A3 *slot; };
 extern "C" {
 
 int ref_dims(int *out) {
-  out[0] = X_out / 3; out[1] = Y_out; out[2] = Z_out;
-  out[3] = X_out / 3 + 6; out[4] = Y_m; out[5] = Z_m;
+  out[0] = X_out / CGLI_NSLAB; out[1] = Y_out; out[2] = Z_out;
+  out[3] = X_out / CGLI_NSLAB + 6; out[4] = Y_m; out[5] = Z_m;
   return 0;
 }
 
@@ -150,7 +155,7 @@ long ref_check_hyperplanes() {
   for (int m = 7; m <= iend + ny + nz; m++) {
     if (N2[m][0] != A.Nijk[m][0] || N2[m][1] != A.Nijk[m][1]) bad++;
   }
-  long n = (long)(X_out / 3) * Y_out * Z_out;
+  long n = (long)(X_out / CGLI_NSLAB) * Y_out * Z_out;
   for (long t = 1; t <= n; t++)
     for (int d = 0; d < 3; d++) if (c2[t][d] != A.ijk[t][d]) bad++;
   free(N2); free(c2);
@@ -161,7 +166,7 @@ long ref_check_hyperplanes() {
  * from a restart file in the layout of Initial_condition.cpp:136-221 */
 /* arrays, hyperplane lists and the reference's metrics */
 int ref_setup(double deltaT, double e) {
-  X_np = X_out / 3 + 6;
+  X_np = X_out / CGLI_NSLAB + 6;
   if (!allocated) {
     for (int v = 0; v < 5; v++) {
       A.U_[v] = alloc3(); A.U[v] = alloc3(); A.Uq[v] = alloc3();
@@ -213,6 +218,7 @@ int ref_init(const char *initial_path, double deltaT, double e) {
 }
 
 void ref_set_force(double f) { cgli_ref_force = f; }
+void ref_set_buoyancy(int on) { cgli_ref_buoyancy = on; }
 double ref_get_force(void) { return cgli_ref_force; }
 
 double *ref_array(const char *name) {
@@ -249,7 +255,8 @@ double *ref_array(const char *name) {
  * Y, X and Z boundary routines in the reference's order */
 void ref_halo_bc(void) {
   int istart = 3, iend = gend1();
-  int l_nbr = MYID - 1, r_nbr = MYID + 1;
+  int l_nbr = MYID == 0 ? MPI_PROC_NULL : MYID - 1;
+  int r_nbr = MYID == CGLI_NSLAB - 1 ? MPI_PROC_NULL : MYID + 1;
   int icount = 3 * Y_m * Z_m;
   MPI_Status st[8];
   for (int v = 0; v < 5; v++)
@@ -363,7 +370,7 @@ double ref_bulk_flux(void) {
         temp = (A.U_[1][i][j][k] * A.J[i][j][k]) * 1. / A.J[i][j][k] / Jsum;
         Q = Q + temp;
       }
-  return Q / (X_out / 3) / Z_out;
+  return Q / (X_out / CGLI_NSLAB) / Z_out;
 }
 
 /* end of a physical step, main.cpp:307 and main.cpp:364-386 */

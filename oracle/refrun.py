@@ -27,7 +27,9 @@ class RefSolver:
         self.inner_solver = inner_solver
         params = dict(nx=ch.nx, ny=ch.ny, nz=ch.nz, dxi=ch.dxi, det=ch.det, dzt=ch.dzt,
                       high=ch.high, mu=_c().MU0, pr=_c().PR, stretch=_c().STRETCH,
-                      twall_lo=_c().T0, twall_hi=_c().T0)
+                      twall_lo=ch.twall_lo, twall_hi=ch.twall_hi)
+        if ch.x_open:
+            params.update(x_open=1, nx_inlet=ch.nx_inlet, nx_outlet=ch.nx_outlet)
         if build:
             path = build_ref.build(params, ch.name)
         else:
@@ -40,6 +42,7 @@ class RefSolver:
         L.ref_setup.argtypes = [ctypes.c_double, ctypes.c_double]
         L.ref_load.argtypes = [ctypes.c_char_p]
         L.ref_set_force.argtypes = [ctypes.c_double]
+        L.ref_set_buoyancy.argtypes = [ctypes.c_int]
         L.ref_bulk_flux.restype = ctypes.c_double
         L.ref_check_hyperplanes.restype = ctypes.c_long
         L.ref_filter.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double]
@@ -63,13 +66,17 @@ class RefSolver:
             q_nm1 = q_n
         with tempfile.TemporaryDirectory() as td:
             path = os.path.join(td, "initial.bin")
-            ch.write_restart(path, q_n, q_nm1)
+            if ch.x_open:
+                ch.write_restart(path, q_n, q_nm1, ranks=1, rank=0)
+            else:
+                ch.write_restart(path, q_n, q_nm1)
             self.lib.ref_setup(ch.dt, _c().PRECOND_EPS)
             if ch.wavy:
                 from .oracle import load_wavy_metrics
                 load_wavy_metrics(self.array, ch)
             self.lib.ref_load(path.encode())
         self.lib.ref_set_force(self.force)
+        self.lib.ref_set_buoyancy(int(ch.buoyancy))
 
     def load(self, path: str) -> None:
         """Set-up, then the initial field read from a restart file written

@@ -16,7 +16,12 @@ solver of DPLUSGS.cpp run in place of Dual_time_stepping (dplur_<workload>:
 the first iteration's MR / NR / U_ hashes, three steps' norms, forces and
 final state).
 
-Usage:  python tests/golden/make_golden.py [--filter | --dplur] [nx ny nz]
+The reference's own open configuration (inflow / outflow x ends with
+characteristic boundaries, sponge layers, heated-section walls, buoyancy),
+run as a single rank 0 of 1: open_<workload> (three steps' norms and final
+state with each inner solver).
+
+Usage:  python tests/golden/make_golden.py [--filter | --dplur | --open] [nx ny nz]
 """
 from __future__ import annotations
 
@@ -175,6 +180,36 @@ def main_dplur(nx=8, ny=12, nz=8):
     print("wrote", base + ".json", base + ".npz")
 
 
+def open_channel(nx=16, ny=12, nz=8):
+    """The open-configuration fixture's workload: 4-cell inlet and outlet
+    sponges, heated lower wall at the reference's 343.0592 K, buoyancy."""
+    return Channel(nx, ny, nz, x_open=True, nx_inlet=4, nx_outlet=4, buoyancy=True, twall_lo=343.0592)
+
+
+def main_open(nx=16, ny=12, nz=8):
+    ch = open_channel(nx, ny, nz)
+    out = {"workload": ch.name, "cells": [nx, ny, nz], "nx_inlet": ch.nx_inlet, "nx_outlet": ch.nx_outlet,
+           "twall_lo": ch.twall_lo, "buoyancy": True, "steps": STEPS, "iters_per_step": ITERS}
+    arrays = {}
+    sl = (slice(None), slice(2, nx + 4), slice(2, ny + 2), slice(2, nz + 2))   # with the x-end ghost planes
+    for solver in ("lusgs", "dplur"):
+        r = RefSolver(ch, threads=1, inner_solver=solver)
+        r.init()
+        norms, forces = [], [r.force]
+        for _ in range(STEPS):
+            _, e = r.step(ITERS)
+            norms.append(list(e))
+            forces.append(r.force)
+        q = r.q()[sl]
+        out[solver] = {"step_norms": norms, "forces": forces, "final_state": digest(q)}
+        arrays[solver] = q
+    base = os.path.join(HERE, "open_" + f"{nx}x{ny}x{nz}")
+    np.savez_compressed(base + ".npz", **arrays)
+    with open(base + ".json", "w") as fh:
+        json.dump(out, fh, indent=1)
+    print("wrote", base + ".json", base + ".npz")
+
+
 if __name__ == "__main__":
     argv = sys.argv[1:]
     which = main
@@ -182,5 +217,7 @@ if __name__ == "__main__":
         which, argv = main_filter, argv[1:]
     elif argv and argv[0] == "--dplur":
         which, argv = main_dplur, argv[1:]
-    args = [int(a) for a in argv[0:3]] or [8, 12, 8]
+    elif argv and argv[0] == "--open":
+        which, argv = main_open, argv[1:]
+    args = [int(a) for a in argv[0:3]] or ([16, 12, 8] if which is main_open else [8, 12, 8])
     which(*args)
