@@ -259,6 +259,12 @@ int cgli_create(const cgli_params *p, cgli_ctx **out) {
     return fail(CGLI_EINVAL, "precision must be CGLI_FP64 or CGLI_MIXED");
   if (!(p->dxi > 0 && p->det > 0 && p->dzt > 0 && p->dt > 0 && p->e > 0 && p->mu > 0 && p->pr > 0))
     return fail(CGLI_EINVAL, "spacings, time step, e, mu and Pr must be positive");
+  if (p->nx_inlet < 0 || p->nx_outlet < 0 || p->nx_inlet + p->nx_outlet > p->nx)
+    return fail(CGLI_EINVAL, "sponge layers must satisfy 0 <= nx_inlet, nx_outlet and nx_inlet + nx_outlet <= Nx");
+  if (!p->x_open && (p->nx_inlet || p->nx_outlet))
+    return fail(CGLI_EINVAL, "sponge layers need x_open (a periodic slab has no inlet or outlet)");
+  if ((p->nx_inlet || p->nx_outlet) && !(p->high > 0))
+    return fail(CGLI_EINVAL, "sponge layers need the channel height `high` > 0");
   cgli_ctx *c = new cgli_ctx();
   c->p = *p;
   cudaError_t e = cudaGetDevice(&c->device);
@@ -271,6 +277,11 @@ int cgli_create(const cgli_params *p, cgli_ctx **out) {
   d.dxi = p->dxi; d.det = p->det; d.dzt = p->dzt; d.dt = p->dt; d.e = p->e;
   d.mu = p->mu; d.pr = p->pr; d.twl = p->twall_lo; d.twh = p->twall_hi;
   d.curved_walls = p->curved_walls ? 1 : 0;
+  d.x_open = p->x_open ? 1 : 0;
+  d.nx_inlet = p->nx_inlet;
+  d.nx_outlet = p->nx_outlet;
+  d.buoyancy = p->buoyancy ? 1 : 0;
+  d.high = p->high;
   int rc = CGLI_OK;
 #define F(x) if (rc == CGLI_OK) rc = field(c, &(x))
   for (int v = 0; v < 5; v++) {
@@ -425,7 +436,7 @@ int cgli_channel_metrics(cgli_ctx *c, double high, double stretch) {
   int rc = check(c); if (rc) return rc;
   if (!(high > 0 && stretch > 0)) return fail(CGLI_EINVAL, "high and stretch must be positive");
   cgli::MetricSet M;
-  cgli::channel_metrics(c->p.nx, c->p.ny, c->p.nz, c->p.det, high, stretch, M);
+  cgli::channel_metrics(c->p.nx, c->p.ny, c->p.nz, c->p.det, high, stretch, M, c->p.x_open != 0);
   return upload_metrics(c, M);
 }
 
@@ -653,6 +664,7 @@ int cgli_get_state(cgli_ctx *c, double *const U_[5]) {
 
 SIMPLE_ENTRY(cgli_halo_x, launch_halo_x, "halo_x")
 SIMPLE_ENTRY(cgli_y_boundary_condition, launch_bc_y, "y_boundary_condition")
+SIMPLE_ENTRY(cgli_x_boundary_condition, launch_bc_x, "x_boundary_condition")
 SIMPLE_ENTRY(cgli_z_boundary_condition, launch_bc_z, "z_boundary_condition")
 SIMPLE_ENTRY(cgli_flux_x, launch_flux_x, "flux_x")
 SIMPLE_ENTRY(cgli_flux_y, launch_flux_y, "flux_y")

@@ -23,6 +23,10 @@ struct Dev {
   long long di, dj;       // strides of i and j (k stride is 1)
   double dxi, det, dzt, dt, e, mu, pr, twl, twh;
   int curved_walls;       // wall-face pressure force with eta_x, eta_z terms
+  int x_open;             // open x ends (single rank 0 of 1), else a periodic slab
+  int nx_inlet, nx_outlet;  // sponge layers (open x only)
+  int buoyancy;           // f = -(rho - 1.1842) 9.81 instead of scal[0]
+  double high;            // channel height parameter (sponge strength)
   double *U_[5], *U[5], *Uq[5];
   double *Uqq[5];         // Q^(n-2)/J for the extrapolated initial guess
   double *J, *m[9];
@@ -32,7 +36,7 @@ struct Dev {
   double *MR[5], *NL[5], *NR[5];
   double *vflux[3][4];
   double *vprim[4];
-  double *scal;           // [0] = driving force
+  double *scal;           // [0] = driving force, [1] = outlet sponge target velocity
   double *partial;        // per-block partial sums of the update norms
   int *status;            // device status word (0 ok)
   // mixed-precision sweep state
@@ -306,6 +310,45 @@ __device__ __forceinline__ void upper_terms(const Split<T> &A, const T n[5], T o
   o[2] = +A.p31 * n[0] + A.m22 * n[2];
   o[3] = +A.p41 * n[0] + A.m22 * n[3];
   o[4] = +A.p51 * n[0] + A.p52 * n[1] + A.p53 * n[2] + A.p54 * n[3] + A.m22 * n[4];
+}
+
+// Sponge terms of Dual_time_stepping.cpp:554-664 at interior cell c (plane i)
+// of an open slab, the reference's Residual1..5: zero outside the inlet
+// layer (planes 3..nx_inlet+2) and the outlet layer (planes
+// max(3, Nx-nx_outlet+2)..Nx+2; the outlet wins where they overlap).  The
+// inlet profile uses the slab's first global index (:586), the outlet one the
+// plane's (:644); the outlet target velocity targetU is d.scal[1].
+__device__ __forceinline__ void sponge_terms(const Dev &d, int i, long long c, double out[5]) {
+#pragma unroll
+  for (int v = 0; v < 5; v++) out[v] = 0.0;
+  if (!d.x_open) return;
+  const int nxin = d.nx_inlet, nxout = d.nx_outlet;
+  const bool outlet = nxout > 0 && i >= max(3, d.nx - nxout + 2);
+  const bool inlet = !outlet && nxin > 0 && i <= nxin + 2;
+  if (!inlet && !outlet) return;
+  const double J = d.J[c], q1 = d.U_[0][c];
+  const double rho = q1 * J, u = d.U_[1][c] / q1, v = d.U_[2][c] / q1, w = d.U_[3][c] / q1;
+  const double VV = u * u + v * v + w * w;
+  const double P = (d.U_[4][c] * J - 0.5 * rho * VV) * (KG - 1);
+  const double C = KG * P / rho;
+  const double th = VV / C, beta = th > d.e ? th : d.e;
+  const double C_plan = 0.5 * sqrt(u * u * (beta - 1) * (beta - 1) + 4 * beta * C);
+  double Us, Sig, t2 = 0, t5 = 0;
+  if (inlet) {
+    Us = pow((nxin - 0.5) / nxin, 3.0) * C_plan;
+    Sig = 0.035 * Us / d.high;
+  } else {
+    Us = pow((i - 0.5 - ((d.nx + 1) - nxout)) / nxout, 3.0) * C_plan;
+    Sig = 1.25 * Us / d.high;
+    const double tU = d.scal[1];
+    t2 = 1.1842 * tU;
+    t5 = 0.5 * 1.1842 * tU * tU;
+  }
+  const long long b = c - d.di;
+  const double Jb = d.J[b], idx = 1 / d.dxi;
+  const double rhs[5] = {rho - 1.1842, rho * u - t2, rho * v, rho * w, d.U_[4][c] * J - 253250.0 - t5};
+#pragma unroll
+  for (int n = 0; n < 5; n++) out[n] = -Us * (d.U_[n][c] * J - d.U_[n][b] * Jb) * idx - Sig * rhs[n];
 }
 
 // Deterministic block reduction of five partial sums (warp shuffles, then

@@ -82,7 +82,12 @@ void launch_residual_fast(const Dev &d, const SweepArgs &a, cudaStream_t s, bool
 void launch_statistics(const Dev &d, cudaStream_t s, double *sums);
 // d.iJ = 1/J on every cell (0 where J = 0)
 void launch_inverse_j(const Dev &d, cudaStream_t s);
+// main.cpp:167-210: x halo (periodic slab only), Y, X (open slab only), Z
 void launch_halo_bc(const Dev &d, cudaStream_t s);
+// X_boundary_condition.cpp on an open slab (no-op on a periodic one)
+void launch_bc_x(const Dev &d, cudaStream_t s);
+// outlet sponge target velocity into d.scal[1] (open slab with an outlet layer)
+void launch_target_u(const Dev &d, cudaStream_t s);
 void launch_halo_x(const Dev &d, cudaStream_t s);
 void launch_bc_y(const Dev &d, cudaStream_t s);
 void launch_bc_z(const Dev &d, cudaStream_t s);

@@ -20,11 +20,16 @@ static inline void stretch(double high, double g, double det, int j, double off,
 }
 
 // Jacobian.cpp:61-243, Jacobian_u.cpp:59-101, Jacobian_v.cpp:79-151,
-// Jacobian_w.cpp:61-106 for an interior slab (planes 0..Nx+5).  Unset
-// entries stay zero.  The ghost-row copy statements of Jacobian.cpp:181-182,
-// :193-194 and :224-237 assign ztdx of the neighbour to ztdy and ztdz; they
-// are kept, so ghost rows carry ztdy = ztdz = 0.
-void channel_metrics(int nx, int ny, int nz, double det, double high, double g, MetricSet &M) {
+// Jacobian_w.cpp:61-106 for an interior slab (planes 0..Nx+5), or with
+// x_open for a slab that is the first and the last rank (cell metrics on
+// planes 3..Nx+2, then the end planes 2 and Nx+3 as copies of their
+// neighbours over j, k = 1..Ny+2 / Nz+2, Jacobian.cpp:110-157, whose ztdx is
+// copied three times so that ztdy, ztdz of the end planes stay zero; ghost
+// rows on planes 2..Nx+3).  Unset entries stay zero.  The ghost-row copy
+// statements of Jacobian.cpp:181-182, :193-194 and :224-237 assign ztdx of
+// the neighbour to ztdy and ztdz; they are kept, so ghost rows carry
+// ztdy = ztdz = 0.
+void channel_metrics(int nx, int ny, int nz, double det, double high, double g, MetricSet &M, bool x_open) {
   const int X = nx + 6, Y = ny + 4, Z = nz + 4;
   const size_t n = (size_t)X * Y * Z;
   auto id = [&](int i, int j, int k) { return ((size_t)i * Y + j) * Z + k; };
@@ -39,14 +44,25 @@ void channel_metrics(int nx, int ny, int nz, double det, double high, double g, 
     double etdy, ydet;
     stretch(high, g, det, j, 1.5, etdy, ydet);
     double J = 1. / (1 * ydet * 1);
-    for (int i = 0; i <= ie + 3; i++)
+    for (int i = x_open ? 3 : 0; i <= (x_open ? ie : ie + 3); i++)
       for (int k = 2; k <= kn; k++) {
         size_t c = id(i, j, k);
         M.m[0][c] = 1; M.m[4][c] = etdy; M.m[8][c] = 1;
         M.J[c] = J;
       }
   }
-  for (int i = 0; i <= ie + 3; i++)
+  if (x_open)
+    for (int side = 0; side < 2; side++) {
+      const int ig = side ? ie + 1 : 2, is = side ? ie : 3;
+      for (int j = 1; j <= nyy; j++)
+        for (int k = 1; k <= nzz; k++) {
+          size_t gidx = id(ig, j, k), c = id(is, j, k);
+          for (int v = 0; v < 7; v++) M.m[v][gidx] = M.m[v][c];
+          M.J[gidx] = M.J[c];
+        }
+    }
+  const int ig0 = x_open ? 2 : 0, ig1 = x_open ? ie + 1 : ie + 3;
+  for (int i = ig0; i <= ig1; i++)
     for (int k = 2; k <= kn; k++)
       for (int side = 0; side < 2; side++) {
         size_t gidx = id(i, side ? nyy : 1, k), c = id(i, side ? jn : 2, k);
@@ -55,7 +71,7 @@ void channel_metrics(int nx, int ny, int nz, double det, double high, double g, 
         M.m[8][gidx] = M.m[6][c];
         M.J[gidx] = M.J[c];
       }
-  for (int i = 0; i <= ie + 3; i++)
+  for (int i = ig0; i <= ig1; i++)
     for (int j = 1; j <= nyy; j++)
       for (int side = 0; side < 2; side++) {
         size_t gidx = id(i, j, side ? nzz : 1), c = id(i, j, side ? kn : 2);

@@ -119,8 +119,10 @@ __global__ void __launch_bounds__((TJ + 2) * 32, TJ <= 6 ? 2 : 1) k_dplur_relax(
         for (int v = 0; v < 9; v++) mm[v] = s[(16 + v) * NT];
       }
       double n[5];
+      // an open slab's end planes hold zero iterates (DPLUSGS.cpp:191-233)
+      const bool zero_end = d.x_open && (p == 2 || p == ie + 1);
 #pragma unroll
-      for (int v = 0; v < 5; v++) n[v] = s[(5 + v) * NT];
+      for (int v = 0; v < 5; v++) n[v] = zero_end ? 0.0 : s[(5 + v) * NT];
       if (row) {
         // the cell's three split Jacobians and its diagonal, each repeated
         // divisor as one reciprocal

@@ -61,14 +61,15 @@ __global__ void k_residual_fast(Dev d, SweepArgs a) {
   double d55 = (KG - 1) * (1 + (KG - 1) * beta) * itemp;
   long long fx1 = ix(d, i, j - 1, k - 1), fx0 = ix(d, i - 1, j - 1, k - 1);
   long long fy1 = ix(d, i - 1, j, k - 1), fz1 = ix(d, i - 1, j - 1, k);
-  double Rk[5];
-  double f = d.scal[0];
+  double Rk[5], sp[5];
+  sponge_terms(d, i, c, sp);
+  double f = d.buoyancy ? -(rho - 1.1842) * 9.81 : d.scal[0];
   const double i2dt = 1 / (2 * deltaT), idx = 1 / d.dxi, idy = 1 / d.det, idz = 1 / d.dzt, iJ = 1 / J;
   for (int n = 0; n < 5; n++) {
     double Rp = -(3 * d.U_[n][c] - 4 * d.U[n][c] + d.Uq[n][c]) * i2dt;
     double Rf = -((d.inF[0][n][fx1] - d.inF[0][n][fx0]) * idx + (d.inF[1][n][fy1] - d.inF[1][n][fx0]) * idy +
                   (d.inF[2][n][fz1] - d.inF[2][n][fx0]) * idz);
-    Rk[n] = Rp + Rf;
+    Rk[n] = sp[n] * iJ + Rp + Rf;
   }
   Rk[1] = Rk[1] + d.vF[0][c] + f * iJ;
   Rk[2] = Rk[2] + d.vF[1][c];
@@ -84,7 +85,8 @@ __global__ void k_residual_fast(Dev d, SweepArgs a) {
     if (MIXED) a.mrf[n][slot] = (float)MR[n];
     else a.mrs[n][slot] = MR[n];
   }
-  if (i == ie || i == 3) {
+  // the lagged halos of the first sweep; an open slab's stay zero
+  if (!d.x_open && (i == ie || i == 3)) {
     double mm[9];
     for (int v2 = 0; v2 < 9; v2++) mm[v2] = d.m[v2][c];
     Diag<double> dd = diag<double>(q, mm, d.dxi, d.det, d.dzt, deltaT);
@@ -114,6 +116,7 @@ void launch_fused_iteration(const Dev &d, const SweepArgs &a, cudaStream_t s, in
   launch_flux_y(d, s);
   launch_flux_z(d, s);
   launch_viscous(d, s);
+  launch_target_u(d, s);
   const bool mixed = precision == 1;
   launch_residual_fast(d, a, s, mixed);
   launch_sweeps(d, a, s, mixed);

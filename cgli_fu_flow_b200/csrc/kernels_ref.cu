@@ -23,7 +23,10 @@ __global__ void k_halo_x(Dev d) {
   q[t] = q[(long long)(ie - 2) * plane + t];
 }
 
-// Y_boundary_condition.cpp:94-182 for interior planes i = 3..ie
+// Y_boundary_condition.cpp:94-182 for interior planes i = 3..ie: the
+// zero-gradient copy of :100-112, replaced inside the heated section
+// (planes nx_inlet+3 .. Nx-nx_outlet+2, :114) by the isothermal no-slip
+// reflection
 __global__ void k_bc_y(Dev d) {
   int k = 2 + blockIdx.x * blockDim.x + threadIdx.x;
   int i = 3 + blockIdx.y;
@@ -32,6 +35,10 @@ __global__ void k_bc_y(Dev d) {
   if (k > kn) return;
   int js = side ? jn : 2, jg = side ? jn + 1 : 1;
   long long c = ix(d, i, js, k), g = ix(d, i, jg, k);
+  if (!(i > d.nx_inlet + 2 && i < d.nx - d.nx_outlet + 3)) {
+    for (int v = 0; v < 5; v++) d.U_[v][g] = d.U_[v][c];
+    return;
+  }
   double q1 = d.U_[0][c], q2 = d.U_[1][c], q3 = d.U_[2][c], q4 = d.U_[3][c], q5 = d.U_[4][c];
   double Jc = d.J[c], Jg = d.J[g];
   double rho = q1 * Jc;
@@ -47,17 +54,124 @@ __global__ void k_bc_y(Dev d) {
   d.U_[4][g] = (P / (KG - 1) + 0.5 * rho * VV) / Jg;
 }
 
-// Z_boundary_condition.cpp:39-66: all planes 0..ie+3, all rows 0..nyyy
+// Z_boundary_condition.cpp:39-66: all rows 0..nyyy of planes 0..ie+3
+// (planes 2..ie+1 on an open slab, :40-44)
 __global__ void k_bc_z(Dev d) {
   long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   long long n = (long long)d.X * d.Y;
   if (t >= n) return;
+  if (d.x_open) {
+    const int i = (int)(t / d.Y);
+    if (i < 2 || i > d.nx + 3) return;
+  }
   int v = blockIdx.y;
   long long row = t * d.dj;
   int kn = d.nz + 1;
   double *q = d.U_[v];
   q[row + 1] = q[row + kn];
   q[row + kn + 1] = q[row + 2];
+}
+
+// X_boundary_condition.cpp:73-338 on an open slab: one pseudo-time step of
+// dtau = dt/200 on the ghost cell of each interior row, with
+// M (Gamma + 3 dtau/(2 dt) M)^-1 applied to the characteristic amplitudes
+// (the outgoing ones from one-sided x differences against the interior
+// neighbour, the incoming ones zero) plus the BDF2 time derivative.
+// blockIdx.z: 0 inlet (plane 2 against 3), 1 outlet (plane ie+1 against ie).
+__global__ void k_bc_x(Dev d) {
+  const int k = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 2 + blockIdx.y;
+  const int side = blockIdx.z;
+  if (k > d.nz + 1) return;
+  const int ie = d.nx + 2;
+  const long long c = ix(d, side ? ie : 3, j, k), g = ix(d, side ? ie + 1 : 2, j, k);
+  const double K = KG, deltaT = d.dt, deltaTau = deltaT / 200., rdx = 1 / d.dxi;
+  double q[5], qi[5];
+#pragma unroll
+  for (int v = 0; v < 5; v++) { q[v] = d.U_[v][g]; qi[v] = d.U_[v][c]; }
+  // interior neighbour
+  const double Jc = d.J[c], iq1 = 1 / qi[0];
+  const double rho_ = qi[0] * Jc, U_ = qi[1] * iq1, V_ = qi[2] * iq1, W_ = qi[3] * iq1;
+  const double P_ = (qi[4] * Jc - 0.5 * rho_ * (U_ * U_ + V_ * V_ + W_ * W_)) * (K - 1);
+  const double T_ = P_ / rho_;
+  // ghost cell
+  const double Jg = d.J[g], ig1 = 1 / q[0];
+  const double rho = q[0] * Jg, U = q[1] * ig1, V = q[2] * ig1, W = q[3] * ig1;
+  const double VV = U * U + V * V + W * W;
+  const double P = (q[4] * Jg - 0.5 * rho * VV) * (K - 1);
+  const double C2 = K * P / rho, C = sqrt(C2);
+  const double T = P / rho;
+  const double H = 0.5 * VV + C * C / (K - 1);
+  const double th = VV / C / C, beta = th > d.e ? th : d.e;
+  // M (Gamma + 3 dtau/(2 dt) M)^-1, :98-147
+  const double itemp = 1 / (K * T * (2 * deltaT + 3 * deltaTau) * (2 * deltaT + 3 * beta * deltaTau));
+  const double temp2 = (K - 1) * (beta - 1) * deltaT * deltaT;
+  const double temp3 = H - H * K - VV + K * (T + VV);
+  const double a4 = -4 * temp2 * itemp, t3 = 4 * temp3 * (beta - 1) * deltaT * deltaT * itemp;
+  const double vel[3] = {U, V, W};
+  double dm[5][5];
+  dm[0][0] = (2 * deltaT * (-2 * (-(K - 1) * (H - VV) - temp3 * beta) * deltaT + 3 * K * T * beta * deltaTau)) * itemp;
+  dm[0][4] = -a4;
+  dm[4][0] = H * t3;
+  dm[4][4] = (2 * deltaT * (2 * H * (K - 1) * (beta - 1) * deltaT + K * T * (2 * deltaT + 3 * beta * deltaTau))) * itemp;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    dm[0][1 + a] = vel[a] * a4;
+    dm[1 + a][0] = vel[a] * t3;
+    dm[1 + a][4] = -vel[a] * a4;
+    dm[4][1 + a] = H * vel[a] * a4;
+#pragma unroll
+    for (int b = 0; b < 3; b++)
+      dm[1 + a][1 + b] = a == b ? (2 * deltaT * (2 * K * (T - vel[a] * vel[a] * (beta - 1)) * deltaT +
+                                                 2 * vel[a] * vel[a] * (beta - 1) * deltaT + 3 * K * T * beta * deltaTau)) * itemp
+                                : vel[a] * vel[b] * a4;
+  }
+  const double U_p = 0.5 * (beta + 1) * U;
+  const double C_p = 0.5 * sqrt(U * U * (beta - 1) * (beta - 1) + 4 * beta * C * C);
+  double L1 = 0, L2 = 0, L3 = 0, L4, L5;
+  if (!side) {
+    // inlet, :151-187: L5 from the interior, L4 from it, L1..L3 only for backflow
+    const double dp = (P_ - P) * rdx, du = (U_ - U) * rdx, dv = (V_ - V) * rdx, dw = (W_ - W) * rdx, dT = (T_ - T) * rdx;
+    L5 = (U_p - C_p) * (dp - rho * (U_p + C_p - U) * du);
+    L4 = L5 * (U_p - C_p - U) / (U_p + C_p - U);
+    if (U <= 0) { L1 = U * (dT + 1.0 / rho * dp * (1 - K) / K); L2 = U * dw; L3 = -U * dv; }
+  } else {
+    // outlet, :292-327
+    const double dp = (P - P_) * rdx, du = (U - U_) * rdx, dv = (V - V_) * rdx, dw = (W - W_) * rdx, dT = (T - T_) * rdx;
+    L4 = (U_p + C_p) * (dp - rho * (U_p - C_p - U) * du);
+    L5 = L4 * (U_p + C_p - U) / (U_p - C_p - U);
+    if (U > 0) { L1 = U * (dT + 1.0 / rho * dp * (1 - K) / K); L2 = U * dw; L3 = -U * dv; }
+  }
+  double KAL[5];
+  KAL[0] = 0.5 / C_p * (L4 * (U_p + C_p - U) - L5 * (U_p - C_p - U));
+  KAL[1] = 0.5 / (rho * C_p) * (L4 - L5);
+  KAL[2] = -L3;
+  KAL[3] = L2;
+  KAL[4] = L1 + 1. / rho * (K - 1) / K * KAL[0];
+  const double iJg = 1 / Jg, i2dt = 1 / (2 * deltaT);
+#pragma unroll
+  for (int v = 0; v < 5; v++) KAL[v] = KAL[v] * iJg + (3 * q[v] - 4 * d.U[v][g] + d.Uq[v][g]) * i2dt;
+#pragma unroll
+  for (int v = 0; v < 5; v++)
+    d.U_[v][g] = q[v] - deltaTau * (dm[v][0] * KAL[0] + dm[v][1] * KAL[1] + dm[v][2] * KAL[2] + dm[v][3] * KAL[3] +
+                                    dm[v][4] * KAL[4]);
+}
+
+// outlet sponge target velocity, Dual_time_stepping.cpp:510-532: the sum
+// over plane 3, rows j = 2..Ny+2, k = 2..Nz+2, of u deltaET / etdy deltaZT,
+// over high deltaZT Nz; one block, into d.scal[1]
+__global__ void k_target_u(Dev d) {
+  const int nj = d.ny + 1, nk = d.nz + 1;
+  double acc[5] = {0, 0, 0, 0, 0};
+  for (int t = threadIdx.x; t < nj * nk; t += blockDim.x) {
+    const int j = 2 + t / nk, k = 2 + t % nk;
+    const long long c = ix(d, 3, j, k);
+    acc[0] += d.U_[1][c] / d.U_[0][c] * d.det / d.m[4][c] * d.dzt;
+  }
+  __shared__ double tot[5];
+  block_sum5(acc, tot);
+  __syncthreads();
+  if (threadIdx.x == 0) d.scal[1] = tot[0] * (1. / (d.high * d.dzt * d.nz));
 }
 
 // ---------------------------------------------------------------- fluxes
@@ -71,8 +185,20 @@ __global__ void k_flux_x(Dev d) {
   // left state ML[i] from cells i-2..i+2, right state MR[i] from i-1..i+3
   long long c = ix(d, i, j + 1, k + 1);
   double L[5], R[5], F[5], fav3, pp;
-  side5L(d, c - 2 * d.di, d.di, L);
-  side5R(d, c - d.di, d.di, R);
+  const int ie = d.nx + 2;
+  const long long di = d.di;
+  if (d.x_open && (i <= 3 || i >= ie - 1)) {
+    // the first and last rank's reduced stencils, Flux_X.cpp:139-216
+    if (i == 2) side2(d, c, c + di, L);
+    else if (i == 3 || i == ie) side3L(d, c - di, di, L);
+    else side5L(d, c - 2 * di, di, L);
+    if (i == 2 || i == ie - 1) side3R(d, c, di, R);
+    else if (i == ie) side2(d, c, c + di, R);
+    else side5R(d, c - di, di, R);
+  } else {
+    side5L(d, c - 2 * di, di, L);
+    side5R(d, c - di, di, R);
+  }
   roe_face(L, R, d.mf[0][0][f], d.mf[0][1][f], d.mf[0][2][f], d.Jf[0][f], d.e, F, fav3, pp);
   for (int v = 0; v < 5; v++) d.inF[0][v][f] = F[v];
 }
@@ -247,13 +373,14 @@ __global__ void k_dts_residual(Dev d) {
   double d55 = (KG - 1) * (1 + (KG - 1) * beta) / temp;
   long long fx1 = ix(d, i, j - 1, k - 1), fx0 = ix(d, i - 1, j - 1, k - 1);
   long long fy1 = ix(d, i - 1, j, k - 1), fz1 = ix(d, i - 1, j - 1, k);
-  double Rk[5];
-  double f = d.scal[0];
+  double Rk[5], sp[5];
+  sponge_terms(d, i, c, sp);
+  double f = d.buoyancy ? -(rho - 1.1842) * 9.81 : d.scal[0];
   for (int n = 0; n < 5; n++) {
     double Rp = -(3 * d.U_[n][c] - 4 * d.U[n][c] + d.Uq[n][c]) / (2 * deltaT);
     double Rf = -((d.inF[0][n][fx1] - d.inF[0][n][fx0]) / d.dxi + (d.inF[1][n][fy1] - d.inF[1][n][fx0]) / d.det +
                   (d.inF[2][n][fz1] - d.inF[2][n][fx0]) / d.dzt);
-    Rk[n] = Rp + Rf;
+    Rk[n] = sp[n] / J + Rp + Rf;
   }
   Rk[1] = Rk[1] + d.vF[0][c] + f / J;
   Rk[2] = Rk[2] + d.vF[1][c];
@@ -276,14 +403,15 @@ __global__ void k_dts_residual(Dev d) {
 
 // ------------------------------------------------------------- sweeps
 // lagged periodic halo planes of the sweep, Dual_time_stepping.cpp:942-976:
-// NL[2] <- NL[ie], NR[ie+1] <- NR[3]
+// NL[2] <- NL[ie], NR[ie+1] <- NR[3]; zero on an open slab (:204-246, and
+// the exchange with absent neighbours leaves them so)
 __global__ void k_sweep_halo(Dev d) {
   long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= d.di) return;
   int v = blockIdx.y;
   int ie = d.nx + 2;
-  d.NL[v][2 * d.di + t] = d.NL[v][(long long)ie * d.di + t];
-  d.NR[v][(long long)(ie + 1) * d.di + t] = d.NR[v][3 * d.di + t];
+  d.NL[v][2 * d.di + t] = d.x_open ? 0.0 : d.NL[v][(long long)ie * d.di + t];
+  d.NR[v][(long long)(ie + 1) * d.di + t] = d.x_open ? 0.0 : d.NR[v][3 * d.di + t];
 }
 
 __device__ __forceinline__ CPrim<double> cp_at(const Dev &d, long long c) {
@@ -401,16 +529,26 @@ __global__ void k_update(Dev d) {
 // ------------------------------------------------------------ launchers
 static dim3 cellgrid(int nk, int nj, int ni, int bx) { return dim3((nk + bx - 1) / bx, nj, ni); }
 
+// main.cpp:167-210: halo exchange, then Y, X, Z boundaries
 void launch_halo_bc(const Dev &d, cudaStream_t s) {
-  long long n = 3 * d.di;
-  k_halo_x<<<dim3((unsigned)((n + 255) / 256), 5), 256, 0, s>>>(d);
+  launch_halo_x(d, s);
   k_bc_y<<<dim3((d.nz + 127) / 128, d.nx, 2), 128, 0, s>>>(d);
+  launch_bc_x(d, s);
   long long rows = (long long)d.X * d.Y;
   k_bc_z<<<dim3((unsigned)((rows + 255) / 256), 5), 256, 0, s>>>(d);
 }
 void launch_halo_x(const Dev &d, cudaStream_t s) {
+  if (d.x_open) return;   // both neighbours absent
   long long n = 3 * d.di;
   k_halo_x<<<dim3((unsigned)((n + 255) / 256), 5), 256, 0, s>>>(d);
+}
+void launch_bc_x(const Dev &d, cudaStream_t s) {
+  if (!d.x_open) return;   // interior rank: no-op
+  k_bc_x<<<dim3((d.nz + 63) / 64, d.ny, 2), 64, 0, s>>>(d);
+}
+void launch_target_u(const Dev &d, cudaStream_t s) {
+  if (!d.x_open || d.nx_outlet == 0) return;
+  k_target_u<<<1, 256, 0, s>>>(d);
 }
 void launch_bc_y(const Dev &d, cudaStream_t s) {
   k_bc_y<<<dim3((d.nz + 127) / 128, d.nx, 2), 128, 0, s>>>(d);
@@ -438,6 +576,7 @@ void launch_dts_residual(const Dev &d, cudaStream_t s) {
 }
 
 void launch_dts(const Dev &d, cudaStream_t s, int update_blocks_x) {
+  launch_target_u(d, s);
   k_dts_residual<<<cellgrid(d.nz, d.ny, d.nx, 64), 64, 0, s>>>(d);
   int ie = d.nx + 2, jn = d.ny + 1, kn = d.nz + 1;
   for (int sweep = 1; sweep <= 2; sweep++) {

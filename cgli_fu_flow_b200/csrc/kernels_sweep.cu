@@ -362,9 +362,9 @@ __global__ void __launch_bounds__(TI *TJ) k_sweep(Dev d, SweepArgs a) {
       } else {
 #pragma unroll
         for (int v = 0; v < 5; v++) dq[v][cur.slot] = n[v];
-        if (BACKWARD) {
+        if (BACKWARD && !d.x_open) {
           // lagged halos of the next sweep: plane ie feeds its forward pass,
-          // plane 3 its backward pass
+          // plane 3 its backward pass (an open slab's halos stay zero)
           const long long h = (long long)j * d.dj + 2 + kl;
           if (i == ie)
             for (int v = 0; v < 5; v++) SweepPtrs<T>::hf(a)[v][h] = n[v];

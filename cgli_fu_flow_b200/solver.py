@@ -36,7 +36,9 @@ class Params(ctypes.Structure):
                 ("dt", ctypes.c_double), ("e", ctypes.c_double),
                 ("mu", ctypes.c_double), ("pr", ctypes.c_double),
                 ("twall_lo", ctypes.c_double), ("twall_hi", ctypes.c_double),
-                ("force", ctypes.c_double), ("precision", ctypes.c_int), ("curved_walls", ctypes.c_int)]
+                ("force", ctypes.c_double), ("precision", ctypes.c_int), ("curved_walls", ctypes.c_int),
+                ("x_open", ctypes.c_int), ("nx_inlet", ctypes.c_int), ("nx_outlet", ctypes.c_int),
+                ("buoyancy", ctypes.c_int), ("high", ctypes.c_double)]
 
 
 EXPORTS = [
@@ -54,7 +56,7 @@ EXPORTS = [
     "cgli_copy_state", "cgli_cnn_time_inference", "cgli_wavy_channel_metrics", "cgli_wavy_channel_metrics_host",
     "cgli_statistics_accumulate", "cgli_statistics_get", "cgli_statistics_reset",
     "cgli_write_restart", "cgli_read_restart", "cgli_write_history", "cgli_read_history",
-    "cgli_dplusgs", "cgli_set_inner_solver",
+    "cgli_dplusgs", "cgli_set_inner_solver", "cgli_x_boundary_condition",
 ]
 
 INNER_SOLVERS = {"lusgs": 0, "dplur": 1}
@@ -146,7 +148,9 @@ def reference_state(ch: C.Channel, J: np.ndarray, q_n: np.ndarray, q_nm1: np.nda
     interior planes filled with the quiescent state over all rows (divided by
     the cell's J, which is zero -- hence inf/nan -- on the outermost ring,
     exactly as in the reference with value-initialised arrays), interior
-    cells from the restart data divided by J, x ghost planes zero."""
+    cells from the restart data divided by J, x ghost planes zero.  An open
+    slab (the first and the last rank) also gets the quiescent state on its
+    end planes 2 and Nx+3 (Initial_condition.cpp:57-61)."""
     X, Y, Z = ch.shape
     nx, ny, nz = ch.nx, ch.ny, ch.nz
     U = np.zeros((5, X, Y, Z))
@@ -155,12 +159,12 @@ def reference_state(ch: C.Channel, J: np.ndarray, q_n: np.ndarray, q_nm1: np.nda
     P = 101300.0
     rho = P / T / C.R_GAS
     quiet = [rho, rho * 0.0, rho * 0.0, rho * 0.0, P / (C.GAMMA - 1) + 0.5 * rho * 0.0]
-    Js = J[3:nx + 3]
+    lo, hi = (2, nx + 4) if ch.x_open else (3, nx + 3)
     with np.errstate(divide="ignore", invalid="ignore"):
         for v in range(5):
-            U[v, 3:nx + 3] = quiet[v] / Js
-            Uq[v, 3:nx + 3] = quiet[v] / Js
-            Jint = Js[:, 2:ny + 2, 2:nz + 2]
+            U[v, lo:hi] = quiet[v] / J[lo:hi]
+            Uq[v, lo:hi] = quiet[v] / J[lo:hi]
+            Jint = J[3:nx + 3, 2:ny + 2, 2:nz + 2]
             U[v, 3:nx + 3, 2:ny + 2, 2:nz + 2] = q_n[v] / Jint
             Uq[v, 3:nx + 3, 2:ny + 2, 2:nz + 2] = q_nm1[v] / Jint
     U_ = U.copy()
@@ -176,8 +180,8 @@ class Solver:
         self.shape = ch.shape
         self.n = int(np.prod(self.shape))
         p = Params(ch.nx, ch.ny, ch.nz, ch.dxi, ch.det, ch.dzt, ch.dt,
-                   C.PRECOND_EPS if e is None else e, C.MU0, C.PR, C.T0, C.T0, ch.force_lam, precision,
-                   int(ch.wavy))
+                   C.PRECOND_EPS if e is None else e, C.MU0, C.PR, ch.twall_lo, ch.twall_hi, ch.force_lam, precision,
+                   int(ch.wavy), int(ch.x_open), ch.nx_inlet, ch.nx_outlet, int(ch.buoyancy), ch.high)
         h = ctypes.c_void_p()
         self._rc(self.L.cgli_create(ctypes.byref(p), ctypes.byref(h)))
         self.h = h
@@ -244,6 +248,10 @@ class Solver:
 
     def y_boundary_condition(self):
         self._rc(self.L.cgli_y_boundary_condition(self.h))
+
+    def x_boundary_condition(self):
+        """X_boundary_condition.cpp (open slab; a no-op on a periodic one)."""
+        self._rc(self.L.cgli_x_boundary_condition(self.h))
 
     def z_boundary_condition(self):
         self._rc(self.L.cgli_z_boundary_condition(self.h))

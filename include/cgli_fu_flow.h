@@ -52,6 +52,21 @@ typedef struct cgli_params {
                             * 1: plus the x and z components of the wall pressure
                             * force, 0.5 (eta_x, eta_z) (p_L + p_R) / J_v, which
                             * flat walls do not have (identical for flat walls) */
+  int x_open;              /* 0: one slab of the x-periodic channel (the workloads);
+                            * 1: the reference's open configuration run as a single
+                            * rank 0 of 1: characteristic inflow / outflow ghost planes
+                            * (cgli_x_boundary_condition), one-sided MUSCL at the x ends
+                            * (Flux_X.cpp:139-216), no x halo, zero implicit halos
+                            * (Dual_time_stepping.cpp:204-246), end-plane metrics of
+                            * Jacobian.cpp:110-157 from cgli_channel_metrics */
+  int nx_inlet, nx_outlet; /* sponge layers of Resolution.h:5-6 (x_open only; the
+                            * residual of Dual_time_stepping.cpp:554-664); the walls are
+                            * isothermal only between them (Y_boundary_condition.cpp:114) */
+  int buoyancy;            /* 1: body force f = -(rho - 1.1842) 9.81 per cell
+                            * (Dual_time_stepping.cpp:831) instead of `force` (the DP-LUR
+                            * solver keeps `force` and has no sponge, as DPLUSGS.cpp) */
+  double high;             /* channel height of prm.h:16 (sponge strength
+                            * Sigma = Sigma_0 U / high); needed with sponge layers */
 } cgli_params;
 
 typedef struct cgli_ctx cgli_ctx;
@@ -135,6 +150,11 @@ int cgli_z_boundary_condition(cgli_ctx *ctx);
 int cgli_flux_x(cgli_ctx *ctx);
 int cgli_flux_y(cgli_ctx *ctx);
 int cgli_flux_z(cgli_ctx *ctx);
+/* X_boundary_condition.cpp:73-338 (x_open): one pseudo-time step of the
+ * characteristic inflow / outflow relations on ghost planes 2 and Nx+3;
+ * no-op for the periodic slab, like the reference's interior ranks.
+ * cgli_halo_x is a no-op on an open slab (both neighbours absent). */
+int cgli_x_boundary_condition(cgli_ctx *ctx);
 /* Viscous_terms.cpp:15-907: fill vF2..vF5 */
 int cgli_viscous_terms(cgli_ctx *ctx);
 /* Dual_time_stepping.cpp:18-1795: residual, 2 x (forward + backward)

@@ -108,3 +108,145 @@ def test_open_oracle_matches_reference_second_grid(solver):
         _, er_o = o.step(4)
         assert np.array_equal(r.q()[_sl(ch)], o.q()[_sl(ch)])
         np.testing.assert_allclose(er_r, er_o, rtol=1e-14)
+
+
+# ------------------------------------------------------------------ GPU
+# Tolerances as for the periodic channel: one routine ~1e-13 of the array's
+# scale (fused multiply-adds and reciprocals), whole steps by relative L2.
+
+STAGE_TOL = 1e-12
+STEP_TOL = 1e-10
+
+
+def _rel_max(a, b):
+    m = np.isfinite(a) & np.isfinite(b)
+    return np.abs(a[m] - b[m]).max() / max(np.abs(b[m]).max(), 1e-300)
+
+
+def _rel_l2(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def _pair(ch, precision=0, solver="lusgs"):
+    from cgli_fu_flow_b200 import build
+    from cgli_fu_flow_b200.solver import Solver
+    from oracle.oracle import Oracle
+    build.build()
+    g = Solver(ch, precision)
+    g.init()
+    o = Oracle(ch, inner_solver=solver)
+    o.init()
+    return g, o
+
+
+@pytest.mark.gpu
+def test_open_metrics_and_initial_state_match_oracle():
+    ch = _open_channel()
+    g, o = _pair(ch)
+    for n in ("J", "xidx", "etdy", "ztdx", "ztdy", "ztdz", "J_u", "etdy_v", "J_v", "J_w"):
+        assert np.array_equal(g.get(n), o.array(n)), n
+    for n in ("U1_", "U2_", "U5_", "U1", "U1q"):
+        a, b = g.get(n), o.array(n)
+        assert np.array_equal(np.isfinite(a), np.isfinite(b)), n
+        assert np.array_equal(a[np.isfinite(a)], b[np.isfinite(b)]), n
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dims", [(16, 12, 8), (37, 20, 34)])
+def test_open_routines_match_oracle(dims):
+    """Each entry point of the open configuration after two steps (a
+    developed state), then one routine-by-routine inner iteration."""
+    ch = _open_channel(*dims, nx_inlet=4, nx_outlet=6)
+    g, o = _pair(ch)
+    for _ in range(2):
+        g.step(4)
+        o.step(4)
+    X = (slice(2, ch.nx + 4), slice(2, ch.ny + 2), slice(2, ch.nz + 2))
+    for v in range(1, 6):
+        assert _rel_l2(g.get(f"U{v}_")[X], o.array(f"U{v}_")[X]) <= 1e-11, v
+    g.set_state(*[np.stack([o.array(f"U{v}{s}") for v in range(1, 6)]) for s in ("_", "", "q")])
+    g.halo_x(); g.y_boundary_condition(); g.x_boundary_condition(); g.z_boundary_condition()
+    for n in ("halo_x", "bc_y", "bc_x", "bc_z"):
+        o.call(n)
+    ring = (slice(2, ch.nx + 4), slice(1, ch.ny + 3), slice(1, ch.nz + 3))
+    for v in range(1, 6):
+        assert _rel_max(g.get(f"U{v}_")[ring], o.array(f"U{v}_")[ring]) <= STAGE_TOL, ("bc", v)
+    g.flux_x(); o.call("flux_x")
+    fx = (slice(2, ch.nx + 3), slice(1, ch.ny + 1), slice(1, ch.nz + 1))
+    for v in range(1, 6):
+        assert _rel_max(g.get(f"inFx{v}")[fx], o.array(f"inFx{v}")[fx]) <= STAGE_TOL, ("fx", v)
+    g.flux_y(); g.flux_z(); g.viscous_terms()
+    for n in ("flux_y", "flux_z", "viscous"):
+        o.call(n)
+    cell = (slice(3, ch.nx + 3), slice(2, ch.ny + 2), slice(2, ch.nz + 2))
+    for v in range(2, 6):
+        assert _rel_max(g.get(f"vF{v}")[cell], o.array(f"vF{v}")[cell]) <= STAGE_TOL, ("vF", v)
+    er_g = g.dual_time_stepping()
+    o.call("dts_residual"); o.call("sweeps")
+    er_o = o.update()
+    # the sponge's energy term E J - 253250 (Dual_time_stepping.cpp:596, :655)
+    # cancels about four digits, so MR carries ten times the stage bar
+    for v in range(1, 6):
+        assert _rel_max(g.get(f"MR{v}")[cell], o.array(f"MR{v}")[cell]) <= 10 * STAGE_TOL, ("MR", v)
+        assert _rel_max(g.get(f"U{v}_")[cell], o.array(f"U{v}_")[cell]) <= STAGE_TOL, ("U_", v)
+    np.testing.assert_allclose(er_g, er_o, rtol=1e-9)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("solver", ["lusgs", "dplur"])
+def test_open_steps_match_reference_fixture(solver):
+    """Three steps of ten inner iterations through cgli_step (the fused path
+    for LU-SGS) against the reference run as rank 0 of 1."""
+    f = _fixture()
+    ch = _open_channel(*f["cells"])
+    g, _ = _pair(ch)
+    g.set_inner_solver(solver)
+    for _ in range(f["steps"]):
+        g.step(f["iters_per_step"])
+    ref = np.load(os.path.join(GOLDEN, "open_16x12x8.npz"))[solver]
+    q = g.q()[_sl(ch)]
+    for v in range(5):
+        assert _rel_l2(q[v], ref[v]) <= STEP_TOL, v
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("solver", ["lusgs", "dplur"])
+def test_open_ten_steps_match_oracle(solver):
+    """A grid with several sweep tiles and relaxation tiles, unequal sponges,
+    buoyancy, the stopping rule deciding the iteration counts on both
+    sides."""
+    ch = _open_channel(40, 24, 36, nx_inlet=5, nx_outlet=7)
+    g, o = _pair(ch, solver=solver)
+    g.set_inner_solver(solver)
+    for s in range(10):
+        it_g, _ = g.step(None, drop=1e-2, cap=10)
+        it_o, _ = o.step(None, drop=1e-2, cap=10)
+        assert it_g == it_o, s
+    q, r = g.q()[_sl(ch)], o.q()[_sl(ch)]
+    for v in range(5):
+        assert _rel_l2(q[v], r[v]) <= STEP_TOL, v
+
+
+@pytest.mark.gpu
+def test_open_mixed_precision_within_1e6():
+    from cgli_fu_flow_b200.solver import MIXED
+    ch = _open_channel(32, 16, 32)
+    g, o = _pair(ch, precision=MIXED)
+    for _ in range(10):
+        g.step(8)
+        o.step(8)
+    q, r = g.q()[_sl(ch)], o.q()[_sl(ch)]
+    errs = [_rel_l2(q[v], r[v]) for v in range(5)]
+    print("open, mixed precision, relative L2 per variable after 10 steps:", errs)
+    assert max(errs) <= 1e-6
+
+
+@pytest.mark.gpu
+def test_open_parameter_errors():
+    from cgli_fu_flow_b200 import build
+    from cgli_fu_flow_b200.solver import CgliError, Solver
+    build.build()
+    with pytest.raises(CgliError):
+        Solver(Channel(16, 12, 8, nx_inlet=2))                  # sponge on a periodic slab
+    with pytest.raises(CgliError):
+        Solver(_open_channel(16, 12, 8, nx_inlet=10, nx_outlet=8))   # layers longer than the slab
