@@ -157,6 +157,16 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def workload_label(ch) -> str:
+    if ch.x_open:
+        return (f"open channel {ch.nx}x{ch.ny}x{ch.nz} cells (the reference's own configuration: inflow / outflow, "
+                f"sponges of {ch.nx_inlet} and {ch.nx_outlet} cells, lower wall {ch.twall_lo} K between them, "
+                f"{'buoyancy' if ch.buoyancy else 'uniform force'}), Mach 0.2, Re_b 5600")
+    if ch.wavy:
+        return f"wavy-wall channel {ch.nx}x{ch.ny}x{ch.nz} cells (amplitude {ch.wave} h), Mach 0.2, Re_b 5600"
+    return f"channel {ch.nx}x{ch.ny}x{ch.nz} cells, Mach 0.2, Re_b 5600"
+
+
 # ------------------------------------------------------------ GPU arm
 def run_gpu(a, dist: Dist) -> dict | None:
     from cgli_fu_flow_b200.solver import Solver, FP64, MIXED
@@ -210,7 +220,7 @@ def run_gpu(a, dist: Dist) -> dict | None:
         "vs_baseline": None,
         "dtype": "f64" if a.precision == "fp64" else "f64 residual / f32 sweeps",
         "data": "synthetic: seeded Poiseuille + 10% uniform perturbation channel (no dataset involved)",
-        "config": {"workload": f"channel {ch.nx}x{ch.ny}x{ch.nz} cells, Mach 0.2, Re_b 5600",
+        "config": {"workload": workload_label(ch),
                    "cells": ch.cells, "precision": a.precision,
                    "inner": f"until 1e-3 drop of all five update norms, cap {a.cap}",
                    "mean_inner_iterations": round(mean_iters, 2), "inner_iterations": iters,
@@ -408,7 +418,7 @@ def run_reference(a, dist: Dist) -> dict | None:
             "n_gpus": dist.world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": round(sec_iter * m_it * 1e3, 1), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic seeded channel",
-            "config": {"workload": f"channel {ch.nx}x{ch.ny}x{ch.nz} cells, Mach 0.2, Re_b 5600",
+            "config": {"workload": workload_label(ch),
                        "cells": ch.cells, "inner_iterations_per_step": m_it},
             "cpu_baseline": {"value": round(value, 5), "unit": "Mcell-steps/s", "cores": cores,
                              "kind": "reference", "sample": sample},

@@ -248,7 +248,13 @@ WORKLOADS = {
     # profiling case: the channel at 160 x 128 x 128 cells (sweep data of one
     # pass ~0.4 GB, larger than L2; ~3 GB on the device)
     "p1": (160, 128, 128),
+    # the reference's own open configuration at the 256 x 192 x 192 size
+    # (OPEN): inflow / outflow, sponges, heated lower wall, buoyancy
+    "o2": (256, 192, 192),
 }
+# open-configuration workloads: sponge layers (inlet, outlet cells) in the
+# proportions of the reference's Resolution.h (100 and 150 of 650 planes)
+OPEN = {"o2": (40, 60)}
 # wall amplitude (fraction of h) of the wavy workloads: 0.01, not the 0.05 of
 # its description, because the reference's scheme diverges within a few
 # steps for amplitudes of 0.02 h and more on this mapping
@@ -256,7 +262,13 @@ WAVY = {"c4": 0.01}
 
 
 def workload(name: str) -> "Channel":
-    """The Channel of a named workload (c4 has the wavy lower wall)."""
+    """The Channel of a named workload (c4 has the wavy lower wall, o2 is the
+    open configuration with the reference's heated lower wall, 343.0592 K,
+    and buoyancy)."""
     if name in WAVY:
         return Channel(*WORKLOADS[name], wavy=True, wave=WAVY[name])
+    if name in OPEN:
+        nin, nout = OPEN[name]
+        return Channel(*WORKLOADS[name], x_open=True, nx_inlet=nin, nx_outlet=nout, buoyancy=True,
+                       twall_lo=343.0592)
     return Channel(*WORKLOADS[name])

@@ -207,7 +207,9 @@ void drop_graph(cgli_ctx *c) {
 // (xidx = ztdz = 1, the other off-diagonal terms 0, J and etdy functions of
 // j alone) over every cell the sweeps read: planes 2..ie+1, rows 2..jn,
 // k = 2..kn.  If so the sweeps read J(j), etdy(j) from two small tables
-// instead of ten 3-D arrays.
+// instead of ten 3-D arrays.  On an open slab the end planes only enter
+// through products with their zero implicit halo, so planes 3..ie decide
+// (the end planes' ztdy, ztdz are zero there, Jacobian.cpp:110-157).
 int check_channel_metrics(cgli_ctx *c) {
   const cgli::Dev &d = c->d;
   size_t n = (size_t)d.X * d.Y * d.Z;
@@ -223,7 +225,7 @@ int check_channel_metrics(cgli_ctx *c) {
   for (int j = 2; j <= jn && ok; j++) {
     size_t r = cgli::ix(d, 3, j, 2);
     jt[j] = J[r]; et[j] = m[4][r];
-    for (int i = 2; i <= ie + 1 && ok; i++)
+    for (int i = d.x_open ? 3 : 2; i <= (d.x_open ? ie : ie + 1) && ok; i++)
       for (int k = 2; k <= kn && ok; k++) {
         size_t q = cgli::ix(d, i, j, k);
         ok = J[q] == jt[j] && m[4][q] == et[j] && m[0][q] == 1.0 && m[8][q] == 1.0 && m[1][q] == 0.0 &&
@@ -442,6 +444,7 @@ int cgli_channel_metrics(cgli_ctx *c, double high, double stretch) {
 
 int cgli_wavy_channel_metrics(cgli_ctx *c, double high, double stretch, double amplitude) {
   int rc = check(c); if (rc) return rc;
+  if (c->p.x_open) return fail(CGLI_EINVAL, "the wavy-wall metrics are defined for the periodic slab only");
   if (!(high > 0 && stretch > 0) || !(fabs(amplitude) < 0.5 * high))
     return fail(CGLI_EINVAL, "need high, stretch > 0 and |amplitude| < high / 2");
   cgli::MetricSet M;

@@ -201,12 +201,22 @@ def build(params: dict, name: str | None = None, jobs: int = 8) -> str:
     return lib
 
 
+def params_for(ch) -> dict:
+    """Build parameters of the reference for a Channel workload (the open
+    configuration adds its sponge layers; wall temperatures are patched in)."""
+    sys.path.insert(0, REPO)
+    from cgli_fu_flow_b200.channel import MU0, PR, STRETCH
+    params = dict(nx=ch.nx, ny=ch.ny, nz=ch.nz, dxi=ch.dxi, det=ch.det, dzt=ch.dzt, high=ch.high,
+                  mu=MU0, pr=PR, stretch=STRETCH, twall_lo=ch.twall_lo, twall_hi=ch.twall_hi)
+    if ch.x_open:
+        params.update(x_open=1, nx_inlet=ch.nx_inlet, nx_outlet=ch.nx_outlet)
+    return params
+
+
 def channel_params(nx: int, ny: int, nz: int) -> dict:
     sys.path.insert(0, REPO)
-    from cgli_fu_flow_b200.channel import Channel, MU0, PR, STRETCH, T0
-    ch = Channel(nx, ny, nz)
-    return dict(nx=nx, ny=ny, nz=nz, dxi=ch.dxi, det=ch.det, dzt=ch.dzt, high=ch.high,
-                mu=MU0, pr=PR, stretch=STRETCH, twall_lo=T0, twall_hi=T0)
+    from cgli_fu_flow_b200.channel import Channel
+    return params_for(Channel(nx, ny, nz))
 
 
 if __name__ == "__main__":

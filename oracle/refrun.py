@@ -25,11 +25,7 @@ class RefSolver:
         if inner_solver not in ("lusgs", "dplur"):
             raise ValueError(inner_solver)
         self.inner_solver = inner_solver
-        params = dict(nx=ch.nx, ny=ch.ny, nz=ch.nz, dxi=ch.dxi, det=ch.det, dzt=ch.dzt,
-                      high=ch.high, mu=_c().MU0, pr=_c().PR, stretch=_c().STRETCH,
-                      twall_lo=ch.twall_lo, twall_hi=ch.twall_hi)
-        if ch.x_open:
-            params.update(x_open=1, nx_inlet=ch.nx_inlet, nx_outlet=ch.nx_outlet)
+        params = build_ref.params_for(ch)
         if build:
             path = build_ref.build(params, ch.name)
         else:
