@@ -157,6 +157,15 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def launches_per_iteration(ch) -> int:
+    """Kernels of one fused LU-SGS inner iteration: x halo, Y and Z boundaries,
+    three fluxes, three viscous kernels, the residual, four (halo products +
+    wavefront pass) pairs, the update and the norm reduction; an open slab
+    adds the X boundary and the sponge target reduction and drops the x halo.
+    A step adds the bulk-flux pair and the time-level shift."""
+    return 21 + (1 if ch.x_open else 0)
+
+
 def workload_label(ch) -> str:
     if ch.x_open:
         return (f"open channel {ch.nx}x{ch.ny}x{ch.nz} cells (the reference's own configuration: inflow / outflow, "
@@ -229,7 +238,7 @@ def run_gpu(a, dist: Dist) -> dict | None:
         "clocks": ck,
         "stage_ms": {k: round(v, 4) for k, v in stages.items()},
         "roofline": roof,
-        "gpu_launches": int(sum(15 * n + 2 for n in iters)),
+        "gpu_launches": int(sum(launches_per_iteration(ch) * n + 3 for n in iters)),
     }
     if e2e:
         out["e2e"] = e2e

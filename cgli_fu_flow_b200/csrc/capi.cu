@@ -724,7 +724,7 @@ int cgli_inner_iteration(cgli_ctx *c, double er[5]) {
     if (e != cudaSuccess) return fail(CGLI_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
   }
   CUDA_TRY(cudaGraphLaunch(c->iter_graph, c->stream));
-  return read_norms(c, er, dplur ? c->update_blocks : c->sweep_tiles);
+  return read_norms(c, er, c->update_blocks);
 }
 
 int cgli_driven_force(cgli_ctx *c, double *bulk_flux) {

@@ -37,7 +37,6 @@ struct SweepArgs {
   const int *order;               // tile visiting order (anti-diagonals)
   const double *Jtab, *etdytab;   // per-j metrics of a grid uniform in x and z
   int channel_metrics;            // 1: use Jtab / etdytab instead of the 3-D arrays
-  int final_pass;                 // backward pass of the last sweep: apply the update
   int spin_limit;                 // bounded wait (polls) for a neighbouring tile
 };
 

@@ -29,9 +29,10 @@
 // The periodic x halo keeps the reference's lag: the forward pass at i = 3
 // uses dQ of plane Nx+2 as it was at the start of the sweep (halo_f), the
 // backward pass at i = Nx+2 uses dQ of plane 3 (halo_b).  The backward pass of
-// the first sweep writes both halos for the second sweep; the final backward
-// pass also applies the primitive update of Dual_time_stepping.cpp:1702-1743
-// and accumulates the squared increments of the residual norms.
+// the first sweep writes both halos for the second sweep; after the final
+// backward pass a separate, fully parallel kernel applies the primitive
+// update of Dual_time_stepping.cpp:1702-1743 and accumulates the squared
+// increments of the residual norms.
 //
 // T is the arithmetic type of the sweep (double, or float for CGLI_MIXED).
 #include "cgli_dev.cuh"
@@ -182,7 +183,6 @@ __global__ void __launch_bounds__(TI *TJ) k_sweep(Dev d, SweepArgs a) {
   __shared__ T sy[2][TI][TJ][5];   // j-direction products
   __shared__ double s_jt[TJ], s_et[TJ];
   __shared__ int s_tile;
-  __shared__ double s_red[5];
   const int il = threadIdx.x / TJ, jl = threadIdx.x % TJ;
   const int nti = (d.nx + TI - 1) / TI, ntj = (d.ny + TJ - 1) / TJ, ntiles = nti * ntj;
   if (threadIdx.x == 0) s_tile = (int)atomicAdd(a.ticket, 1u);
@@ -215,7 +215,6 @@ __global__ void __launch_bounds__(TI *TJ) k_sweep(Dev d, SweepArgs a) {
   T *xb = SweepPtrs<T>::xb(a), *yb = SweepPtrs<T>::yb(a);
   T *const *dq = SweepPtrs<T>::dq(a);
   T carry_z[5] = {0, 0, 0, 0, 0};
-  double acc[5] = {0, 0, 0, 0, 0};
 
   // hand-over values of the next two steps, loaded ahead: a neighbouring
   // tile runs just far enough ahead for its value to exist when needed, so
@@ -336,30 +335,7 @@ __global__ void __launch_bounds__(TI *TJ) k_sweep(Dev d, SweepArgs a) {
 #pragma unroll
         for (int v = 0; v < 5; v++) __stcg(dst + v, oy[v]);
       }
-      if (BACKWARD && a.final_pass) {
-        // Dual_time_stepping.cpp:1702-1743: primitive update in place (FP64)
-        const long long cc = ix(d, i, j, 2 + kl);
-        const double J = Met::kChannel ? s_jt[jl] : d.J[cc];
-        double q1 = d.U_[0][cc];
-        double rhoold = q1 * J;
-        double Uold = d.U_[1][cc] / q1, Vold = d.U_[2][cc] / q1, Wold = d.U_[3][cc] / q1;
-        double VVold = Uold * Uold + Vold * Vold + Wold * Wold;
-        double Pold = (d.U_[4][cc] * J - 0.5 * rhoold * VVold) * (KG - 1);
-        double Told = Pold / rhoold;
-        double P = Pold + (double)n[0] * J, U = Uold + (double)n[1] * J, V = Vold + (double)n[2] * J;
-        double W = Wold + (double)n[3] * J, Tn = Told + (double)n[4] * J;
-        double rho = P / Tn;
-        d.U_[0][cc] = rho / J;
-        d.U_[1][cc] = rho * U / J;
-        d.U_[2][cc] = rho * V / J;
-        d.U_[3][cc] = rho * W / J;
-        d.U_[4][cc] = (P / (KG - 1) + 0.5 * rho * (U * U + V * V + W * W)) / J;
-        acc[0] += (rho - rhoold) * (rho - rhoold);
-        acc[1] += (U - Uold) * (U - Uold);
-        acc[2] += (V - Vold) * (V - Vold);
-        acc[3] += (W - Wold) * (W - Wold);
-        acc[4] += (Tn - Told) * (Tn - Told);
-      } else {
+      {
 #pragma unroll
         for (int v = 0; v < 5; v++) dq[v][cur.slot] = n[v];
         if (BACKWARD && !d.x_open) {
@@ -381,12 +357,44 @@ __global__ void __launch_bounds__(TI *TJ) k_sweep(Dev d, SweepArgs a) {
     cur = nxt;
     __syncthreads();
   }
-  if (BACKWARD && a.final_pass) {
-    block_sum5(acc, s_red);
-    __syncthreads();
-    if (threadIdx.x == 0)
-      for (int v = 0; v < 5; v++) d.partial[5 * (long long)tile + v] = s_red[v];
+}
+
+// Dual_time_stepping.cpp:1702-1743 after the last backward pass: the
+// primitive update of every interior cell from its final dQ (read from the
+// tile-skewed layout), fully parallel rather than inside the wavefront's
+// chain of dependent steps, with per-block partial sums of the squared
+// increments (:1761-1776); one block per (j, i) row of k.  The divisions by
+// q1, rho, T and J are reciprocals (1/J from the table).
+template <typename T>
+__global__ void __launch_bounds__(128) k_update_skewed(Dev d, SweepArgs a) {
+  const int j = 2 + blockIdx.x, i = 3 + blockIdx.y;
+  T *const *dq = SweepPtrs<T>::dq(a);
+  double acc[5] = {0, 0, 0, 0, 0};
+  for (int k = 2 + threadIdx.x; k <= d.nz + 1; k += blockDim.x) {
+    const long long c = ix(d, i, j, k), slot = skew_slot(d, i, j, k);
+    const double J = d.J[c], iJ = d.iJ[c];
+    const double q1 = d.U_[0][c], iq1 = 1 / q1;
+    const double rhoold = q1 * J;
+    const double Uold = d.U_[1][c] * iq1, Vold = d.U_[2][c] * iq1, Wold = d.U_[3][c] * iq1;
+    const double VVold = Uold * Uold + Vold * Vold + Wold * Wold;
+    const double Pold = (d.U_[4][c] * J - 0.5 * rhoold * VVold) * (KG - 1);
+    const double Told = Pold / rhoold;
+    const double P = Pold + (double)dq[0][slot] * J, U = Uold + (double)dq[1][slot] * J;
+    const double V = Vold + (double)dq[2][slot] * J, W = Wold + (double)dq[3][slot] * J;
+    const double Tn = Told + (double)dq[4][slot] * J;
+    const double rho = P / Tn, rJ = rho * iJ;
+    d.U_[0][c] = rJ;
+    d.U_[1][c] = rJ * U;
+    d.U_[2][c] = rJ * V;
+    d.U_[3][c] = rJ * W;
+    d.U_[4][c] = (P * (1 / (KG - 1)) + 0.5 * rho * (U * U + V * V + W * W)) * iJ;
+    acc[0] += (rho - rhoold) * (rho - rhoold);
+    acc[1] += (U - Uold) * (U - Uold);
+    acc[2] += (V - Vold) * (V - Vold);
+    acc[3] += (W - Wold) * (W - Wold);
+    acc[4] += (Tn - Told) * (Tn - Told);
   }
+  block_sum5(acc, d.partial + 5 * ((long long)blockIdx.y * gridDim.x + blockIdx.x));
 }
 
 // tickets follow the anti-diagonals ta + tb of the tile grid
@@ -406,9 +414,7 @@ static void run_sweeps(const Dev &d, const SweepArgs &a, cudaStream_t s) {
   T *xb = sizeof(T) == 8 ? (T *)a.xbuf : (T *)a.xbuff;
   T *yb = sizeof(T) == 8 ? (T *)a.ybuf : (T *)a.ybuff;
   for (int sweep = 0; sweep < 2; sweep++) {
-    SweepArgs f = a, b = a;
-    f.final_pass = 0;
-    b.final_pass = sweep == 1;
+    const SweepArgs &f = a, &b = a;
     for (int pass = 0; pass < 2; pass++) {
       // ticket reset and sentinel fill of the hand-over buffers
       cudaMemsetAsync(a.ticket, 0, sizeof(unsigned int), s);
@@ -424,6 +430,7 @@ static void run_sweeps(const Dev &d, const SweepArgs &a, cudaStream_t s) {
       }
     }
   }
+  k_update_skewed<T><<<dim3(d.ny, d.nx), 128, 0, s>>>(d, a);
 }
 
 template <int TI, int TJ, class Met, typename T>
@@ -432,8 +439,7 @@ static void run_one_pass(const Dev &d, const SweepArgs &a, cudaStream_t s, bool 
   const size_t xbytes = (size_t)ntiles * TJ * d.nz * 5 * sizeof(T), ybytes = (size_t)ntiles * TI * d.nz * 5 * sizeof(T);
   T *xb = sizeof(T) == 8 ? (T *)a.xbuf : (T *)a.xbuff;
   T *yb = sizeof(T) == 8 ? (T *)a.ybuf : (T *)a.ybuff;
-  SweepArgs b = a;
-  b.final_pass = final_pass;
+  const SweepArgs &b = a;
   cudaMemsetAsync(a.ticket, 0, sizeof(unsigned int), s);
   cudaMemsetAsync(xb, 0xff, xbytes, s);
   cudaMemsetAsync(yb, 0xff, ybytes, s);
@@ -445,6 +451,7 @@ static void run_one_pass(const Dev &d, const SweepArgs &a, cudaStream_t s, bool 
     k_halo_products<Met, true, T><<<hg, 64, 0, s>>>(d, b);
     k_sweep<TI, TJ, Met, true, T><<<ntiles, TI * TJ, 0, s>>>(d, b);
   }
+  if (final_pass) k_update_skewed<T><<<dim3(d.ny, d.nx), 128, 0, s>>>(d, a);
 }
 
 void launch_sweep_pass(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed, bool backward, bool final_pass) {
