@@ -4,6 +4,11 @@
 #include "cgli_dev.cuh"
 #include "cgli_launch.h"
 
+// CTAs per SM the residual kernel is compiled for (register cap)
+#ifndef CGLI_RESIDUAL_MINBLOCKS
+#define CGLI_RESIDUAL_MINBLOCKS 1
+#endif
+
 namespace cgli {
 
 // Dual_time_stepping.cpp:737-922 for the fast path: MR of every interior
@@ -11,7 +16,7 @@ namespace cgli {
 // (the reference initialises NL = NR = D^-1 MR, :897-908, and the sweep
 // exchanges planes ie and 3 before its first pass, :942-976)
 template <bool MIXED>
-__global__ void k_residual_fast(Dev d, SweepArgs a) {
+__global__ void __launch_bounds__(64, CGLI_RESIDUAL_MINBLOCKS) k_residual_fast(Dev d, SweepArgs a) {
   int k = 2 + blockIdx.x * blockDim.x + threadIdx.x;
   int j = 2 + blockIdx.y;
   int i = 2 + blockIdx.z;

@@ -7,6 +7,17 @@
 #include "cgli_launch.h"
 #include "viscous_face.cuh"
 
+// CTAs of 64 threads per SM the inviscid flux and the viscous face kernels
+// are compiled for (register caps: 12 CTAs leave the fluxes 80 registers, a
+// few spilled, 18 % faster than the uncapped 116 at 256x192x192; 8 CTAs
+// leave the viscous faces 128, 3 % faster than 154, 10 CTAs are slower)
+#ifndef CGLI_FLUX_MINBLOCKS
+#define CGLI_FLUX_MINBLOCKS 12
+#endif
+#ifndef CGLI_VISCOUS_MINBLOCKS
+#define CGLI_VISCOUS_MINBLOCKS 8
+#endif
+
 namespace cgli {
 
 // ---------------------------------------------------------------- halos
@@ -176,7 +187,7 @@ __global__ void k_target_u(Dev d) {
 
 // ---------------------------------------------------------------- fluxes
 // x faces i = 2..ie, tangential j = 1..jn-1, k = 1..kn-1 (Flux_X.cpp:96-357)
-__global__ void k_flux_x(Dev d) {
+__global__ void __launch_bounds__(64, CGLI_FLUX_MINBLOCKS) k_flux_x(Dev d) {
   int k = 1 + blockIdx.x * blockDim.x + threadIdx.x;
   int j = 1 + blockIdx.y;
   int i = 2 + blockIdx.z;
@@ -222,7 +233,7 @@ __device__ __forceinline__ void muscl_y(const Dev &d, int i, int j, int k, doubl
 }
 
 // y faces j = 1..jn, i = 2..ie-1, k = 1..kn-1 (Flux_Y.cpp:94-413)
-__global__ void k_flux_y(Dev d) {
+__global__ void __launch_bounds__(64, CGLI_FLUX_MINBLOCKS) k_flux_y(Dev d) {
   int k = 1 + blockIdx.x * blockDim.x + threadIdx.x;
   int j = 1 + blockIdx.y;
   int i = 2 + blockIdx.z;
@@ -260,7 +271,7 @@ __device__ __forceinline__ void muscl_z(const Dev &d, int i, int j, int k, doubl
 }
 
 // z faces k = 1..kn, i = 2..ie-1, j = 1..jn-1 (Flux_Z.cpp:91-359)
-__global__ void k_flux_z(Dev d) {
+__global__ void __launch_bounds__(64, CGLI_FLUX_MINBLOCKS) k_flux_z(Dev d) {
   int k = 1 + blockIdx.x * blockDim.x + threadIdx.x;
   int j = 1 + blockIdx.y;
   int i = 2 + blockIdx.z;
@@ -296,7 +307,7 @@ __device__ __forceinline__ VP vp(const Dev &d, long long c) {
 // face viscous fluxes of cell (i,j,k): x face i-1/2 for j<=jn, k<=kn; y face
 // j-1/2 for i<=ie, k<=kn; z face k-1/2 for i<=ie, j<=jn (the faces the
 // divergence of Viscous_terms.cpp:875-904 reads)
-__global__ void k_viscous_faces(Dev d) {
+__global__ void __launch_bounds__(64, CGLI_VISCOUS_MINBLOCKS) k_viscous_faces(Dev d) {
   int k = 2 + blockIdx.x * blockDim.x + threadIdx.x;
   int j = 2 + blockIdx.y;
   int i = 3 + blockIdx.z;
