@@ -11,18 +11,32 @@
 
 namespace cgli {
 
+// the nine metric terms of cell c (row j): per-row tables on the channel grid
+template <bool CH>
+__device__ __forceinline__ void cell_metrics(const Dev &d, const SweepArgs &a, int j, long long c, double mm[9]) {
+  if (CH) {
+    mm[0] = 1; mm[1] = 0; mm[2] = 0; mm[3] = 0; mm[4] = a.etdytab[j]; mm[5] = 0; mm[6] = 0; mm[7] = 0; mm[8] = 1;
+  } else {
+#pragma unroll
+    for (int v2 = 0; v2 < 9; v2++) mm[v2] = d.m[v2][c];
+  }
+}
+
 // Dual_time_stepping.cpp:737-922 for the fast path: MR of every interior
 // cell, and D^-1 MR on planes ie and 3 as the lagged halos of the first sweep
 // (the reference initialises NL = NR = D^-1 MR, :897-908, and the sweep
-// exchanges planes ie and 3 before its first pass, :942-976)
-template <bool MIXED>
+// exchanges planes ie and 3 before its first pass, :942-976).  CH: the grid
+// is uniform in x and z (a.channel_metrics), J and etdy come from the per-row
+// tables instead of ten 3-D metric arrays.
+template <bool MIXED, bool CH>
 __global__ void __launch_bounds__(64, CGLI_RESIDUAL_MINBLOCKS) k_residual_fast(Dev d, SweepArgs a) {
   int k = 2 + blockIdx.x * blockDim.x + threadIdx.x;
   int j = 2 + blockIdx.y;
   int i = 2 + blockIdx.z;
   if (k > d.nz + 1) return;
   long long c = ix(d, i, j, k);
-  const double J = d.J[c], deltaT = d.dt;
+  const double J = CH ? a.Jtab[j] : d.J[c], deltaT = d.dt;
+
   const int ie = d.nx + 2;
   const bool halo_plane = (i == 2 || i == ie + 1);
   const long long slot = halo_plane ? 0 : skew_slot(d, i, j, k);
@@ -30,7 +44,7 @@ __global__ void __launch_bounds__(64, CGLI_RESIDUAL_MINBLOCKS) k_residual_fast(D
     // the cell's sweep record; planes 2 and ie+1 (the periodic halo copies)
     // go to the per-(j,k) halo records
     double mm[9], r[REC_N];
-    for (int v2 = 0; v2 < 9; v2++) mm[v2] = d.m[v2][c];
+    cell_metrics<CH>(d, a, j, c, mm);
     make_record(d.U_[0][c], d.U_[1][c], d.U_[2][c], d.U_[3][c], d.U_[4][c], J, mm, d.e, 1.0 / d.dxi, 1.0 / d.det,
                 1.0 / d.dzt, deltaT, r);
     const long long h = (long long)j * d.dj + k;
@@ -93,7 +107,7 @@ __global__ void __launch_bounds__(64, CGLI_RESIDUAL_MINBLOCKS) k_residual_fast(D
   // the lagged halos of the first sweep; an open slab's stay zero
   if (!d.x_open && (i == ie || i == 3)) {
     double mm[9];
-    for (int v2 = 0; v2 < 9; v2++) mm[v2] = d.m[v2][c];
+    cell_metrics<CH>(d, a, j, c, mm);
     Diag<double> dd = diag<double>(q, mm, d.dxi, d.det, d.dzt, deltaT);
     double n5[5] = {dd.d11 * MR[0], dd.d22 * MR[1], dd.d22 * MR[2], dd.d22 * MR[3], dd.d51 * MR[0] + dd.d22 * MR[4]};
     long long h = (long long)j * d.dj + k;
@@ -111,8 +125,13 @@ __global__ void __launch_bounds__(64, CGLI_RESIDUAL_MINBLOCKS) k_residual_fast(D
 
 void launch_residual_fast(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed) {
   dim3 g((d.nz + 63) / 64, d.ny, d.nx + 2);
-  if (mixed) k_residual_fast<true><<<g, 64, 0, s>>>(d, a);
-  else k_residual_fast<false><<<g, 64, 0, s>>>(d, a);
+  if (a.channel_metrics) {
+    if (mixed) k_residual_fast<true, true><<<g, 64, 0, s>>>(d, a);
+    else k_residual_fast<false, true><<<g, 64, 0, s>>>(d, a);
+  } else {
+    if (mixed) k_residual_fast<true, false><<<g, 64, 0, s>>>(d, a);
+    else k_residual_fast<false, false><<<g, 64, 0, s>>>(d, a);
+  }
 }
 
 void launch_fused_iteration(const Dev &d, const SweepArgs &a, cudaStream_t s, int precision) {

@@ -38,6 +38,11 @@
 #include "cgli_dev.cuh"
 #include "cgli_launch.h"
 
+// tiles per SM the wavefront kernel is compiled for (a register cap)
+#ifndef CGLI_SWEEP_MINBLOCKS
+#define CGLI_SWEEP_MINBLOCKS 1
+#endif
+
 namespace cgli {
 
 template <typename T> struct SweepPtrs;
@@ -178,7 +183,7 @@ __global__ void k_halo_products(Dev d, SweepArgs a) {
 }
 
 template <int TI, int TJ, class Met, bool BACKWARD, typename T>
-__global__ void __launch_bounds__(TI *TJ) k_sweep(Dev d, SweepArgs a) {
+__global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, SweepArgs a) {
   __shared__ T sx[2][TI][TJ][5];   // i-direction products, double-buffered by step parity
   __shared__ T sy[2][TI][TJ][5];   // j-direction products
   __shared__ double s_jt[TJ], s_et[TJ];
