@@ -338,33 +338,38 @@ def run_arms(a, ch, dist) -> dict:
 
 
 def run_e2e(a, ch, prec, dist: Dist) -> dict:
-    """The same steps through the C ABI with pinned host buffers: every step
-    uploads U_, U, Uq (the step's inputs) and downloads U_ (its result)."""
+    """The same steps through the C ABI with the time levels kept on the host
+    in pinned buffers: every step uploads Q^n (as U_ and U) and Q^(n-1) (as
+    Uq) with cgli_set_array, runs cgli_step, and downloads Q^(n+1) with
+    cgli_get_state; the host rotates its three buffers (no host copies)."""
     import torch
     from cgli_fu_flow_b200.solver import Solver, reference_state
     sol = Solver(ch, prec)
     J = sol.get("J")
     U_, U, Uq = reference_state(ch, J, ch.initial_conserved(), ch.initial_conserved())
     shape = (5,) + ch.shape
-    pin = {k: torch.empty(shape, dtype=torch.float64, pin_memory=True) for k in ("U_", "U", "Uq")}
-    hp = {k: v.numpy() for k, v in pin.items()}
-    hp["U_"][:] = U_
-    hp["U"][:] = U
-    hp["Uq"][:] = Uq
-    for _ in range(max(1, min(a.warmup, 2))):
-        sol.set_state(hp["U_"], hp["U"], hp["Uq"])
+    pin = [torch.empty(shape, dtype=torch.float64, pin_memory=True) for _ in range(3)]
+    buf = [t.numpy() for t in pin]
+    buf[0][:] = U
+    buf[1][:] = Uq
+    sol.set_state(U_, U, Uq)       # a fresh run: the stopping rule's running maxima start here
+
+    def one_step(b):
+        for v in range(5):
+            sol.set(f"U{v + 1}_", b[0][v])
+            sol.set(f"U{v + 1}", b[0][v])
+            sol.set(f"U{v + 1}q", b[1][v])
         sol.step(None, a.drop, a.cap)
+        sol.q_into(b[2])
+        return [b[2], b[0], b[1]]  # Q^(n+1), Q^n, free
+
+    for _ in range(max(1, min(a.warmup, 2))):
+        buf = one_step(buf)
     n = ch.shape[0] * ch.shape[1] * ch.shape[2] * 8
     dist.barrier()
     sol.event(2)
     for _ in range(a.steps):
-        sol.set_state(hp["U_"], hp["U"], hp["Uq"])
-        sol.step(None, a.drop, a.cap)
-        out = sol.q()
-        # the host keeps the time levels: Q^(n-1) <- Q^n, Q^n <- Q^(n+1)
-        hp["Uq"][:] = hp["U"]
-        hp["U"][:] = out
-        hp["U_"][:] = out
+        buf = one_step(buf)
     sol.event(3)
     ms = dist.max(sol.elapsed_ms(2, 3))
     sol.close()

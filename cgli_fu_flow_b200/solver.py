@@ -242,6 +242,12 @@ class Solver:
         self._rc(self.L.cgli_get_state(self.h, _ptrs(out)))
         return np.stack(out)
 
+    def q_into(self, out: np.ndarray) -> None:
+        """cgli_get_state into a caller's contiguous (5, X_np, Y_m, Z_m) array
+        (e.g. pinned host memory), without allocating."""
+        assert out.shape == (5,) + self.shape and out.flags.c_contiguous and out.dtype == np.float64
+        self._rc(self.L.cgli_get_state(self.h, _ptrs([out[v] for v in range(5)])))
+
     # ---------------------------------------------------- reference routines
     def halo_x(self):
         self._rc(self.L.cgli_halo_x(self.h))
