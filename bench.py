@@ -339,8 +339,8 @@ def run_arms(a, ch, dist) -> dict:
 
 def run_e2e(a, ch, prec, dist: Dist) -> dict:
     """The same steps through the C ABI with the time levels kept on the host
-    in pinned buffers: every step uploads Q^n (as U_ and U) and Q^(n-1) (as
-    Uq) with cgli_set_array, runs cgli_step, and downloads Q^(n+1) with
+    in pinned buffers: every step uploads Q^n and Q^(n-1) with
+    cgli_set_levels, runs cgli_step, and downloads Q^(n+1) with
     cgli_get_state; the host rotates its three buffers (no host copies)."""
     import torch
     from cgli_fu_flow_b200.solver import Solver, reference_state
@@ -355,10 +355,7 @@ def run_e2e(a, ch, prec, dist: Dist) -> dict:
     sol.set_state(U_, U, Uq)       # a fresh run: the stopping rule's running maxima start here
 
     def one_step(b):
-        for v in range(5):
-            sol.set(f"U{v + 1}_", b[0][v])
-            sol.set(f"U{v + 1}", b[0][v])
-            sol.set(f"U{v + 1}q", b[1][v])
+        sol.set_levels(b[0], b[1])
         sol.step(None, a.drop, a.cap)
         sol.q_into(b[2])
         return [b[2], b[0], b[1]]  # Q^(n+1), Q^n, free
@@ -374,7 +371,7 @@ def run_e2e(a, ch, prec, dist: Dist) -> dict:
     ms = dist.max(sol.elapsed_ms(2, 3))
     sol.close()
     value = dist.sum(float(ch.cells) * a.steps) / (ms / 1e3) / 1e6
-    return {"value": round(value, 3), "unit": "Mcell-steps/s", "h2d_bytes_per_step": 15 * n,
+    return {"value": round(value, 3), "unit": "Mcell-steps/s", "h2d_bytes_per_step": 10 * n,
             "d2h_bytes_per_step": 5 * n}
 
 

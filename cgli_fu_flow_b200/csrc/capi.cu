@@ -486,6 +486,22 @@ int cgli_set_state(cgli_ctx *c, const double *const U_[5], const double *const U
   return CGLI_OK;
 }
 
+int cgli_set_levels(cgli_ctx *c, const double *const U[5], const double *const Uq[5]) {
+  int rc = check(c); if (rc) return rc;
+  if (!U || !Uq) return fail(CGLI_EINVAL, "null argument");
+  if (!c->have_state) return fail(CGLI_ESTATE, "state not set (cgli_set_state once before cgli_set_levels)");
+  size_t n = (size_t)c->d.X * c->d.Y * c->d.Z * sizeof(double);
+  for (int v = 0; v < 5; v++) {
+    if (!U[v] || !Uq[v]) return fail(CGLI_EINVAL, "null state array");
+    CUDA_TRY(cudaMemcpyAsync(c->d.Uqq[v], c->d.Uq[v], n, cudaMemcpyDeviceToDevice, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(c->d.U[v], U[v], n, cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(c->d.U_[v], c->d.U[v], n, cudaMemcpyDeviceToDevice, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(c->d.Uq[v], Uq[v], n, cudaMemcpyHostToDevice, c->stream));
+  }
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return CGLI_OK;
+}
+
 int cgli_copy_state(cgli_ctx *dst, const cgli_ctx *src) {
   int rc = check(dst); if (rc) return rc;
   if (!src || !src->have_state) return fail(CGLI_ESTATE, "source context has no state");

@@ -56,7 +56,7 @@ EXPORTS = [
     "cgli_copy_state", "cgli_cnn_time_inference", "cgli_wavy_channel_metrics", "cgli_wavy_channel_metrics_host",
     "cgli_statistics_accumulate", "cgli_statistics_get", "cgli_statistics_reset",
     "cgli_write_restart", "cgli_read_restart", "cgli_write_history", "cgli_read_history",
-    "cgli_dplusgs", "cgli_set_inner_solver", "cgli_x_boundary_condition",
+    "cgli_dplusgs", "cgli_set_inner_solver", "cgli_x_boundary_condition", "cgli_set_levels",
 ]
 
 INNER_SOLVERS = {"lusgs": 0, "dplur": 1}
@@ -85,6 +85,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cgli_channel_metrics.argtypes = [P, D, D]
     L.cgli_set_state.argtypes = [P, P, P, P]
     L.cgli_get_state.argtypes = [P, P]
+    L.cgli_set_levels.argtypes = [P, P, P]
     for n in ("cgli_halo_x", "cgli_y_boundary_condition", "cgli_z_boundary_condition", "cgli_flux_x",
               "cgli_flux_y", "cgli_flux_z", "cgli_viscous_terms", "cgli_end_step"):
         getattr(L, n).argtypes = [P]
@@ -241,6 +242,13 @@ class Solver:
         out = [np.empty(self.shape) for _ in range(5)]
         self._rc(self.L.cgli_get_state(self.h, _ptrs(out)))
         return np.stack(out)
+
+    def set_levels(self, qn: np.ndarray, qnm1: np.ndarray) -> None:
+        """cgli_set_levels: Q^n/J and Q^(n-1)/J, each (5, X_np, Y_m, Z_m)
+        contiguous (e.g. pinned), for a host-driven loop."""
+        for x in (qn, qnm1):
+            assert x.shape == (5,) + self.shape and x.flags.c_contiguous and x.dtype == np.float64
+        self._rc(self.L.cgli_set_levels(self.h, _ptrs([qn[v] for v in range(5)]), _ptrs([qnm1[v] for v in range(5)])))
 
     def q_into(self, out: np.ndarray) -> None:
         """cgli_get_state into a caller's contiguous (5, X_np, Y_m, Z_m) array

@@ -114,6 +114,13 @@ int cgli_set_state(cgli_ctx *ctx, const double *const U_[5], const double *const
                    const double *const Uq[5]);
 /* Reads back Q^(n+1,m) (5 arrays). */
 int cgli_get_state(cgli_ctx *ctx, double *const U_[5]);
+/* The time levels of the next step from a host-driven loop that keeps them
+ * itself (it does main.cpp:364-386 on the host): U_ = U = U[v] (Q^n/J) and
+ * Uq = Uq[v] (Q^(n-1)/J), reference layout.  Q^n crosses the bus once (U_ is
+ * a device copy), and the previous device Uq becomes Q^(n-2) of the
+ * extrapolated guess.  Unlike cgli_set_state, the running maxima of the
+ * stopping rule and the step history carry on. */
+int cgli_set_levels(cgli_ctx *ctx, const double *const U[5], const double *const Uq[5]);
 /* ---- restart files in the reference's format.  cgli_write_restart writes
  * Q^n = U*J and Q^(n-1) = Uq*J of this slab into `path` as Output.cpp:187-284
  * lays out LES%05d.bin: ten fields, each spanning a global x extent of

@@ -322,3 +322,28 @@ def test_mixed_mean_velocity_profile_within_half_percent(lib):
     diff = np.abs(prof[1] - prof[0]).max() / ch.u_b
     print("mean U profile, mixed vs FP64, max difference / U_b:", diff)
     assert diff <= 5e-3
+
+
+def test_host_driven_loop_with_set_levels_matches_resident_run(lib):
+    """A loop that keeps the time levels on the host (cgli_get_state after
+    each step, cgli_set_levels before the next) reproduces the device-resident
+    run bit for bit, stopping-rule iteration counts included (the running
+    maxima carry on through cgli_set_levels)."""
+    import numpy as np
+    from cgli_fu_flow_b200.solver import Solver
+    ch = Channel(16, 12, 8)
+    a, b = Solver(ch), Solver(ch)
+    a.init(); b.init()
+    shape = (5,) + ch.shape
+    qn = np.stack([b.get(f"U{v}") for v in range(1, 6)])
+    qm = np.stack([b.get(f"U{v}q") for v in range(1, 6)])
+    out = np.empty(shape)
+    for _ in range(4):
+        it_a, _ = a.step(None, drop=1e-2, cap=10)
+        b.set_levels(np.ascontiguousarray(qn), np.ascontiguousarray(qm))
+        it_b, _ = b.step(None, drop=1e-2, cap=10)
+        assert it_a == it_b
+        b.q_into(out)
+        qm, qn = qn, out.copy()
+    sl = (slice(None), slice(3, ch.nx + 3), slice(2, ch.ny + 2), slice(2, ch.nz + 2))
+    assert np.array_equal(a.q()[sl], b.q()[sl])
