@@ -326,25 +326,23 @@ int cgli_create(const cgli_params *p, cgli_ctx **out) {
     for (int v = 0; v < 5; v++) {
       if (mixed) {
         if (rc == CGLI_OK) rc = alloc(c, nsk * es, (void **)&a.dqf[v]);
-        if (rc == CGLI_OK) rc = alloc(c, nsk * es, (void **)&a.mrf[v]);
         if (rc == CGLI_OK) rc = alloc(c, plane * es, (void **)&a.halo_ff[v]);
         if (rc == CGLI_OK) rc = alloc(c, plane * es, (void **)&a.halo_bf[v]);
         if (rc == CGLI_OK) rc = alloc(c, plane * es, (void **)&a.hxpf[v]);
       } else {
         if (rc == CGLI_OK) rc = alloc(c, nsk * es, (void **)&a.dq[v]);
-        if (rc == CGLI_OK) rc = alloc(c, nsk * es, (void **)&a.mrs[v]);
         if (rc == CGLI_OK) rc = alloc(c, plane * es, (void **)&a.halo_f[v]);
         if (rc == CGLI_OK) rc = alloc(c, plane * es, (void **)&a.halo_b[v]);
         if (rc == CGLI_OK) rc = alloc(c, plane * es, (void **)&a.hxp[v]);
       }
     }
+    if (rc == CGLI_OK)
+      rc = alloc(c, nsk * cgli::CR_N * es, mixed ? (void **)&a.cellrecf : (void **)&a.cellrec);
     for (int v = 0; v < cgli::REC_N; v++) {
       if (mixed) {
-        if (rc == CGLI_OK) rc = alloc(c, nsk * es, (void **)&a.recf[v]);
         if (rc == CGLI_OK) rc = alloc(c, plane * es, (void **)&a.hrecf_f[v]);
         if (rc == CGLI_OK) rc = alloc(c, plane * es, (void **)&a.hrecf_b[v]);
       } else {
-        if (rc == CGLI_OK) rc = alloc(c, nsk * es, (void **)&a.rec[v]);
         if (rc == CGLI_OK) rc = alloc(c, plane * es, (void **)&a.hrec_f[v]);
         if (rc == CGLI_OK) rc = alloc(c, plane * es, (void **)&a.hrec_b[v]);
       }
@@ -365,6 +363,10 @@ int cgli_create(const cgli_params *p, cgli_ctx **out) {
     if (rc == CGLI_OK) rc = alloc(c, sizeof(double) * d.Y, (void **)&et);
     a.Jtab = jt; a.etdytab = et;
     a.spin_limit = 1 << 22;
+  }
+  if (rc == CGLI_OK) {
+    cudaError_t e = cgli::sweep_kernel_attributes();
+    if (e != cudaSuccess) rc = fail(CGLI_ECUDA, std::string("sweep kernel attributes: ") + cudaGetErrorString(e));
   }
   if (rc == CGLI_OK && cudaMallocHost(&c->h_norms, 16 * sizeof(double)) != cudaSuccess)
     rc = fail(CGLI_ENOMEM, "cudaMallocHost");

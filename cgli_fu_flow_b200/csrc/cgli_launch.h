@@ -9,6 +9,10 @@
 
 namespace cgli {
 
+// words per slot of SweepArgs::cellrec: record, MR, pad
+constexpr int CR_N = REC_N + 5 + 1;
+constexpr int CR_MR = REC_N;
+
 // tile shape of the wavefront sweeps: TI x TJ (i, j) columns per CTA
 constexpr int SWEEP_TI = 8;
 constexpr int SWEEP_TJ = 16;
@@ -19,10 +23,12 @@ struct SweepArgs {
   // per-cell sweep data in the tile-skewed layout: slot (tile, forward step,
   // thread) = (tile * S + s) * TI*TJ + t, S = Nz + TI + TJ - 2
   double *dq[5];                  // dQ: forward result, then backward result (in place)
-  double *mrs[5];                 // residual MR
-  double *rec[REC_N];             // split-Jacobian / diagonal record
+  // per slot, CR_N consecutive words: the split-Jacobian / diagonal record
+  // (REC_N), the residual MR (5) and one pad word, so that the residual
+  // writes and the sweep reads whole 16-byte vectors of one cell
+  double *cellrec;
   // the same in float for CGLI_MIXED
-  float *dqf[5], *mrf[5], *recf[REC_N];
+  float *dqf[5], *cellrecf;
   // periodic lagged halos, indexed j*Z_m + k: dQ of plane ie (forward) / 3
   // (backward) and the records of planes 2 / ie+1
   double *halo_f[5], *halo_b[5], *hrec_f[REC_N], *hrec_b[REC_N];
@@ -55,6 +61,8 @@ __host__ __device__ __forceinline__ long long skew_size(const Dev &d) {
 }
 
 void sweep_tile_order(int nti, int ntj, std::vector<int> &order);
+// shared-memory opt-in of the wavefront kernels (once per process and device)
+cudaError_t sweep_kernel_attributes();
 void launch_sweeps(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed);
 // one pass (forward / backward, final with the update) of the sweeps
 void launch_sweep_pass(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed, bool backward, bool final_pass);

@@ -48,20 +48,32 @@ __global__ void __launch_bounds__(64, CGLI_RESIDUAL_MINBLOCKS) k_residual_fast(D
     make_record(d.U_[0][c], d.U_[1][c], d.U_[2][c], d.U_[3][c], d.U_[4][c], J, mm, d.e, 1.0 / d.dxi, 1.0 / d.det,
                 1.0 / d.dzt, deltaT, r);
     const long long h = (long long)j * d.dj + k;
-    for (int v2 = 0; v2 < REC_N; v2++) {
-      if (MIXED) {
-        float rv = (float)r[v2];
-        if (i == 2) a.hrecf_f[v2][h] = rv;
-        else if (i == ie + 1) a.hrecf_b[v2][h] = rv;
-        else a.recf[v2][slot] = rv;
-      } else {
-        if (i == 2) a.hrec_f[v2][h] = r[v2];
-        else if (i == ie + 1) a.hrec_b[v2][h] = r[v2];
-        else a.rec[v2][slot] = r[v2];
+    if (halo_plane) {
+      for (int v2 = 0; v2 < REC_N; v2++) {
+        if (MIXED) {
+          if (i == 2) a.hrecf_f[v2][h] = (float)r[v2];
+          else a.hrecf_b[v2][h] = (float)r[v2];
+        } else {
+          if (i == 2) a.hrec_f[v2][h] = r[v2];
+          else a.hrec_b[v2][h] = r[v2];
+        }
       }
+      return;
+    }
+    // the record part of the cell's contiguous block (MR follows at the end)
+    if (MIXED) {
+      float4 *o = reinterpret_cast<float4 *>(a.cellrecf + slot * CR_N);
+      o[0] = make_float4((float)r[0], (float)r[1], (float)r[2], (float)r[3]);
+      o[1] = make_float4((float)r[4], (float)r[5], (float)r[6], (float)r[7]);
+      o[2] = make_float4((float)r[8], (float)r[9], (float)r[10], (float)r[11]);
+      float2 *o2 = reinterpret_cast<float2 *>(a.cellrecf + slot * CR_N + 12);
+      o2[0] = make_float2((float)r[12], (float)r[13]);
+    } else {
+      double2 *o = reinterpret_cast<double2 *>(a.cellrec + slot * CR_N);
+#pragma unroll
+      for (int q = 0; q < 7; q++) o[q] = make_double2(r[2 * q], r[2 * q + 1]);
     }
   }
-  if (halo_plane) return;
   CPrim<double> q = cprim<double>(d.U_[0][c], d.U_[1][c], d.U_[2][c], d.U_[3][c], d.U_[4][c], J, d.e);
   double rho = q.rho, u = q.u, v = q.v, w = q.w, VV = q.VV, T = q.Tt, H = q.H, beta = q.beta;
   // Gamma^-1 of Dual_time_stepping.cpp:771-802; divisions by rho and by
@@ -100,9 +112,17 @@ __global__ void __launch_bounds__(64, CGLI_RESIDUAL_MINBLOCKS) k_residual_fast(D
   MR[2] = (d31 * Rk[0] + d22 * Rk[2]);
   MR[3] = (d41 * Rk[0] + d22 * Rk[3]);
   MR[4] = (d51 * Rk[0] + d52 * Rk[1] + d53 * Rk[2] + d54 * Rk[3] + d55 * Rk[4]);
-  for (int n = 0; n < 5; n++) {
-    if (MIXED) a.mrf[n][slot] = (float)MR[n];
-    else a.mrs[n][slot] = MR[n];
+  // MR after the record in the cell's contiguous block of CR_N words
+  if (MIXED) {
+    float2 *o2 = reinterpret_cast<float2 *>(a.cellrecf + slot * CR_N + CR_MR);
+    o2[0] = make_float2((float)MR[0], (float)MR[1]);
+    float4 *o = reinterpret_cast<float4 *>(a.cellrecf + slot * CR_N + 16);
+    o[0] = make_float4((float)MR[2], (float)MR[3], (float)MR[4], 0.f);
+  } else {
+    double2 *o = reinterpret_cast<double2 *>(a.cellrec + slot * CR_N + CR_MR);
+    o[0] = make_double2(MR[0], MR[1]);
+    o[1] = make_double2(MR[2], MR[3]);
+    o[2] = make_double2(MR[4], 0.0);
   }
   // the lagged halos of the first sweep; an open slab's stay zero
   if (!d.x_open && (i == ie || i == 3)) {

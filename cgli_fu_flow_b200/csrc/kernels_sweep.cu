@@ -37,6 +37,7 @@
 // T is the arithmetic type of the sweep (double, or float for CGLI_MIXED).
 #include "cgli_dev.cuh"
 #include "cgli_launch.h"
+#include "tc_sm100.cuh"
 
 // tiles per SM the wavefront kernel is compiled for (a register cap)
 #ifndef CGLI_SWEEP_MINBLOCKS
@@ -48,8 +49,7 @@ namespace cgli {
 template <typename T> struct SweepPtrs;
 template <> struct SweepPtrs<double> {
   __device__ __forceinline__ static double *const *dq(const SweepArgs &a) { return a.dq; }
-  __device__ __forceinline__ static double *const *mr(const SweepArgs &a) { return a.mrs; }
-  __device__ __forceinline__ static double *const *rec(const SweepArgs &a) { return a.rec; }
+  __device__ __forceinline__ static const double *cellrec(const SweepArgs &a) { return a.cellrec; }
   __device__ __forceinline__ static double *const *hf(const SweepArgs &a) { return a.halo_f; }
   __device__ __forceinline__ static double *const *hb(const SweepArgs &a) { return a.halo_b; }
   __device__ __forceinline__ static double *const *hrec(const SweepArgs &a, bool b) { return b ? a.hrec_b : a.hrec_f; }
@@ -59,8 +59,7 @@ template <> struct SweepPtrs<double> {
 };
 template <> struct SweepPtrs<float> {
   __device__ __forceinline__ static float *const *dq(const SweepArgs &a) { return a.dqf; }
-  __device__ __forceinline__ static float *const *mr(const SweepArgs &a) { return a.mrf; }
-  __device__ __forceinline__ static float *const *rec(const SweepArgs &a) { return a.recf; }
+  __device__ __forceinline__ static const float *cellrec(const SweepArgs &a) { return a.cellrecf; }
   __device__ __forceinline__ static float *const *hf(const SweepArgs &a) { return a.halo_ff; }
   __device__ __forceinline__ static float *const *hb(const SweepArgs &a) { return a.halo_bf; }
   __device__ __forceinline__ static float *const *hrec(const SweepArgs &a, bool b) { return b ? a.hrecf_b : a.hrecf_f; }
@@ -121,6 +120,51 @@ __device__ __forceinline__ void recv5(const T *src, T out[5], int *status, int l
   }
 }
 
+// REC_N record words and (mr non-null) the 5 MR words of one slot, through
+// the read-only path (CGLI_SWEEP_LDG) or plain loads
+#ifndef CGLI_SWEEP_LDG
+#define CGLI_SWEEP_LDG 0
+#endif
+__device__ __forceinline__ double2 ld_rec(const double2 *q) {
+#if CGLI_SWEEP_LDG
+  return __ldg(q);
+#else
+  return *q;
+#endif
+}
+__device__ __forceinline__ float4 ld_rec(const float4 *q) {
+#if CGLI_SWEEP_LDG
+  return __ldg(q);
+#else
+  return *q;
+#endif
+}
+__device__ __forceinline__ void load_cellrec(const double *p, double rec[REC_N], double *mr) {
+  const double2 *q = reinterpret_cast<const double2 *>(p);
+#pragma unroll
+  for (int t = 0; t < 7; t++) {
+    const double2 v = ld_rec(q + t);
+    rec[2 * t] = v.x;
+    rec[2 * t + 1] = v.y;
+  }
+  if (mr) {
+    const double2 a = ld_rec(q + 7), b = ld_rec(q + 8), c = ld_rec(q + 9);
+    mr[0] = a.x; mr[1] = a.y; mr[2] = b.x; mr[3] = b.y; mr[4] = c.x;
+  }
+}
+__device__ __forceinline__ void load_cellrec(const float *p, float rec[REC_N], float *mr) {
+  const float4 *q = reinterpret_cast<const float4 *>(p);
+  const float4 a = ld_rec(q), b = ld_rec(q + 1), c = ld_rec(q + 2), e = ld_rec(q + 3);
+  rec[0] = a.x; rec[1] = a.y; rec[2] = a.z; rec[3] = a.w;
+  rec[4] = b.x; rec[5] = b.y; rec[6] = b.z; rec[7] = b.w;
+  rec[8] = c.x; rec[9] = c.y; rec[10] = c.z; rec[11] = c.w;
+  rec[12] = e.x; rec[13] = e.y;
+  if (mr) {
+    const float4 f = ld_rec(q + 4);
+    mr[0] = e.z; mr[1] = e.w; mr[2] = f.x; mr[3] = f.y; mr[4] = f.z;
+  }
+}
+
 // one cell's sweep inputs
 template <typename T>
 struct Cell {
@@ -143,10 +187,11 @@ __device__ __forceinline__ void fetch_cell(const Dev &d, const SweepArgs &a, con
   const int sf = BACKWARD ? S - 1 - s : s;   // forward step of this cell
   const long long slot = tile_base + (long long)sf * (TI * TJ) + threadIdx.x;
   x.slot = slot;
+  // the record (and, forward, MR) arrive in shared memory with the CTA's
+  // block of the step (k_sweep); backward, this cell's forward result
+  if (BACKWARD)
 #pragma unroll
-  for (int v = 0; v < REC_N; v++) x.rec[v] = SweepPtrs<T>::rec(a)[v][slot];
-#pragma unroll
-  for (int v = 0; v < 5; v++) x.mr[v] = BACKWARD ? SweepPtrs<T>::dq(a)[v][slot] : SweepPtrs<T>::mr(a)[v][slot];
+    for (int v = 0; v < 5; v++) x.mr[v] = SweepPtrs<T>::dq(a)[v][slot];
   if (halo_edge) {
     // periodic lagged halo: the x neighbour's product, formed before the
     // pass (k_halo_products)
@@ -188,6 +233,12 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
   __shared__ T sy[2][TI][TJ][5];   // j-direction products
   __shared__ double s_jt[TJ], s_et[TJ];
   __shared__ int s_tile;
+  __shared__ __align__(8) uint64_t s_bar[2];
+  // the CTA's records of two steps: step s's TI*TJ slots are one contiguous
+  // block of TI*TJ*CR_N words in the tile-skewed layout, brought in with one
+  // bulk copy a step ahead
+  extern __shared__ __align__(128) unsigned char s_dyn[];
+  T *const s_rec = reinterpret_cast<T *>(s_dyn);
   const int il = threadIdx.x / TJ, jl = threadIdx.x % TJ;
   const int nti = (d.nx + TI - 1) / TI, ntj = (d.ny + TJ - 1) / TJ, ntiles = nti * ntj;
   if (threadIdx.x == 0) s_tile = (int)atomicAdd(a.ticket, 1u);
@@ -204,10 +255,25 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
     s_jt[threadIdx.x] = (Met::kChannel && jj <= jn) ? a.Jtab[jj] : 1.0;
     s_et[threadIdx.x] = (Met::kChannel && jj <= jn) ? a.etdytab[jj] : 0.0;
   }
+  if (threadIdx.x == 0) {
+    tc::mbar_init(tc::smem_addr(&s_bar[0]), 1);
+    tc::mbar_init(tc::smem_addr(&s_bar[1]), 1);
+    tc::mbar_fence_init();
+  }
   __syncthreads();
   const int Nz = d.nz;
   const int S = Nz + TI - 1 + TJ - 1;
   const long long tile_base = (long long)tile * S * (TI * TJ);
+  constexpr uint32_t kBlock = TI * TJ * CR_N * sizeof(T);
+  const T *const crec = SweepPtrs<T>::cellrec(a);
+  auto issue = [&](int step) {   // one thread
+    const int sf = BACKWARD ? S - 1 - step : step;
+    const uint32_t bar = tc::smem_addr(&s_bar[step & 1]);
+    tc::mbar_expect_tx(bar, kBlock);
+    tc::bulk_load(tc::smem_addr(s_rec + (step & 1) * (TI * TJ * CR_N)), crec + (tile_base + (long long)sf * (TI * TJ)) * CR_N,
+                  kBlock, bar);
+  };
+  if (threadIdx.x == 0) issue(0);
   const int pa = BACKWARD ? ta + 1 : ta - 1, pb = BACKWARD ? tb + 1 : tb - 1;
   const int tile_pa = pa * ntj + tb, tile_pb = ta * ntj + pb;
   const bool halo_edge = BACKWARD ? (i == ie) : (i == 3);
@@ -256,8 +322,13 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
     const int rel = BACKWARD ? s - (TI - 1 - il) - (TJ - 1 - jl) : s - il - jl;
     const int kl = BACKWARD ? Nz - 1 - rel : rel;
     // loads of the next cell go out first and land during the dependent part
+    if (threadIdx.x == 0 && s + 1 < S) issue(s + 1);   // buffer (s+1)&1 was last read before the previous barrier
     if (s + 1 < S) fetch_cell<TI, TJ, Met, BACKWARD, T>(d, a, s_et, il, jl, j, s + 1, S, tile_base, inside, halo_edge, nxt);
     else nxt.active = false;
+    // this step's records (bounded wait; a timeout is reported like a tile's)
+    if (!tc::mbar_wait(tc::smem_addr(&s_bar[s & 1]), (s >> 1) & 1, a.spin_limit)) atomicExch(d.status, CGLI_TIMEOUT_CODE);
+    if (cur.active)
+      load_cellrec(s_rec + (s & 1) * (TI * TJ * CR_N) + threadIdx.x * CR_N, cur.rec, BACKWARD ? (T *)nullptr : cur.mr);
     if (cur.active) {
       const int pbuf = (s - 1) & 1;
       T tx[5], ty[5];
@@ -428,10 +499,10 @@ static void run_sweeps(const Dev &d, const SweepArgs &a, cudaStream_t s) {
       const dim3 hg((d.nz + 63) / 64, d.ny);
       if (pass == 0) {
         k_halo_products<Met, false, T><<<hg, 64, 0, s>>>(d, f);
-        k_sweep<TI, TJ, Met, false, T><<<ntiles, TI * TJ, 0, s>>>(d, f);
+        k_sweep<TI, TJ, Met, false, T><<<ntiles, TI * TJ, 2 * TI * TJ * CR_N * sizeof(T), s>>>(d, f);
       } else {
         k_halo_products<Met, true, T><<<hg, 64, 0, s>>>(d, b);
-        k_sweep<TI, TJ, Met, true, T><<<ntiles, TI * TJ, 0, s>>>(d, b);
+        k_sweep<TI, TJ, Met, true, T><<<ntiles, TI * TJ, 2 * TI * TJ * CR_N * sizeof(T), s>>>(d, b);
       }
     }
   }
@@ -451,10 +522,10 @@ static void run_one_pass(const Dev &d, const SweepArgs &a, cudaStream_t s, bool 
   const dim3 hg((d.nz + 63) / 64, d.ny);
   if (!backward) {
     k_halo_products<Met, false, T><<<hg, 64, 0, s>>>(d, b);
-    k_sweep<TI, TJ, Met, false, T><<<ntiles, TI * TJ, 0, s>>>(d, b);
+    k_sweep<TI, TJ, Met, false, T><<<ntiles, TI * TJ, 2 * TI * TJ * CR_N * sizeof(T), s>>>(d, b);
   } else {
     k_halo_products<Met, true, T><<<hg, 64, 0, s>>>(d, b);
-    k_sweep<TI, TJ, Met, true, T><<<ntiles, TI * TJ, 0, s>>>(d, b);
+    k_sweep<TI, TJ, Met, true, T><<<ntiles, TI * TJ, 2 * TI * TJ * CR_N * sizeof(T), s>>>(d, b);
   }
   if (final_pass) k_update_skewed<T><<<dim3(d.ny, d.nx), 128, 0, s>>>(d, a);
 }
@@ -467,6 +538,25 @@ void launch_sweep_pass(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mi
     if (a.channel_metrics) run_one_pass<SWEEP_TI, SWEEP_TJ, MetricsChannel, double>(d, a, s, backward, final_pass);
     else run_one_pass<SWEEP_TI, SWEEP_TJ, MetricsGeneral, double>(d, a, s, backward, final_pass);
   }
+}
+
+// the wavefront kernels' shared memory (static products plus the dynamic
+// two-step record buffer) exceeds 48 KB: opt in once, outside any capture
+template <class Met, typename T>
+static cudaError_t opt_in() {
+  const int dyn = 2 * SWEEP_TI * SWEEP_TJ * CR_N * sizeof(T);   // two steps' records
+  cudaError_t e = cudaFuncSetAttribute(k_sweep<SWEEP_TI, SWEEP_TJ, Met, false, T>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_sweep<SWEEP_TI, SWEEP_TJ, Met, true, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+  return e;
+}
+cudaError_t sweep_kernel_attributes() {
+  cudaError_t e = opt_in<MetricsChannel, double>();
+  if (e == cudaSuccess) e = opt_in<MetricsGeneral, double>();
+  if (e == cudaSuccess) e = opt_in<MetricsChannel, float>();
+  if (e == cudaSuccess) e = opt_in<MetricsGeneral, float>();
+  return e;
 }
 
 void launch_sweeps(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed) {
