@@ -237,6 +237,8 @@ int check_channel_metrics(cgli_ctx *c) {
     CUDA_TRY(cudaMemcpy((void *)c->sw.etdytab, et.data(), sizeof(double) * d.Y, cudaMemcpyHostToDevice));
   }
   c->sw.channel_metrics = ok ? 1 : 0;
+  c->d.face_tables = 0;
+  c->d.face_tables = cgli::check_face_tables(c->d, c->d.status + 8, c->stream) ? 1 : 0;
   cgli::launch_inverse_j(d, c->stream);
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   c->metrics_checked = true;
@@ -305,6 +307,7 @@ int cgli_create(const cgli_params *p, cgli_ctx **out) {
   if (rc == CGLI_OK) rc = alloc(c, 16 * sizeof(double), (void **)&d.scal);
   if (rc == CGLI_OK) rc = alloc(c, (8 + 296) * sizeof(double), (void **)&c->d_out);
   if (rc == CGLI_OK) rc = alloc(c, 16 * sizeof(int), (void **)&d.status);
+  if (rc == CGLI_OK) rc = alloc(c, 3 * 2 * sizeof(double) * d.Y, (void **)&d.ftab);
   c->update_blocks = p->nx * p->ny;
   // relaxation tile shape of the DP-LUR solver (tuning; defaults 6 rows, 32 planes)
   if (const char *ev = getenv("CGLI_DPLUR_TILE_ROWS")) cgli::dplur_tile_rows = atoi(ev) == 14 ? 14 : 6;

@@ -32,6 +32,11 @@ struct Dev {
   double *J, *m[9];
   double *iJ;             // 1/J per cell (0 where J = 0), formed when the metrics change
   double *Jf[3], *mf[3][9];
+  // per-row face metrics [3 sets][Y][etdy, J], used when face_tables is set:
+  // every face of each set has the channel's form xi = (1,0,0),
+  // eta = (0,etdy(row),0), zeta = (0,0,1) with J a function of the row
+  double *ftab;
+  int face_tables;
   double *inF[3][5], *vF[4];
   double *MR[5], *NL[5], *NR[5];
   double *vflux[3][4];
@@ -45,6 +50,21 @@ struct Dev {
 
 __host__ __device__ __forceinline__ long long ix(const Dev &d, int i, int j, int k) {
   return (long long)i * d.di + (long long)j * d.dj + k;
+}
+
+// the nine metric terms and J of face set `set` (0 x, 1 y, 2 z faces) at
+// face index f, whose row index is jj: from the per-row tables when the
+// face metrics have the channel's form, else from the 3-D face arrays
+__device__ __forceinline__ void face_metrics(const Dev &d, int set, long long f, int jj, double mm[9], double &Jf) {
+  if (d.face_tables) {
+    const double *t = d.ftab + ((long long)set * d.Y + jj) * 2;
+    mm[0] = 1; mm[1] = 0; mm[2] = 0; mm[3] = 0; mm[4] = t[0]; mm[5] = 0; mm[6] = 0; mm[7] = 0; mm[8] = 1;
+    Jf = t[1];
+  } else {
+#pragma unroll
+    for (int v = 0; v < 9; v++) mm[v] = d.mf[set][v][f];
+    Jf = d.Jf[set][f];
+  }
 }
 
 // ---------------------------------------------------------------- MUSCL

@@ -91,6 +91,9 @@ void launch_statistics(const Dev &d, cudaStream_t s, double *sums);
 void launch_inverse_j(const Dev &d, cudaStream_t s);
 // main.cpp:167-210: x halo (periodic slab only), Y, X (open slab only), Z
 void launch_halo_bc(const Dev &d, cudaStream_t s);
+// true (and d.ftab filled) when every face metric has the channel's form
+// with a per-row etdy and J; dflag: one device int of scratch
+bool check_face_tables(const Dev &d, int *dflag, cudaStream_t s);
 // X_boundary_condition.cpp on an open slab (no-op on a periodic one)
 void launch_bc_x(const Dev &d, cudaStream_t s);
 // outlet sponge target velocity into d.scal[1] (open slab with an outlet layer)

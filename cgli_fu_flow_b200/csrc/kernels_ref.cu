@@ -168,6 +168,31 @@ __global__ void k_bc_x(Dev d) {
                                     dm[v][4] * KAL[4]);
 }
 
+// Clears *ok if some face of set `set` in the ranges the face generator
+// fills (x: i 2..ie, rows 1..jn-1, k 1..kn-1; y: i 2..ie-1, rows 1..jn,
+// k 1..kn-1; z: i 2..ie-1, rows 1..jn-1, k 1..kn) is not of the channel's
+// form with the etdy and J of its row's face (2, row, 1)
+__global__ void k_check_face_set(Dev d, int set, int i1, int j1, int k1, int *ok) {
+  const int k = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 1 + blockIdx.y, i = 2 + blockIdx.z;
+  if (k > k1 || j > j1 || i > i1) return;
+  const long long f = ix(d, i, j, k), r = ix(d, 2, j, 1);
+  const double *const *m = d.mf[set];
+  const bool good = m[0][f] == 1.0 && m[1][f] == 0.0 && m[2][f] == 0.0 && m[3][f] == 0.0 && m[5][f] == 0.0 &&
+                    m[6][f] == 0.0 && m[7][f] == 0.0 && m[8][f] == 1.0 && m[4][f] == m[4][r] &&
+                    d.Jf[set][f] == d.Jf[set][r];
+  if (!good) atomicExch(ok, 0);
+}
+__global__ void k_fill_face_tables(Dev d) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= d.Y) return;
+  for (int set = 0; set < 3; set++) {
+    const long long r = ix(d, 2, j, 1);
+    d.ftab[((long long)set * d.Y + j) * 2] = d.mf[set][4][r];
+    d.ftab[((long long)set * d.Y + j) * 2 + 1] = d.Jf[set][r];
+  }
+}
+
 // outlet sponge target velocity, Dual_time_stepping.cpp:510-532: the sum
 // over plane 3, rows j = 2..Ny+2, k = 2..Nz+2, of u deltaET / etdy deltaZT,
 // over high deltaZT Nz; one block, into d.scal[1]
@@ -210,7 +235,9 @@ __global__ void __launch_bounds__(64, CGLI_FLUX_MINBLOCKS) k_flux_x(Dev d) {
     side5L(d, c - 2 * di, di, L);
     side5R(d, c - di, di, R);
   }
-  roe_face(L, R, d.mf[0][0][f], d.mf[0][1][f], d.mf[0][2][f], d.Jf[0][f], d.e, F, fav3, pp);
+  double mm[9], Jf;
+  face_metrics(d, 0, f, j, mm, Jf);
+  roe_face(L, R, mm[0], mm[1], mm[2], Jf, d.e, F, fav3, pp);
   for (int v = 0; v < 5; v++) d.inF[0][v][f] = F[v];
 }
 
@@ -242,15 +269,17 @@ __global__ void __launch_bounds__(64, CGLI_FLUX_MINBLOCKS) k_flux_y(Dev d) {
   long long f = ix(d, i, j, k);
   double L[5], R[5], F[5], fav3, pp;
   muscl_y(d, i + 1, j, k + 1, L, R);
-  double ety = d.mf[1][4][f], Jf = d.Jf[1][f];
-  roe_face(L, R, d.mf[1][3][f], ety, d.mf[1][5][f], Jf, d.e, F, fav3, pp);
+  double mm[9], Jf;
+  face_metrics(d, 1, f, j, mm, Jf);
+  const double ety = mm[4];
+  roe_face(L, R, mm[3], ety, mm[5], Jf, d.e, F, fav3, pp);
   if (j == 1 || j == jn) {
     F[0] = 0; F[1] = 0; F[3] = 0; F[4] = 0;
     F[2] = 0.5 * (ety * pp - 1. * fav3) / Jf;
     if (d.curved_walls) {
       // a curved wall also carries the x and z pressure force
-      F[1] = 0.5 * (d.mf[1][3][f] * pp) / Jf;
-      F[3] = 0.5 * (d.mf[1][5][f] * pp) / Jf;
+      F[1] = 0.5 * (mm[3] * pp) / Jf;
+      F[3] = 0.5 * (mm[5] * pp) / Jf;
     }
   }
   for (int v = 0; v < 5; v++) d.inF[1][v][f] = F[v];
@@ -279,7 +308,9 @@ __global__ void __launch_bounds__(64, CGLI_FLUX_MINBLOCKS) k_flux_z(Dev d) {
   long long f = ix(d, i, j, k);
   double L[5], R[5], F[5], fav3, pp;
   muscl_z(d, i + 1, j + 1, k, L, R);
-  roe_face(L, R, d.mf[2][6][f], d.mf[2][7][f], d.mf[2][8][f], d.Jf[2][f], d.e, F, fav3, pp);
+  double mm[9], Jf;
+  face_metrics(d, 2, f, j, mm, Jf);
+  roe_face(L, R, mm[6], mm[7], mm[8], Jf, d.e, F, fav3, pp);
   for (int v = 0; v < 5; v++) d.inF[2][v][f] = F[v];
 }
 
@@ -319,27 +350,27 @@ __global__ void __launch_bounds__(64, CGLI_VISCOUS_MINBLOCKS) k_viscous_faces(De
   VP o = vp(d, c);
   if (j <= jn && k <= kn) {
     double out[4];
-    double mm[9];
-    for (int v = 0; v < 9; v++) mm[v] = d.mf[0][v][f];
+    double mm[9], Jf;
+    face_metrics(d, 0, f, j - 1, mm, Jf);
     visc_face_x(d.dxi, d.det, d.dzt, d.mu, d.pr, o, vp(d, c - di), vp(d, c + dj), vp(d, c - di + dj), vp(d, c - dj), vp(d, c - di - dj),
-                vp(d, c + 1), vp(d, c - di + 1), vp(d, c - 1), vp(d, c - di - 1), mm, d.Jf[0][f], out);
+                vp(d, c + 1), vp(d, c - di + 1), vp(d, c - 1), vp(d, c - di - 1), mm, Jf, out);
     for (int v = 0; v < 4; v++) d.vflux[0][v][c] = out[v];
   }
   if (i <= ie && k <= kn) {
     double out[4];
-    double mm[9];
-    for (int v = 0; v < 9; v++) mm[v] = d.mf[1][v][f];
+    double mm[9], Jf;
+    face_metrics(d, 1, f, j - 1, mm, Jf);
     visc_face_y(d.dxi, d.det, d.dzt, d.mu, d.pr, o, vp(d, c - dj), vp(d, c + di), vp(d, c + di - dj), vp(d, c - di), vp(d, c - di - dj),
-                vp(d, c + 1), vp(d, c - dj + 1), vp(d, c - 1), vp(d, c - dj - 1), mm, d.Jf[1][f], out);
+                vp(d, c + 1), vp(d, c - dj + 1), vp(d, c - 1), vp(d, c - dj - 1), mm, Jf, out);
     for (int v = 0; v < 4; v++) d.vflux[1][v][c] = out[v];
   }
   if (i <= ie && j <= jn) {
     double out[4];
-    double mm[9];
-    for (int v = 0; v < 9; v++) mm[v] = d.mf[2][v][f];
+    double mm[9], Jf;
+    face_metrics(d, 2, f, j - 1, mm, Jf);
     visc_face_z(d.dxi, d.det, d.dzt, d.mu, d.pr, o, vp(d, c - 1), vp(d, c + di), vp(d, c + di - 1), vp(d, c - di), vp(d, c - di - 1),
                 vp(d, c + dj), vp(d, c + dj - 1), vp(d, c - dj), vp(d, c - dj - 1), vp(d, c - di + dj),
-                mm, d.Jf[2][f], out);
+                mm, Jf, out);
     for (int v = 0; v < 4; v++) d.vflux[2][v][c] = out[v];
   }
 }
@@ -557,6 +588,21 @@ void launch_bc_x(const Dev &d, cudaStream_t s) {
   if (!d.x_open) return;   // interior rank: no-op
   k_bc_x<<<dim3((d.nz + 63) / 64, d.ny, 2), 64, 0, s>>>(d);
 }
+bool check_face_tables(const Dev &d, int *dflag, cudaStream_t s) {
+  const int ie = d.nx + 2, jn = d.ny + 1, kn = d.nz + 1;
+  const int one = 1;
+  if (cudaMemcpyAsync(dflag, &one, sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess) return false;
+  const int rng[3][3] = {{ie, jn - 1, kn - 1}, {ie - 1, jn, kn - 1}, {ie - 1, jn - 1, kn}};
+  for (int set = 0; set < 3; set++)
+    k_check_face_set<<<dim3((rng[set][2] + 127) / 128, rng[set][1], rng[set][0] - 1), 128, 0, s>>>(
+        d, set, rng[set][0], rng[set][1], rng[set][2], dflag);
+  int ok = 0;
+  if (cudaMemcpyAsync(&ok, dflag, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess) return false;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return false;
+  if (ok) k_fill_face_tables<<<(d.Y + 127) / 128, 128, 0, s>>>(d);
+  return ok != 0;
+}
+
 void launch_target_u(const Dev &d, cudaStream_t s) {
   if (!d.x_open || d.nx_outlet == 0) return;
   k_target_u<<<1, 256, 0, s>>>(d);
