@@ -227,6 +227,30 @@ __global__ void k_halo_products(Dev d, SweepArgs a) {
   for (int v = 0; v < 5; v++) SweepPtrs<T>::hxp(a)[v][h] = o[v];
 }
 
+// The split products of one direction for a face metric with a single
+// nonzero component m on momentum component q = DIR + 1 (the channel grid:
+// xi = (1,0,0), eta = (0,etdy,0), zeta = (0,0,1)): lower_terms / upper_terms
+// of split_from_record with the zero entries left out.
+template <typename T, int DIR, bool BACKWARD>
+__device__ __forceinline__ void channel_products(const T r[REC_N], T m, const T n[5], T o[5]) {
+  constexpr int q = DIR + 1;
+  const T U = r[R_UX + DIR], lam = r[R_LX + DIR], beta = r[R_BETA];
+  const T p1q = r[R_H] * m, pq1 = r[R_HR] * m, p5q = r[R_HBT] * m, p51 = r[R_G] * U;
+  if (!BACKWARD) {
+    const T p11 = (T)0.5 * (beta * U + lam), p22 = (T)0.5 * (U + lam);
+    o[0] = -p11 * n[0] - p1q * n[q];
+#pragma unroll
+    for (int v = 1; v <= 3; v++) o[v] = v == q ? -pq1 * n[0] - p22 * n[v] : -p22 * n[v];
+    o[4] = -p51 * n[0] - p5q * n[q] - p22 * n[4];
+  } else {
+    const T m11 = (T)0.5 * (beta * U - lam), m22 = (T)0.5 * (U - lam);
+    o[0] = +m11 * n[0] + p1q * n[q];
+#pragma unroll
+    for (int v = 1; v <= 3; v++) o[v] = v == q ? +pq1 * n[0] + m22 * n[v] : m22 * n[v];
+    o[4] = +p51 * n[0] + p5q * n[q] + m22 * n[4];
+  }
+}
+
 template <int TI, int TJ, class Met, bool BACKWARD, typename T>
 __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, SweepArgs a) {
   __shared__ T sx[2][TI][TJ][5];   // i-direction products, double-buffered by step parity
@@ -384,7 +408,14 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
       T mm[9];
       Met::template dirs<T>(d, s_et, c, jl, mm);
       T ox[5], oy[5];
-      {
+      if (Met::kChannel) {
+        // the channel's face metrics have one nonzero component per
+        // direction (1, etdy, 1 on the x, y, z components), so only the
+        // nonzero split entries are formed and applied
+        channel_products<T, 0, BACKWARD>(cur.rec, (T)1, n, ox);
+        channel_products<T, 1, BACKWARD>(cur.rec, mm[4], n, oy);
+        channel_products<T, 2, BACKWARD>(cur.rec, (T)1, n, carry_z);
+      } else {
         Split<T> Ax = split_from_record<T>(cur.rec, 0, mm[0], mm[1], mm[2]);
         Split<T> Ay = split_from_record<T>(cur.rec, 1, mm[3], mm[4], mm[5]);
         Split<T> Az = split_from_record<T>(cur.rec, 2, mm[6], mm[7], mm[8]);
