@@ -67,6 +67,9 @@ struct cgli_ctx {
   int history = 0;                    // completed steps since the state was set
   int predictor = 0;                  // 0 previous level, 1 extrapolation, 2 learned
   int inner_solver = CGLI_LUSGS;      // CGLI_LUSGS or CGLI_DPLUR
+  cudaEvent_t sweep_ev[2] = {};       // recorded around the wavefront passes inside the iteration graph
+  double sweep_ms = 0;                // their accumulated device time since the last reset
+  long long sweep_passes = 0;
   cgli_cnn *cnn = nullptr;            // learned initial guess (not owned)
   std::vector<double> step_norms;     // the five norms of every inner iteration of the last step
   double *stats = nullptr;            // [11][nx][ny] running sums (allocated on first use)
@@ -383,6 +386,8 @@ int cgli_create(const cgli_params *p, cgli_ctx **out) {
   }
   for (auto &e : c->events)
     if (rc == CGLI_OK && cudaEventCreate(&e) != cudaSuccess) rc = fail(CGLI_ECUDA, "cudaEventCreate");
+  for (auto &e : c->sweep_ev)
+    if (rc == CGLI_OK && cudaEventCreate(&e) != cudaSuccess) rc = fail(CGLI_ECUDA, "cudaEventCreate");
   if (rc != CGLI_OK) {
     std::string keep = g_err;
     cgli_destroy(c);
@@ -402,6 +407,8 @@ int cgli_destroy(cgli_ctx *c) {
   if (c->iter_graph) cudaGraphExecDestroy(c->iter_graph);
   if (c->dts_graph) cudaGraphExecDestroy(c->dts_graph);
   for (auto &e : c->events)
+    if (e) cudaEventDestroy(e);
+  for (auto &e : c->sweep_ev)
     if (e) cudaEventDestroy(e);
   for (void *p : c->allocs) cudaFree(p);
   if (c->h_norms) cudaFreeHost(c->h_norms);
@@ -736,8 +743,18 @@ int cgli_inner_iteration(cgli_ctx *c, double er[5]) {
   if (!c->iter_graph) {
     cudaGraph_t g;
     CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    if (dplur) cgli::launch_dplur_iteration(c->d, c->sw, c->stream);
-    else cgli::launch_fused_iteration(c->d, c->sw, c->stream, c->p.precision);
+    if (dplur) {
+      cgli::launch_dplur_iteration(c->d, c->sw, c->stream);
+    } else {
+      // the four wavefront passes are bracketed by two events, so that their
+      // device time is known for every iteration the graph runs
+      cgli::launch_fused_residual(c->d, c->sw, c->stream, c->p.precision);
+      // (external records: event-record nodes of the graph, not capture-internal dependencies)
+      cudaEventRecordWithFlags(c->sweep_ev[0], c->stream, cudaEventRecordExternal);
+      cgli::launch_sweeps(c->d, c->sw, c->stream, c->p.precision == CGLI_MIXED);
+      cudaEventRecordWithFlags(c->sweep_ev[1], c->stream, cudaEventRecordExternal);
+      cgli::launch_sweep_update(c->d, c->sw, c->stream, c->p.precision == CGLI_MIXED);
+    }
     cudaError_t e = cudaStreamEndCapture(c->stream, &g);
     if (e != cudaSuccess) return fail(CGLI_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
     e = cudaGraphInstantiate(&c->iter_graph, g, 0);
@@ -745,7 +762,17 @@ int cgli_inner_iteration(cgli_ctx *c, double er[5]) {
     if (e != cudaSuccess) return fail(CGLI_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
   }
   CUDA_TRY(cudaGraphLaunch(c->iter_graph, c->stream));
-  return read_norms(c, er, c->update_blocks);
+  rc = read_norms(c, er, c->update_blocks);   // synchronises the stream
+  if (rc == CGLI_OK && !dplur) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, c->sweep_ev[0], c->sweep_ev[1]) == cudaSuccess) {
+      c->sweep_ms += ms;
+      c->sweep_passes += 4;
+    } else {
+      cudaGetLastError();   // timing unavailable: leave no error behind for the next call
+    }
+  }
+  return rc;
 }
 
 int cgli_driven_force(cgli_ctx *c, double *bulk_flux) {
@@ -947,6 +974,15 @@ int cgli_event_record(cgli_ctx *c, int slot) {
   int rc = check(c); if (rc) return rc;
   if (slot < 0 || slot >= 8) return fail(CGLI_EINVAL, "event slot out of range");
   CUDA_TRY(cudaEventRecord(c->events[slot], c->stream));
+  return CGLI_OK;
+}
+
+int cgli_sweep_time(cgli_ctx *c, double *ms, long long *passes, int reset) {
+  int rc = check(c); if (rc) return rc;
+  if (!ms || !passes) return fail(CGLI_EINVAL, "null argument");
+  *ms = c->sweep_ms;
+  *passes = c->sweep_passes;
+  if (reset) { c->sweep_ms = 0; c->sweep_passes = 0; }
   return CGLI_OK;
 }
 

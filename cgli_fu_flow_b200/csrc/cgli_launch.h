@@ -63,7 +63,12 @@ __host__ __device__ __forceinline__ long long skew_size(const Dev &d) {
 void sweep_tile_order(int nti, int ntj, std::vector<int> &order);
 // shared-memory opt-in of the wavefront kernels (once per process and device)
 cudaError_t sweep_kernel_attributes();
+// the four wavefront passes (two sweeps) of one inner iteration
 void launch_sweeps(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed);
+// the update and norm partials after the last pass (k_update_skewed)
+void launch_sweep_update(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed);
+// everything of a fused inner iteration before the sweeps
+void launch_fused_residual(const Dev &d, const SweepArgs &a, cudaStream_t s, int precision);
 // one pass (forward / backward, final with the update) of the sweeps
 void launch_sweep_pass(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed, bool backward, bool final_pass);
 // Dual_time_stepping.cpp:737-922 residual on the natural layout: MR and

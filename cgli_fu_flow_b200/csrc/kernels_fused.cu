@@ -154,16 +154,20 @@ void launch_residual_fast(const Dev &d, const SweepArgs &a, cudaStream_t s, bool
   }
 }
 
-void launch_fused_iteration(const Dev &d, const SweepArgs &a, cudaStream_t s, int precision) {
+void launch_fused_residual(const Dev &d, const SweepArgs &a, cudaStream_t s, int precision) {
   launch_halo_bc(d, s);
   launch_flux_x(d, s);
   launch_flux_y(d, s);
   launch_flux_z(d, s);
   launch_viscous(d, s);
   launch_target_u(d, s);
-  const bool mixed = precision == 1;
-  launch_residual_fast(d, a, s, mixed);
-  launch_sweeps(d, a, s, mixed);
+  launch_residual_fast(d, a, s, precision == 1);
+}
+
+void launch_fused_iteration(const Dev &d, const SweepArgs &a, cudaStream_t s, int precision) {
+  launch_fused_residual(d, a, s, precision);
+  launch_sweeps(d, a, s, precision == 1);
+  launch_sweep_update(d, a, s, precision == 1);
 }
 
 }  // namespace cgli

@@ -537,7 +537,6 @@ static void run_sweeps(const Dev &d, const SweepArgs &a, cudaStream_t s) {
       }
     }
   }
-  k_update_skewed<T><<<dim3(d.ny, d.nx), 128, 0, s>>>(d, a);
 }
 
 template <int TI, int TJ, class Met, typename T>
@@ -588,6 +587,11 @@ cudaError_t sweep_kernel_attributes() {
   if (e == cudaSuccess) e = opt_in<MetricsChannel, float>();
   if (e == cudaSuccess) e = opt_in<MetricsGeneral, float>();
   return e;
+}
+
+void launch_sweep_update(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed) {
+  if (mixed) k_update_skewed<float><<<dim3(d.ny, d.nx), 128, 0, s>>>(d, a);
+  else k_update_skewed<double><<<dim3(d.ny, d.nx), 128, 0, s>>>(d, a);
 }
 
 void launch_sweeps(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed) {

@@ -36,10 +36,11 @@ def hbm_peak() -> tuple[float, str]:
         return 6650.0, "fallback"
 
 
-def sweep_roofline(ch, stage_ms: dict, precision: str) -> dict:
+def sweep_roofline(ch, pass_ms: float, precision: str) -> dict:
+    """pass_ms: mean device time of one wavefront pass."""
     cells = ch.cells
     bpc = SWEEP_BYTES_PER_CELL[precision]
-    dur_ms = 0.5 * (stage_ms["sweep_forward"] + stage_ms["sweep_backward"])
+    dur_ms = pass_ms
     achieved = bpc * cells / (dur_ms / 1e3) / 1e9
     peak, kind = hbm_peak()
     tpc = MEASURED_TRAFFIC_PER_CELL.get(precision)

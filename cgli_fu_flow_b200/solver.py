@@ -57,6 +57,7 @@ EXPORTS = [
     "cgli_statistics_accumulate", "cgli_statistics_get", "cgli_statistics_reset",
     "cgli_write_restart", "cgli_read_restart", "cgli_write_history", "cgli_read_history",
     "cgli_dplusgs", "cgli_set_inner_solver", "cgli_x_boundary_condition", "cgli_set_levels",
+    "cgli_sweep_time",
 ]
 
 INNER_SOLVERS = {"lusgs": 0, "dplur": 1}
@@ -86,6 +87,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cgli_set_state.argtypes = [P, P, P, P]
     L.cgli_get_state.argtypes = [P, P]
     L.cgli_set_levels.argtypes = [P, P, P]
+    L.cgli_sweep_time.argtypes = [P, DP, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
     for n in ("cgli_halo_x", "cgli_y_boundary_condition", "cgli_z_boundary_condition", "cgli_flux_x",
               "cgli_flux_y", "cgli_flux_z", "cgli_viscous_terms", "cgli_end_step"):
         getattr(L, n).argtypes = [P]
@@ -308,6 +310,14 @@ class Solver:
     def event(self, slot: int) -> None:
         """Records CUDA event `slot` on the context's stream."""
         self._rc(self.L.cgli_event_record(self.h, slot))
+
+    def sweep_time(self, reset: bool = False) -> tuple[float, int]:
+        """(ms, passes): device time of the wavefront passes of every inner
+        iteration since the last reset (events inside the iteration graph)."""
+        ms = ctypes.c_double()
+        n = ctypes.c_longlong()
+        self._rc(self.L.cgli_sweep_time(self.h, ctypes.byref(ms), ctypes.byref(n), int(reset)))
+        return ms.value, n.value
 
     def elapsed_ms(self, a: int, b: int) -> float:
         ms = ctypes.c_float()

@@ -285,6 +285,11 @@ int cgli_filter(cgli_ctx *ctx, double roe_criterion, double e_high, double e_low
  * read the milliseconds between two recorded slots (synchronises on b). */
 int cgli_event_record(cgli_ctx *ctx, int slot);
 int cgli_event_elapsed(cgli_ctx *ctx, int a, int b, float *ms);
+/* Device time of the wavefront passes (LU-SGS) of every inner iteration run
+ * through cgli_inner_iteration / cgli_step since the last reset, from two
+ * events recorded around them inside the iteration graph: total ms and the
+ * number of passes (4 per inner iteration); reset != 0 clears the totals. */
+int cgli_sweep_time(cgli_ctx *ctx, double *ms, long long *passes, int reset);
 
 /* Stage timing of one inner iteration of the fast path, each stage launched
  * on its own between CUDA events on the context stream, `reps` times; writes

@@ -347,3 +347,16 @@ def test_host_driven_loop_with_set_levels_matches_resident_run(lib):
         qm, qn = qn, out.copy()
     sl = (slice(None), slice(3, ch.nx + 3), slice(2, ch.ny + 2), slice(2, ch.nz + 2))
     assert np.array_equal(a.q()[sl], b.q()[sl])
+
+
+def test_sweep_time_counts_the_passes_of_every_iteration(lib):
+    """cgli_sweep_time: events inside the iteration graph time the four
+    wavefront passes of every inner iteration; reset clears the totals."""
+    from cgli_fu_flow_b200.solver import Solver
+    g = Solver(Channel(16, 12, 8))
+    g.init()
+    g.sweep_time(reset=True)
+    it, _ = g.step(None, drop=1e-2, cap=6)
+    ms, passes = g.sweep_time(reset=True)
+    assert passes == 4 * it and ms > 0
+    assert g.sweep_time() == (0.0, 0)
