@@ -14,6 +14,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libcgli_fu_flow.so")
+DRIVER = os.path.join(HERE, "cgli_run")                 # the C++ host driver (csrc/driver)
+DRIVER_SRC = os.path.join(HERE, "csrc", "driver", "cgli_run.cpp")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
@@ -29,8 +31,20 @@ def deps() -> list[str]:
         [os.path.join(REPO, "include", "cgli_fu_flow.h"), os.path.abspath(__file__)]
 
 
+def build_driver(force: bool = False) -> str:
+    """The C++ host driver (main.cpp's step loop on the C ABI), linked
+    against the in-tree library with an $ORIGIN run path."""
+    if not force and os.path.exists(DRIVER) and all(
+            os.path.getmtime(d) <= os.path.getmtime(DRIVER) for d in (DRIVER_SRC, LIB)):
+        return DRIVER
+    subprocess.run(["g++", "-O2", "-std=c++17", "-Wall", "-I", os.path.join(REPO, "include"), DRIVER_SRC,
+                    "-L", HERE, "-lcgli_fu_flow", "-Wl,-rpath,$ORIGIN", "-o", DRIVER], check=True)
+    return DRIVER
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and os.path.exists(LIB) and all(os.path.getmtime(d) <= os.path.getmtime(LIB) for d in deps()):
+        build_driver()
         return LIB
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
@@ -53,6 +67,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if failed:
         raise RuntimeError("nvcc failed")
     subprocess.run([NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"], check=True)
+    build_driver(force=True)
     return LIB
 
 
