@@ -150,8 +150,10 @@ __device__ __forceinline__ void roe_face(const double L[5], const double R[5], d
                                          double mz, double Jf, double e, double F[5], double &Fav3o,
                                          double &ppo) {
   // The reference's statements in its order; each group of divisions by one
-  // denominator is one reciprocal and products (results differ from the
-  // reference's in the last bits only).
+  // denominator is one reciprocal and products, and the divisions by the
+  // constant gamma - 1 are products with its reciprocal (results differ from
+  // the reference's in the last bits only).
+  constexpr double rkg = 1.0 / (KG - 1);
   const double sq = sqrt(mx * mx + my * my + mz * mz);
   const double insqr = 1.0 / sq;
   const double NX = mx * insqr, NY = my * insqr, NZ = mz * insqr;
@@ -161,14 +163,14 @@ __device__ __forceinline__ void roe_face(const double L[5], const double R[5], d
   const double _VV = _u * _u + _v * _v + _w * _w;
   const double iP = (L[4] - 0.5 * _rho * _VV) * (KG - 1);
   const double iC = KG * iP * irl;
-  const double _H = 0.5 * _VV + iC / (KG - 1);
+  const double _H = 0.5 * _VV + iC * rkg;
   const double rho_ = R[0], irr = 1.0 / rho_;
   const double u_ = R[1] * irr, v_ = R[2] * irr, w_ = R[3] * irr;
   const double U_ = mx * u_ + my * v_ + mz * w_;
   const double VV_ = u_ * u_ + v_ * v_ + w_ * w_;
   const double P_ = (R[4] - 0.5 * rho_ * VV_) * (KG - 1);
   const double C_ = KG * P_ * irr;
-  const double H_ = 0.5 * VV_ + C_ / (KG - 1);
+  const double H_ = 0.5 * VV_ + C_ * rkg;
   const double temp5 = sqrt(_rho), temp6 = sqrt(rho_);
   const double i4 = 1.0 / (temp5 + temp6);
   const double rho = sqrt(_rho * rho_);
@@ -184,7 +186,7 @@ __device__ __forceinline__ void roe_face(const double L[5], const double R[5], d
   const double dU2 = rho_ * u_ - _rho * _u;
   const double dU3 = rho_ * v_ - _rho * _v;
   const double dU4 = rho_ * w_ - _rho * _w;
-  const double dU5 = (P_ / (KG - 1) + 0.5 * rho_ * VV_) - (iP / (KG - 1) + 0.5 * _rho * _VV);
+  const double dU5 = (P_ * rkg + 0.5 * rho_ * VV_) - (iP * rkg + 0.5 * _rho * _VV);
   const double theda_p = VV * iCc;
   const double beta = theda_p > e ? theda_p : e;   // max() macro semantics
   const double Un = U * insqr;
