@@ -75,17 +75,27 @@ def parse():
 
 # --------------------------------------------------------------- plumbing
 class Dist:
-    def __init__(self):
+    """One process per GPU (RANK / LOCAL_RANK / WORLD_SIZE from the launcher).
+    The replicas share no data; the process group only carries the barriers
+    around the timed region and the max / sum of the timings.  backend
+    "nccl" on GPUs; "gloo" (CPU tensors) runs the same plumbing without a
+    GPU, as the tests do."""
+
+    def __init__(self, backend: str = "nccl", timeout_s: float = 120.0):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.dist = None
+        self.device = "cuda" if backend == "nccl" else "cpu"
         if self.world > 1:
             import datetime
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+            # a short timeout: a rank that never arrives ends the others'
+            # next collective with an error instead of a hang
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
             self.dist = dist
             self.torch = torch
 
@@ -96,20 +106,29 @@ class Dist:
     def max(self, x: float) -> float:
         if not self.dist:
             return x
-        t = self.torch.tensor([x], dtype=self.torch.float64, device="cuda")
+        t = self.torch.tensor([x], dtype=self.torch.float64, device=self.device)
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
         return float(t.item())
 
     def sum(self, x: float) -> float:
         if not self.dist:
             return x
-        t = self.torch.tensor([x], dtype=self.torch.float64, device="cuda")
+        t = self.torch.tensor([x], dtype=self.torch.float64, device=self.device)
         self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
         return float(t.item())
 
     def close(self):
         if self.dist:
             self.dist.destroy_process_group()
+            self.dist = None
+
+
+def aggregate(dist: Dist, ms: float, cells_steps: float) -> tuple[float, float]:
+    """Whole-job throughput of the replicas: the cell-steps of all ranks over
+    the slowest rank's device time.  Returns (max ms, Mcell-steps/s)."""
+    ms_max = dist.max(ms)
+    total = dist.sum(cells_steps)
+    return ms_max, total / (ms_max / 1e3) / 1e6
 
 
 class Clocks:
@@ -200,9 +219,7 @@ def run_gpu(a, dist: Dist) -> dict | None:
     sweep_ms, sweep_passes = sol.sweep_time()
     ck = clocks.stop()
     dist.barrier()
-    ms_max = dist.max(ms)
-    cells_steps = dist.sum(float(ch.cells) * a.steps)
-    value = cells_steps / (ms_max / 1e3) / 1e6
+    ms_max, value = aggregate(dist, ms, float(ch.cells) * a.steps)
     mean_iters = float(np.mean(iters))
 
     # per-stage device times of one inner iteration (the roofline kernels)
