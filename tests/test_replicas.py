@@ -53,6 +53,10 @@ def _leaver(rank: int, world: int, port: int, q) -> None:
         q.put((rank, "no error", time.time() - t0))
     except Exception as e:  # noqa: BLE001 - any error is the detection
         q.put((rank, type(e).__name__, time.time() - t0))
+    # flush the queue's feeder thread before leaving without the group's
+    # teardown (which would wait for the rank that left)
+    q.close()
+    q.join_thread()
     os._exit(0)
 
 
