@@ -123,11 +123,7 @@ void launch_end_step(const Dev &d, cudaStream_t s);
 // extrapolated initial guess of a step (order 1 or 2) on the interior cells
 void launch_predict(const Dev &d, cudaStream_t s, int order);
 
-// one complete inner iteration on the fast path (halo, boundaries, residual,
-// sweeps, update, partial norms); capturable into a CUDA graph
 // message returned by cgli_last_error() on this thread
 void set_last_error(const std::string &msg);
-
-void launch_fused_iteration(const Dev &d, const SweepArgs &a, cudaStream_t s, int precision);
 
 }  // namespace cgli

@@ -164,10 +164,4 @@ void launch_fused_residual(const Dev &d, const SweepArgs &a, cudaStream_t s, int
   launch_residual_fast(d, a, s, precision == 1);
 }
 
-void launch_fused_iteration(const Dev &d, const SweepArgs &a, cudaStream_t s, int precision) {
-  launch_fused_residual(d, a, s, precision);
-  launch_sweeps(d, a, s, precision == 1);
-  launch_sweep_update(d, a, s, precision == 1);
-}
-
 }  // namespace cgli
