@@ -312,12 +312,6 @@ int cgli_create(const cgli_params *p, cgli_ctx **out) {
   if (rc == CGLI_OK) rc = alloc(c, 16 * sizeof(int), (void **)&d.status);
   if (rc == CGLI_OK) rc = alloc(c, 3 * 2 * sizeof(double) * d.Y, (void **)&d.ftab);
   c->update_blocks = p->nx * p->ny;
-  // relaxation tile shape of the DP-LUR solver (tuning; defaults 6 rows, 32 planes)
-  if (const char *ev = getenv("CGLI_DPLUR_TILE_ROWS")) cgli::dplur_tile_rows = atoi(ev) == 14 ? 14 : 6;
-  if (const char *ev = getenv("CGLI_DPLUR_CHUNK")) {
-    int v = atoi(ev);
-    if (v >= 2 && v <= 4096) cgli::dplur_chunk = v;
-  }
   const int nti = (p->nx + cgli::SWEEP_TI - 1) / cgli::SWEEP_TI, ntj = (p->ny + cgli::SWEEP_TJ - 1) / cgli::SWEEP_TJ;
   c->sweep_tiles = nti * ntj;
   size_t nblk = (size_t)std::max(c->update_blocks, c->sweep_tiles);

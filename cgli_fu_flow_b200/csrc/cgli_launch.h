@@ -83,9 +83,6 @@ void launch_dplur(const Dev &d, const SweepArgs &sw, cudaStream_t s);
 void launch_dplur_relax(const Dev &d, const SweepArgs &sw, cudaStream_t s, bool from_nr);
 // halo, boundaries, fluxes, viscous terms, then launch_dplur
 void launch_dplur_iteration(const Dev &d, const SweepArgs &sw, cudaStream_t s);
-// relaxation tile rows (6 or 14) and x planes per CTA
-extern int dplur_tile_rows;
-extern int dplur_chunk;
 // residual assembly writing MR and the first sweep's lagged halo planes
 void launch_residual_fast(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed);
 

@@ -322,17 +322,14 @@ RelaxPtrs ptrs(double *const *src, double *const *dst, const SweepArgs &sw) {
 
 }  // namespace
 
-int dplur_tile_rows = 6;   // TJ of the relaxation tiles (6 or 14)
-int dplur_chunk = 32;      // x planes per CTA
+// relaxation tiles of 6 j rows marching over 32 x planes, the shape chosen
+// by measurement at 256x192x192 (14 rows and other plane counts)
+constexpr int kDplurChunk = 32;
 
 void launch_dplur_relax(const Dev &d, const SweepArgs &sw, cudaStream_t s, bool from_nr) {
   RelaxPtrs a = from_nr ? ptrs(d.NR, d.NL, sw) : ptrs(d.NL, d.NR, sw);
-  const bool ch = sw.channel_metrics != 0;
-  // 14-row tiles only with the metric tables: the staged general metrics
-  // would not fit in shared memory
-  if (dplur_tile_rows == 14 && ch) relax<14, true>(d, a, s, dplur_chunk);
-  else if (ch) relax<6, true>(d, a, s, dplur_chunk);
-  else relax<6, false>(d, a, s, dplur_chunk);
+  if (sw.channel_metrics) relax<6, true>(d, a, s, kDplurChunk);
+  else relax<6, false>(d, a, s, kDplurChunk);
 }
 
 // residual (MR, NR = D^-1 MR), four relaxations NR->NL->NR->NL->NR, update
