@@ -99,6 +99,27 @@ def test_dplur_oracle_matches_reference_second_grid():
 
 
 @pytest.mark.skipif(not have_reference(), reason="reference sources not present")
+@pytest.mark.parametrize("dims,threads", [((3, 6, 4), 2), ((11, 7, 9), 3)])
+def test_dplur_oracle_matches_reference_at_edge_sizes(dims, threads):
+    """The smallest accepted grid and an odd-sized one: the relaxation's
+    neighbour terms at every wall and end row, bit-identical over two
+    steps, norms up to the reference's global 3 Nx."""
+    from oracle.oracle import Oracle
+    from oracle.refrun import RefSolver
+    ch = Channel(*dims)
+    r = RefSolver(ch, threads=threads, inner_solver="dplur")
+    r.init()
+    o = Oracle(ch, inner_solver="dplur")
+    o.init()
+    sl = (slice(None),) + _regions(ch)["cell"]
+    for _ in range(2):
+        _, er_r = r.step(4)
+        _, er_o = o.step(4)
+        assert np.array_equal(r.q()[sl], o.q()[sl])
+        np.testing.assert_allclose(3.0 * np.asarray(er_r), er_o, rtol=1e-14)
+
+
+@pytest.mark.skipif(not have_reference(), reason="reference sources not present")
 def test_dplur_oracle_matches_reference_wavy_grid():
     from oracle.oracle import Oracle
     from oracle.refrun import RefSolver
