@@ -305,7 +305,7 @@ def test_statistics_match_restatement(lib):
 
 
 def test_mixed_mean_velocity_profile_within_half_percent(lib):
-    """The configs[2] criterion on a small channel: the mean streamwise
+    """The mixed-precision acceptance criterion on a small channel: the mean streamwise
     velocity profile over x, z and the steps of the mixed path agrees with
     the FP64 path's within 0.5 % (max over the wall-normal cells, relative to
     the bulk velocity)."""
