@@ -3,7 +3,7 @@
  *
  * TEST INFRASTRUCTURE ONLY.  Nothing in the product links or calls this file;
  * only tests/, __graft_entry__.smoke() and the CPU-baseline leg of bench.py
- * use it, and only as the checker.
+ * use it, and only as the source of expected values.
  *
  * Every routine follows one reference routine (cited file:line) statement for
  * statement in its floating-point arithmetic: the same expressions in the

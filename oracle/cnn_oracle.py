@@ -2,7 +2,7 @@
 backward of the 3-D convolutional network, with BF16 rounding at the same
 points as the CUDA kernels.
 
-Test infrastructure only: imported by tests/ as the checker of the
+Test infrastructure only: imported by tests/ for the expected values of the
 tensor-core kernels (values and gradients), never by the product.
 
 The network (no reference code exists for it; it is defined by the project):

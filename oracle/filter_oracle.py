@@ -1,7 +1,7 @@
 """CPU restatement of the reference's high-order filter sensor, Filter.cpp:12-1720.
 
 Test infrastructure only: imported by tests/ and tests/golden/make_golden.py
-as the checker of the CUDA filter kernels, never by the product.
+as the expected values for the CUDA filter kernels, never by the product.
 
 numpy float64, every expression evaluated in the order Filter.cpp writes it
 (numpy does not fuse multiply-adds), so the result is bit-identical to the
