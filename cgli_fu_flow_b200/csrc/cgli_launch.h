@@ -13,9 +13,17 @@ namespace cgli {
 constexpr int CR_N = REC_N + 5 + 1;
 constexpr int CR_MR = REC_N;
 
-// tile shape of the wavefront sweeps: TI x TJ (i, j) columns per CTA
-constexpr int SWEEP_TI = 8;
-constexpr int SWEEP_TJ = 16;
+// tile shape of the wavefront sweeps: TI x TJ (i, j) columns per CTA (one
+// thread each, so TI * TJ <= 1024 and a multiple of 32)
+#ifndef CGLI_SWEEP_TI
+#define CGLI_SWEEP_TI 8
+#endif
+#ifndef CGLI_SWEEP_TJ
+#define CGLI_SWEEP_TJ 16
+#endif
+constexpr int SWEEP_TI = CGLI_SWEEP_TI;
+constexpr int SWEEP_TJ = CGLI_SWEEP_TJ;
+static_assert(SWEEP_TI * SWEEP_TJ <= 1024 && (SWEEP_TI * SWEEP_TJ) % 32 == 0, "sweep tile shape");
 constexpr int CGLI_TIMEOUT_CODE = 6;
 
 // buffers of the tile-wavefront sweeps (kernels_sweep.cu)
