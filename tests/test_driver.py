@@ -26,6 +26,18 @@ def test_driver_rejects_incomplete_command_line():
     assert r.returncode == 1 and "usage" in r.stderr
 
 
+def test_driver_reports_library_errors(tmp_path):
+    """A call the library refuses (here a grid below the smallest accepted
+    one; on a machine without a GPU the context cannot be created at all)
+    ends the driver with status 2 and the library's message."""
+    r = subprocess.run([_driver(), "--nx", "2", "--ny", "4", "--nz", "4", "--dxi", "1e-3", "--det", "0.25",
+                        "--dzt", "1e-3", "--dt", "1e-6", "--e", "0.1", "--mu", "1.85e-5", "--pr", "0.72",
+                        "--high", "1e-3", "--stretch", "2.0", "--initial", str(tmp_path / "none.bin"),
+                        "--steps", "1"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 2, (r.returncode, r.stderr)
+    assert r.stderr.startswith("cgli_run: cgli_create: ") and len(r.stderr.strip()) > len("cgli_run: cgli_create:")
+
+
 def _args(ch, initial, output, steps, extra=()):
     f = lambda x: repr(float(x))
     return [_driver(), "--nx", str(ch.nx), "--ny", str(ch.ny), "--nz", str(ch.nz), "--dxi", f(ch.dxi),
