@@ -93,6 +93,29 @@ def test_filter_oracle_matches_reference_build_second_grid():
             assert np.array_equal(ref[f][M[f]], mine[f][M[f]]), (q, "XYZ"[f])
 
 
+@pytest.mark.skipif(not os.path.isdir(REF), reason="reference sources not present")
+@pytest.mark.parametrize("dims", [(11, 14, 9), (8, 6, 5)])
+def test_filter_oracle_matches_reference_build_odd_sizes(dims):
+    """Odd extents and the smallest wall-normal extent, on a state two steps
+    from the seeded field: EpX/EpY/EpZ bit-identical at three thresholds."""
+    from oracle.refrun import RefSolver
+    ch = Channel(*dims)
+    r = RefSolver(ch, threads=2, build=True)
+    r.init()
+    r.step(2)
+    r.lib.ref_halo_bc()
+    U = [r.array(f"U{v}_").copy() for v in range(1, 6)]
+    J, yp = r.array("J").copy(), ch.y_point()
+    R = F.sensor(U, J, yp, ch.nx, ch.ny, ch.nz, x_ends=None)
+    M = F.face_masks(ch.nx, ch.ny, ch.nz, J.shape, x_ends=None)
+    for q in (0.25, 0.5, 0.75):
+        crit = float(np.quantile(R[0][M[0]], q))
+        ref = r.filter(yp, crit, E_HIGH, E_LOW)
+        mine, _, _ = F.filter_ep(U, J, yp, ch.nx, ch.ny, ch.nz, crit, E_HIGH, E_LOW, x_ends=None)
+        for f in range(3):
+            assert np.array_equal(ref[f][M[f]], mine[f][M[f]]), (q, "XYZ"[f])
+
+
 # ------------------------------------------------------------------ GPU
 
 def _gpu(ch):
