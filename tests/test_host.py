@@ -124,3 +124,13 @@ def test_force_controller_steers_toward_target():
     st = {}
     f_lo = C.force_update(st, ch.target_flux * 0.99, ch)
     assert f_lo > ch.force_lam
+
+
+def test_wavefront_step_count():
+    """Hyperplane steps of one wavefront pass of 8 x 16 tiles (the profiling
+    runner's per-step figure): nz + 22 for one tile, plus 8 per extra tile
+    in x and 16 per extra tile in y (ragged tiles count whole)."""
+    from cgli_fu_flow_b200.run import wavefront_steps
+    assert wavefront_steps(8, 16, 192) == 214
+    assert wavefront_steps(256, 192, 192) == 256 + 192 + 192 - 2
+    assert wavefront_steps(9, 17, 10) == 10 + 22 + 8 + 16
