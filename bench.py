@@ -46,7 +46,6 @@ import numpy as np  # noqa: E402
 from cgli_fu_flow_b200 import channel as C  # noqa: E402
 
 METRIC = "Mcell-steps/s at fixed inner-residual drop (1e-3, cap 30)"
-ITERS_FILE = os.path.join(HERE, "cgli_fu_flow_b200", "workload_iters.json")
 
 
 def parse():
@@ -61,7 +60,7 @@ def parse():
     ap.add_argument("--cap", type=int, default=30)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--cpu-iters", type=int, default=2, help="reference inner iterations in the CPU sample")
+    ap.add_argument("--cpu-iters", type=int, default=4, help="reference inner iterations in the CPU sample")
     ap.add_argument("--arms", default="all", choices=["all", "none"])
     ap.add_argument("--collect", type=int, default=48, help="steps before the common point of the arms")
     ap.add_argument("--skip", type=int, default=16, help="first steps (initial transient) not used for training")
@@ -195,6 +194,14 @@ def workload_label(ch) -> str:
     return f"channel {ch.nx}x{ch.ny}x{ch.nz} cells, Mach 0.2, Re_b 5600"
 
 
+def bench_config(a, ch) -> dict:
+    """The workload of a bench line, the same object in both arms."""
+    return {"workload": workload_label(ch), "cells": ch.cells, "precision": a.precision,
+            "inner": f"until every one of the five update norms is below {a.drop:g} of its running maximum over "
+                     f"the run (main.cpp:287-297), cap {a.cap}",
+            "start": "seeded field", "l2": "inputs larger than L2 (state and records ~0.8 GB per field group)"}
+
+
 # ------------------------------------------------------------ GPU arm
 def run_gpu(a, dist: Dist) -> dict | None:
     from cgli_fu_flow_b200.solver import Solver, FP64, MIXED
@@ -251,12 +258,9 @@ def run_gpu(a, dist: Dist) -> dict | None:
         "vs_baseline": None,
         "dtype": "f64" if a.precision == "fp64" else "f64 residual / f32 sweeps",
         "data": "synthetic: seeded Poiseuille + 10% uniform perturbation channel (no dataset involved)",
-        "config": {"workload": workload_label(ch),
-                   "cells": ch.cells, "precision": a.precision,
-                   "inner": f"until 1e-3 drop of all five update norms, cap {a.cap}",
-                   "mean_inner_iterations": round(mean_iters, 2), "inner_iterations": iters,
-                   "parallelism": "replicas" if dist.world > 1 else "single GPU",
-                   "l2": "inputs larger than L2 (state and records ~0.8 GB per field group)"},
+        "config": bench_config(a, ch),
+        "parallelism": "replicas" if dist.world > 1 else "single GPU",
+        "mean_inner_iterations": round(mean_iters, 2), "inner_iterations": iters,
         "clocks": ck,
         "stage_ms": {k: round(v, 4) for k, v in stages.items()},
         "roofline": roof,
@@ -398,12 +402,16 @@ def run_e2e(a, ch, prec, dist: Dist) -> dict:
 
 
 # ------------------------------------------------------------ CPU reference
-def mean_iters_for(workload: str, precision: str = "fp64", default: int = 30) -> float:
-    try:
-        with open(ITERS_FILE) as fh:
-            return float(json.load(fh)[f"{workload}/{precision}"])
-    except Exception:
-        return float(default)
+def reference_build(ch) -> tuple[str, str] | None:
+    """The reference's compiled routines for the workload: the -O3 timing
+    build (the reference Makefile's flags) if present, else the pinning
+    build; (flavor, path) or None."""
+    from oracle import build_ref
+    for flavor in ("perf", "pin"):
+        path = build_ref.lib_path(ch.name, flavor)
+        if os.path.exists(path):
+            return flavor, path
+    return None
 
 
 def cpu_reference_sample(ch, iters: int, warm: int = 1) -> dict:
@@ -411,7 +419,8 @@ def cpu_reference_sample(ch, iters: int, warm: int = 1) -> dict:
     inner iterations of the workload with every host core (OpenMP)."""
     from oracle.refrun import RefSolver
     cores = os.cpu_count() or 1
-    r = RefSolver(ch, threads=cores, build=False)
+    flavor, _ = reference_build(ch)
+    r = RefSolver(ch, threads=cores, build=False, flavor=flavor)
     r.init()
     for _ in range(warm):
         r.inner_iteration()
@@ -419,40 +428,56 @@ def cpu_reference_sample(ch, iters: int, warm: int = 1) -> dict:
     for _ in range(iters):
         r.inner_iteration()
     dt = (time.perf_counter() - t) / iters
-    return {"sec_per_inner_iteration": dt, "cores": cores}
+    return {"sec_per_inner_iteration": dt, "cores": cores, "build": flavor}
+
+
+BUILD_NAMES = {"perf": "g++ -O3 -fopenmp, the reference Makefile's optimisation level",
+               "pin": "g++ -O2 -fopenmp -ffp-contract=off, the build the oracle is pinned to"}
 
 
 def run_reference(a, dist: Dist) -> dict | None:
+    """The reference's own CPU implementation of the step on the host cores:
+    whole physical steps of its compiled routines from the seeded field, each
+    iterated with its own stopping rule (main.cpp:287-304: every norm below
+    `drop` of its running maximum, cap), W untimed, then K timed by wall
+    clock -- the same steps of the same run as the GPU arm's, so the same
+    inner-iteration counts."""
     if dist.rank != 0:
         return None
     ch = C.workload(a.workload)
-    lib = os.path.join(HERE, "oracle", "_ref", ch.name, "libref.so")
-    if not os.path.exists(lib):
-        return {"impl": "reference", "unavailable": f"reference build {lib} missing (build() compiles it where the "
-                                                    "reference sources are present)"}
-    m_it = mean_iters_for(a.workload, "fp64")
+    found = reference_build(ch)
+    if found is None:
+        return {"impl": "reference", "unavailable": f"reference build for {ch.name} missing (build() compiles it "
+                                                    "where the reference sources are present)"}
+    flavor, path = found
     from oracle.refrun import RefSolver
     cores = os.cpu_count() or 1
-    r = RefSolver(ch, threads=cores, build=False)
+    r = RefSolver(ch, threads=cores, build=False, flavor=flavor)
     r.init()
-    per_step = []
-    for s in range(a.warmup + a.steps):
-        t = time.perf_counter()
-        r.inner_iteration()
-        dt = time.perf_counter() - t
-        if s >= a.warmup:
-            per_step.append(dt)
-    sec_iter = float(np.mean(per_step))
-    value = ch.cells / (sec_iter * m_it) / 1e6
-    sample = (f"{a.steps} timed inner iterations (after {a.warmup}) of the reference's routines on the "
-              f"{ch.nx}x{ch.ny}x{ch.nz} channel; one physical step = {m_it:g} inner iterations, the count the "
-              f"FP64 GPU path needs for the 1e-3 drop on this workload")
+    warm_iters, iters = [], []
+    t0 = time.perf_counter()
+    for _ in range(a.warmup):
+        it, _ = r.step(None, a.drop, a.cap)
+        warm_iters.append(it)
+    warm_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        it, _ = r.step(None, a.drop, a.cap)
+        iters.append(it)
+    sec = time.perf_counter() - t0
+    value = ch.cells * a.steps / sec / 1e6
+    sample = (f"{a.steps} whole physical steps (after {a.warmup} untimed) of the reference's routines "
+              f"({BUILD_NAMES[flavor]}; OpenMP on {cores} threads; single process, no MPI library here) on the "
+              f"{ch.nx}x{ch.ny}x{ch.nz} channel from the seeded field, each iterated to its own stopping rule; "
+              f"wall clock")
     return {"impl": "reference", "metric": METRIC, "value": round(value, 5), "unit": "Mcell-steps/s",
             "n_gpus": dist.world, "steps": a.steps, "warmup": a.warmup,
-            "ms_per_step": round(sec_iter * m_it * 1e3, 1), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic seeded channel",
-            "config": {"workload": workload_label(ch),
-                       "cells": ch.cells, "inner_iterations_per_step": m_it},
+            "ms_per_step": round(sec / a.steps * 1e3, 1), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic: seeded Poiseuille + 10% uniform perturbation "
+                                                         "channel (no dataset involved)",
+            "config": bench_config(a, ch), "parallelism": f"host cores (OpenMP, {cores} threads)",
+            "mean_inner_iterations": round(float(np.mean(iters)), 2), "inner_iterations": iters,
+            "warmup_inner_iterations": warm_iters, "warmup_s": round(warm_s, 1),
             "cpu_baseline": {"value": round(value, 5), "unit": "Mcell-steps/s", "cores": cores,
                              "kind": "reference", "sample": sample},
             "e2e": {"value": round(value, 5), "unit": "Mcell-steps/s", "h2d_bytes_per_step": 0,
@@ -505,16 +530,17 @@ def main():
             out = run_gpu(a, dist)
             if out is not None and not a.no_cpu_baseline and dist.world == 1:
                 ch = C.workload(a.workload)
-                lib = os.path.join(HERE, "oracle", "_ref", ch.name, "libref.so")
-                if os.path.exists(lib):
+                if reference_build(ch) is not None:
                     smp = cpu_reference_sample(ch, a.cpu_iters)
-                    m_it = out["config"]["mean_inner_iterations"]
+                    m_it = out["mean_inner_iterations"]
                     v = ch.cells / (smp["sec_per_inner_iteration"] * m_it) / 1e6
                     out["cpu_baseline"] = {
                         "value": round(v, 5), "unit": "Mcell-steps/s", "cores": smp["cores"], "kind": "reference",
                         "sample": f"{a.cpu_iters} inner iterations of the reference's compiled routines on the same "
-                                  f"workload ({smp['sec_per_inner_iteration']:.2f} s each, OpenMP on "
-                                  f"{smp['cores']} threads), scaled by the GPU run's {m_it:g} iterations per step"}
+                                  f"workload ({BUILD_NAMES[smp['build']]}; {smp['sec_per_inner_iteration']:.2f} s "
+                                  f"each, OpenMP on {smp['cores']} threads), times the {m_it:g} inner iterations "
+                                  f"per step that this run's timed steps needed (the reference needs the same "
+                                  f"count: its numerics match to 1e-10)"}
                 else:
                     out["cpu_baseline"] = {"value": None, "unit": "Mcell-steps/s", "cores": 0, "kind": "reference",
                                            "sample": "reference build missing"}

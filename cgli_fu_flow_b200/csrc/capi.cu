@@ -362,7 +362,7 @@ int cgli_create(const cgli_params *p, cgli_ctx **out) {
     if (rc == CGLI_OK) rc = alloc(c, sizeof(double) * d.Y, (void **)&jt);
     if (rc == CGLI_OK) rc = alloc(c, sizeof(double) * d.Y, (void **)&et);
     a.Jtab = jt; a.etdytab = et;
-    a.spin_limit = 1 << 22;
+    a.spin_limit = CGLI_WAIT_LIMIT_DEFAULT;
   }
   if (rc == CGLI_OK) {
     cudaError_t e = cgli::sweep_kernel_attributes();
@@ -804,6 +804,21 @@ int cgli_set_predictor(cgli_ctx *c, int mode) {
     return fail(CGLI_EINVAL, "predictor mode must be 0 (previous level), 1 (extrapolation) or 2 (learned)");
   if (mode == 2 && !c->cnn) return fail(CGLI_ESTATE, "predictor 2 needs a network (cgli_set_learned_guess)");
   c->predictor = mode;
+  return CGLI_OK;
+}
+
+int cgli_sweep_tile_shape(int *ti, int *tj) {
+  if (!ti || !tj) return fail(CGLI_EINVAL, "null argument");
+  *ti = cgli::SWEEP_TI;
+  *tj = cgli::SWEEP_TJ;
+  return CGLI_OK;
+}
+
+int cgli_set_wait_limit(cgli_ctx *c, int polls) {
+  int rc = check(c); if (rc) return rc;
+  if (polls < 0) return fail(CGLI_EINVAL, "wait limit must be >= 0 polls");
+  if (polls != c->sw.spin_limit) drop_graph(c);   // the graph holds the launch arguments
+  c->sw.spin_limit = polls;
   return CGLI_OK;
 }
 

@@ -21,8 +21,12 @@
 // column through global buffers filled with a sentinel bit pattern before the
 // pass; the consumer spins (bounded) on the values themselves until none is
 // the sentinel, so a hand-over needs no fence and no counter (4- and 8-byte
-// stores are single-copy atomic).  On timeout the kernel records the timeout
-// code in the status word and carries on; the host reports CGLI_ETIMEOUT.
+// stores are single-copy atomic).  When a wait gives up (the hand-over poll or
+// the record copy's mbarrier, SweepArgs::spin_limit polls) the tile records
+// the timeout code in the status word, waits (bounded) for its own bulk
+// copies still in flight and returns; the tiles downstream then give up on
+// it in turn, the update kernel leaves the state alone, and the host reports
+// CGLI_ETIMEOUT.
 // Tiles take tickets in an order where every dependency holds a smaller
 // ticket, so a waiting CTA only ever waits on CTAs that are already running.
 //
@@ -101,9 +105,10 @@ __device__ __forceinline__ float ld_gpu(const float *p) {
 __device__ __forceinline__ bool is_sentinel(double v) { return __double_as_longlong(v) == -1ll; }
 __device__ __forceinline__ bool is_sentinel(float v) { return __float_as_int(v) == -1; }
 
-// bounded spin on five values handed over by a neighbouring tile
+// bounded spin on five values handed over by a neighbouring tile; false
+// (and the timeout code in the status word) when it gives up
 template <typename T>
-__device__ __forceinline__ void recv5(const T *src, T out[5], int *status, int limit) {
+__device__ __forceinline__ bool recv5(const T *src, T out[5], int *status, int limit) {
   for (int it = 0;; it++) {
     bool ok = true;
 #pragma unroll
@@ -111,14 +116,18 @@ __device__ __forceinline__ void recv5(const T *src, T out[5], int *status, int l
       out[v] = ld_gpu(src + v);
       ok = ok && !is_sentinel(out[v]);
     }
-    if (ok) return;
+    if (ok) return true;
     if (it >= limit) {
       atomicExch(status, CGLI_TIMEOUT_CODE);
-      return;
+      return false;
     }
     __nanosleep(20);
   }
 }
+
+// polls for the wait on a tile's own bulk copies before it returns after a
+// timeout (the copies complete on their own; this only bounds the wait)
+constexpr int kDrainPolls = 1 << 20;
 
 // REC_N record words and (mr non-null) the 5 MR words of one slot, through
 // the read-only path (CGLI_SWEEP_LDG) or plain loads
@@ -350,7 +359,11 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
     if (s + 1 < S) fetch_cell<TI, TJ, Met, BACKWARD, T>(d, a, s_et, il, jl, j, s + 1, S, tile_base, inside, halo_edge, nxt);
     else nxt.active = false;
     // this step's records (bounded wait; a timeout is reported like a tile's)
-    if (!tc::mbar_wait(tc::smem_addr(&s_bar[s & 1]), (s >> 1) & 1, a.spin_limit)) atomicExch(d.status, CGLI_TIMEOUT_CODE);
+    int gave_up = 0;
+    if (!tc::mbar_wait(tc::smem_addr(&s_bar[s & 1]), (s >> 1) & 1, a.spin_limit)) {
+      atomicExch(d.status, CGLI_TIMEOUT_CODE);
+      gave_up = 1;
+    }
     if (cur.active)
       load_cellrec(s_rec + (s & 1) * (TI * TJ * CR_N) + threadIdx.x * CR_N, cur.rec, BACKWARD ? (T *)nullptr : cur.mr);
     if (cur.active) {
@@ -367,7 +380,7 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
         bool ok = true;
 #pragma unroll
         for (int v = 0; v < 5; v++) { tx[v] = px0[v]; ok = ok && !is_sentinel(px0[v]); }
-        if (!ok) recv5<T>(xsrc + (long long)kl * 5, tx, d.status, a.spin_limit);
+        if (!ok && !recv5<T>(xsrc + (long long)kl * 5, tx, d.status, a.spin_limit)) gave_up = 1;
       }
       if (!recv_y) {
         const int sjl = BACKWARD ? jl + 1 : jl - 1;
@@ -377,7 +390,7 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
         bool ok = true;
 #pragma unroll
         for (int v = 0; v < 5; v++) { ty[v] = py0[v]; ok = ok && !is_sentinel(py0[v]); }
-        if (!ok) recv5<T>(ysrc + (long long)kl * 5, ty, d.status, a.spin_limit);
+        if (!ok && !recv5<T>(ysrc + (long long)kl * 5, ty, d.status, a.spin_limit)) gave_up = 1;
       } else {
 #pragma unroll
         for (int v = 0; v < 5; v++) ty[v] = 0;  // wall ghost row: dQ = 0 there
@@ -462,7 +475,16 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
       if (s + 2 < S) preload(s + 2, px1, py1);
     }
     cur = nxt;
-    __syncthreads();
+    if (__syncthreads_or(gave_up)) {
+      // a wait of this step gave up: wait (bounded) for the record copies
+      // still in flight into this CTA's shared memory, then stop; the
+      // consumers of this tile's products give up on it in turn
+      if (threadIdx.x == 0) {
+        tc::mbar_wait(tc::smem_addr(&s_bar[s & 1]), (s >> 1) & 1, kDrainPolls);
+        if (s + 1 < S) tc::mbar_wait(tc::smem_addr(&s_bar[(s + 1) & 1]), ((s + 1) >> 1) & 1, kDrainPolls);
+      }
+      return;
+    }
   }
 }
 
@@ -474,6 +496,8 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
 // q1, rho, T and J are reciprocals (1/J from the table).
 template <typename T>
 __global__ void __launch_bounds__(128) k_update_skewed(Dev d, SweepArgs a) {
+  // a wavefront pass that gave up left dQ incomplete: keep the state
+  if (*(volatile int *)d.status) return;
   const int j = 2 + blockIdx.x, i = 3 + blockIdx.y;
   T *const *dq = SweepPtrs<T>::dq(a);
   double acc[5] = {0, 0, 0, 0, 0};

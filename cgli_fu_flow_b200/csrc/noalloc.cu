@@ -10,11 +10,11 @@
 // :1761-1782, the same arithmetic as the context path (kernels_ref.cu,
 // k_update + k_norms), whose per-row partial sums live in context memory.
 // Here the partial sums live in one file-scope device array of fixed size,
-// resolved once per device with cudaGetSymbolAddress.
+// whose device address every call looks up with cudaGetSymbolAddress (no
+// allocation) on the current device.
 #include <cuda_runtime.h>
 
 #include <cmath>
-#include <mutex>
 #include <string>
 
 #include "../../include/cgli_fu_flow.h"
@@ -35,10 +35,11 @@ struct CPtr5 {
   const double *p[5];
 };
 
-// k_update of kernels_ref.cu with the partial sums written to `partial`
-__global__ void k_update_noalloc(int nz, long long di, long long dj, Ptr5 q, const double *J, CPtr5 nr,
+// k_update of kernels_ref.cu with the partial sums written to `partial`;
+// one block per (i, j) row, row r = (i - 3) * Ny + (j - 2) on a 1-D grid
+__global__ void k_update_noalloc(int ny, int nz, long long di, long long dj, Ptr5 q, const double *J, CPtr5 nr,
                                  double *partial) {
-  const int i = 3 + blockIdx.y, j = 2 + blockIdx.x;
+  const int i = 3 + blockIdx.x / ny, j = 2 + blockIdx.x % ny;
   double acc[5] = {0, 0, 0, 0, 0};
   for (int k = 2 + threadIdx.x; k <= nz + 1; k += blockDim.x) {
     const long long c = (long long)i * di + (long long)j * dj + k;
@@ -68,7 +69,7 @@ __global__ void k_update_noalloc(int nz, long long di, long long dj, Ptr5 q, con
   }
   // every row writes its own five sums, so no part of the scratch has to
   // start at zero; only the rows of this call are read back
-  cgli::block_sum5(acc, partial + 5 * ((long long)blockIdx.y * gridDim.x + blockIdx.x));
+  cgli::block_sum5(acc, partial + 5 * (long long)blockIdx.x);
 }
 
 // k_norms of kernels_ref.cu
@@ -81,9 +82,6 @@ __global__ void k_norms_noalloc(const double *partial, int nrows, double scale, 
   __syncthreads();
   if (threadIdx.x < 5) out[threadIdx.x] = sqrt(tot[threadIdx.x]) * scale;
 }
-
-std::mutex g_mu;
-double *g_scratch_addr[256] = {};   // device address of g_noalloc_scratch, per device ordinal
 
 int fail(int code, const std::string &m) {
   cgli::set_last_error(m);   // reported by cgli_last_error()
@@ -108,29 +106,21 @@ int cgli_update_norms_noalloc(int nx, int ny, int nz, double *const U_[5], const
     q.p[v] = U_[v];
     n.p[v] = NR[v];
   }
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return fail(CGLI_ECUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-  if (dev < 0 || dev >= 256) return fail(CGLI_EINVAL, "device ordinal out of range");
-  double *scratch;
-  {
-    // first call on this device (with it current): resolve the device address
-    // of the static array; its host-side name is not a device address
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_scratch_addr[dev]) {
-      void *p = nullptr;
-      e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-      if (e != cudaSuccess || !p)
-        return fail(CGLI_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-      g_scratch_addr[dev] = (double *)p;
-    }
-    scratch = g_scratch_addr[dev];
-  }
+  // The device address of the static array on the current device.  The
+  // array's host-side name is only a stand-in for it; the address belongs to
+  // the device's current context and changes if that context is torn down
+  // and created again (cudaDeviceReset), so it is looked up on every call
+  // (a table lookup in the runtime: nothing is allocated).
+  void *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p)
+    return fail(CGLI_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+  double *scratch = (double *)p;
   cudaStream_t s = (cudaStream_t)stream;
   const long long dj = nz + 4, di = (long long)(ny + 4) * (nz + 4);
   const int nrows = nx * ny;
   double *norms = scratch + 5 * (long long)CGLI_NOALLOC_MAX_ROWS;
-  k_update_noalloc<<<dim3(ny, nx), 128, 0, s>>>(nz, di, dj, q, J, n, scratch);
+  k_update_noalloc<<<nrows, 128, 0, s>>>(ny, nz, di, dj, q, J, n, scratch);
   k_norms_noalloc<<<1, 1024, 0, s>>>(scratch, nrows, 1.0 / ((double)nx * ny * nz), norms);
   e = cudaGetLastError();
   if (e != cudaSuccess) return fail(CGLI_ECUDA, std::string("launch: ") + cudaGetErrorString(e));

@@ -10,8 +10,8 @@ the last norms and the device time of the step); --iterations N runs N bare
 inner iterations from the seeded field (the five norms of each), the form
 used for kernel profiles; --stages REPS runs two inner iterations, then times
 each stage of one inner iteration REPS times (cgli_profile_stages) and also
-reports the wavefront passes per hyperplane step of the 8 x 16 tile
-wavefront.  --dims runs the seeded channel on any grid instead of a named
+reports the wavefront passes per dependent step of the tile wavefront (the
+tile shape the library was built with, cgli_sweep_tile_shape).  --dims runs the seeded channel on any grid instead of a named
 workload.  One JSON line per step / iteration / stage report.
 """
 from __future__ import annotations
@@ -22,7 +22,7 @@ import json
 from . import channel as C
 
 
-def wavefront_steps(nx: int, ny: int, nz: int, ti: int = 8, tj: int = 16) -> int:
+def wavefront_steps(nx: int, ny: int, nz: int, ti: int, tj: int) -> int:
     """Hyperplane steps of one wavefront pass of ti x tj tiles: the last
     tile starts ti (tj) steps after its x (y) neighbour and runs nz + ti +
     tj - 2 steps."""
@@ -55,14 +55,16 @@ def main(argv=None) -> None:
             er = sol.inner_iteration()
             print(json.dumps({"iteration": n + 1, "norms": [float(x) for x in er]}), flush=True)
     if a.stages:
+        from .solver import sweep_tile_shape
         for _ in range(2):
             sol.inner_iteration()
         st = sol.profile_stages(a.stages)
+        ti, tj = sweep_tile_shape()
+        nsteps = wavefront_steps(ch.nx, ch.ny, ch.nz, ti, tj)
         print(json.dumps({"cells": [ch.nx, ch.ny, ch.nz], "stage_ms": {k: round(v, 4) for k, v in st.items()},
-                          "wavefront_steps": wavefront_steps(ch.nx, ch.ny, ch.nz),
-                          "us_per_wavefront_step": {
-                              d: round(st[f"sweep_{d}"] * 1e3 / wavefront_steps(ch.nx, ch.ny, ch.nz), 3)
-                              for d in ("forward", "backward")}}), flush=True)
+                          "tile": [ti, tj], "wavefront_steps": nsteps,
+                          "us_per_wavefront_step": {d: round(st[f"sweep_{d}"] * 1e3 / nsteps, 3)
+                                                    for d in ("forward", "backward")}}), flush=True)
     for n in range(a.steps):
         sol.event(0)
         it, er = sol.step(None, a.drop, a.cap)

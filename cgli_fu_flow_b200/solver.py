@@ -57,7 +57,7 @@ EXPORTS = [
     "cgli_statistics_accumulate", "cgli_statistics_get", "cgli_statistics_reset",
     "cgli_write_restart", "cgli_read_restart", "cgli_write_history", "cgli_read_history",
     "cgli_dplusgs", "cgli_set_inner_solver", "cgli_x_boundary_condition", "cgli_set_levels",
-    "cgli_sweep_time",
+    "cgli_sweep_time", "cgli_set_wait_limit", "cgli_sweep_tile_shape",
 ]
 
 INNER_SOLVERS = {"lusgs": 0, "dplur": 1}
@@ -99,6 +99,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cgli_hyperplane.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, P, ctypes.c_long, P, ctypes.c_long]
     L.cgli_profile_stages.argtypes = [P, ctypes.c_int, DP]
     L.cgli_set_predictor.argtypes = [P, ctypes.c_int]
+    L.cgli_set_wait_limit.argtypes = [P, ctypes.c_int]
+    L.cgli_sweep_tile_shape.argtypes = [ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
     L.cgli_filter.argtypes = [P, D, D, D]
     F = ctypes.c_float
     FP = ctypes.POINTER(ctypes.c_float)
@@ -352,6 +354,10 @@ class Solver:
         2: extrapolation plus the learned correction (set_learned_guess)."""
         self._rc(self.L.cgli_set_predictor(self.h, mode))
 
+    def set_wait_limit(self, polls: int) -> None:
+        """Polls before a wavefront wait gives up (cgli_set_wait_limit)."""
+        self._rc(self.L.cgli_set_wait_limit(self.h, polls))
+
     def write_restart(self, path: str, global_nx: int | None = None, x_offset: int = 0,
                       history: bool = True) -> None:
         """The reference's LES%05d.bin layout (this slab of a global_nx-plane
@@ -434,6 +440,16 @@ class Solver:
             # the time-level shift leaves U_ = Q^(n+1): the converged bulk flux
             self.set_force(C.force_update(self.ctrl, self.bulk_flux(), self.ch))
         return it.value, np.array(er[:])
+
+
+def sweep_tile_shape() -> tuple[int, int]:
+    """(ti, tj): the wavefront tile the loaded library was built with."""
+    L = load_library()
+    ti, tj = ctypes.c_int(), ctypes.c_int()
+    rc = L.cgli_sweep_tile_shape(ctypes.byref(ti), ctypes.byref(tj))
+    if rc:
+        raise CgliError(rc, L.cgli_last_error().decode())
+    return ti.value, tj.value
 
 
 def hyperplane_lists(nx: int, ny: int, nz: int):

@@ -218,6 +218,22 @@ int cgli_step_norms(cgli_ctx *ctx, double *norms, int max_iters, int *iters);
  * cell where the network's output is not finite). */
 int cgli_set_predictor(cgli_ctx *ctx, int mode);
 
+/* Bound of every device-side wait of the LU-SGS wavefront passes (the
+ * reference has none: its OpenMP barriers wait without limit): a tile
+ * waiting for its neighbour's products or for its own record copy polls at
+ * most `polls` times (default CGLI_WAIT_LIMIT_DEFAULT, well over a second),
+ * then records a timeout, finishes its copies in flight and stops; the
+ * update leaves U_ unchanged, the call returns CGLI_ETIMEOUT and the next
+ * call runs normally.  0 makes every wait give up at once (for tests of the
+ * timeout path). */
+#define CGLI_WAIT_LIMIT_DEFAULT 4194304
+int cgli_set_wait_limit(cgli_ctx *ctx, int polls);
+/* The (i, j) column tile of the wavefront passes this library was built
+ * with (no counterpart in the reference, which sweeps whole hyperplanes):
+ * each pass takes Nz + ti + tj - 2 + ti (ceil(Nx/ti) - 1) + tj (ceil(Ny/tj) - 1)
+ * dependent steps.  Host only. */
+int cgli_sweep_tile_shape(int *ti, int *tj);
+
 /* ---- learned initial guess (no counterpart in the reference).  A 3-D
  * convolutional network, 15 -> 32 -> 32 -> 32 -> 32 -> 5 channels, 3x3x3
  * kernels, GELU after the first four layers, periodic in x and z, zero
@@ -314,13 +330,15 @@ int cgli_profile_stages(cgli_ctx *ctx, int reps, double *ms);
  *          all device pointers in the reference layout of an Nx x Ny x Nz slab;
  *   er[5]  host output, sqrt(sum of squared increments) / (Nx Ny Nz) for
  *          rho, u, v, w, p/rho; stream: a cudaStream_t or NULL.
- * Rejects Nx*Ny > CGLI_NOALLOC_MAX_ROWS with CGLI_EINVAL.  The first call on a
- * device (with that device current) looks up the array's device address once;
- * make that first call before any stream capture.  All calls share the array
- * and it keeps the last call's contents (each call overwrites the rows it
- * reads, nothing has to start at zero), so calls that overlap on the GPU --
- * concurrent streams, host threads, devices sharing the process -- race and
- * must be serialised by the caller.  Returns after the norms are on the host. */
+ * Rejects Nx*Ny > CGLI_NOALLOC_MAX_ROWS with CGLI_EINVAL.  Every call looks up
+ * the array's device address on the current device (cudaGetSymbolAddress,
+ * which allocates nothing), so the address stays right after the device's
+ * context is reset.  Each device holds its own copy of the array; on one
+ * device all calls share it and it keeps the last call's contents (each call
+ * overwrites the rows it reads, nothing has to start at zero), so calls that
+ * overlap on the same device -- concurrent streams or host threads -- race
+ * and must be serialised by the caller; calls on different devices do not.
+ * Returns after the norms are on the host. */
 #define CGLI_NOALLOC_MAX_ROWS 131072
 int cgli_update_norms_noalloc(int nx, int ny, int nz, double *const U_[5], const double *J,
                               const double *const NR[5], double er[5], void *stream);

@@ -74,6 +74,12 @@ PATCHES = {
 }
 
 CXXFLAGS = ["-O2", "-fopenmp", "-fPIC", "-w", "-std=gnu++14", "-ffp-contract=off"]
+# The timing build ("perf"): the optimisation level of the reference's own
+# Makefile (mpicxx -O3, Makefile:9,15) with OpenMP; the pinning build above
+# keeps -O2 without contraction so that the C restatement matches it bit for
+# bit.  Both compile the same patched sources.
+CXXFLAGS_PERF = ["-O3", "-fopenmp", "-fPIC", "-w", "-std=gnu++14"]
+FLAVORS = {"pin": CXXFLAGS, "perf": CXXFLAGS_PERF}
 
 
 def r17(x: float) -> str:
@@ -161,29 +167,38 @@ def patched_source(fname: str) -> str:
     return text
 
 
-def compile_one(fname: str, outdir: str, cfgdir: str) -> str:
+def compile_one(fname: str, outdir: str, cfgdir: str, flags: list[str] = CXXFLAGS) -> str:
     obj = os.path.join(outdir, fname.replace(".cpp", ".o"))
     incs = ["-I", cfgdir, "-I", os.path.join(HERE, "mpi_stub"), "-I", REF_SRC]
     if fname == "ref_harness.cpp":
-        cmd = ["g++", *CXXFLAGS, *incs, "-c", os.path.join(HERE, fname), "-o", obj]
+        cmd = ["g++", *flags, *incs, "-c", os.path.join(HERE, fname), "-o", obj]
         subprocess.run(cmd, check=True)
     else:
-        cmd = ["g++", *CXXFLAGS, *incs, "-x", "c++", "-c", "-", "-o", obj]
+        cmd = ["g++", *flags, *incs, "-x", "c++", "-c", "-", "-o", obj]
         subprocess.run(cmd, input=patched_source(fname).encode(), check=True)
     return obj
 
 
-def build(params: dict, name: str | None = None, jobs: int = 8) -> str:
+def lib_path(name: str, flavor: str = "pin") -> str:
+    """Where build() puts the library of workload `name` (the timing build
+    in a directory of its own, <name>_O3)."""
+    return os.path.join(HERE, "_ref", name if flavor == "pin" else f"{name}_O3", "libref.so")
+
+
+def build(params: dict, name: str | None = None, jobs: int = 8, flavor: str = "pin") -> str:
     """Builds (if needed) and returns the path of libref.so for `params`
     (keys nx, ny, nz, dxi, det, dzt, high, mu, pr, stretch, twall_lo, twall_hi,
-    and for the open configuration x_open, nx_inlet, nx_outlet)."""
+    and for the open configuration x_open, nx_inlet, nx_outlet).  flavor
+    "pin" is the build the oracle is pinned to, "perf" the timing build with
+    the reference Makefile's -O3."""
     if not os.path.isdir(REF_SRC):
         raise FileNotFoundError(f"reference sources not found at {REF_SRC}")
     name = name or f"channel_{params['nx']}x{params['ny']}x{params['nz']}"
-    outdir = os.path.join(HERE, "_ref", name)
-    lib = os.path.join(outdir, "libref.so")
+    flags = FLAVORS[flavor]
+    lib = lib_path(name, flavor)
+    outdir = os.path.dirname(lib)
     stamp = os.path.join(outdir, "params.json")
-    want = json.dumps(params, sort_keys=True)
+    want = json.dumps(dict(params, cxxflags=flags) if flavor != "pin" else params, sort_keys=True)
     deps = [os.path.join(HERE, "ref_harness.cpp"), os.path.join(HERE, "mpi_stub", "mpi.h"),
             os.path.abspath(__file__)]
     if os.path.exists(lib) and os.path.exists(stamp):
@@ -194,7 +209,7 @@ def build(params: dict, name: str | None = None, jobs: int = 8) -> str:
     cfgdir = os.path.join(outdir, "cfg")
     gen_headers(cfgdir, params)
     with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
-        objs = list(ex.map(lambda f: compile_one(f, outdir, cfgdir), SOURCES + ["ref_harness.cpp"]))
+        objs = list(ex.map(lambda f: compile_one(f, outdir, cfgdir, flags), SOURCES + ["ref_harness.cpp"]))
     subprocess.run(["g++", "-shared", "-fopenmp", "-o", lib, *objs, "-Wl,--no-undefined", "-lm"], check=True)
     with open(stamp, "w") as fh:
         fh.write(want)

@@ -19,17 +19,21 @@ from . import build_ref
 class RefSolver:
     """One reference process (rank 1 of 3, periodic x) for one workload."""
 
-    def __init__(self, ch, threads: int = 0, build: bool = True, inner_solver: str = "lusgs"):
+    def __init__(self, ch, threads: int = 0, build: bool = True, inner_solver: str = "lusgs",
+                 flavor: str = "pin"):
         """inner_solver: "lusgs" (Dual_time_stepping, the reference's default)
-        or "dplur" (DPLUSGS.cpp, the call main.cpp:268-284 leaves commented)."""
+        or "dplur" (DPLUSGS.cpp, the call main.cpp:268-284 leaves commented).
+        flavor: "pin" (the build the oracle is pinned to) or "perf" (-O3, the
+        reference Makefile's flags, for timing)."""
         if inner_solver not in ("lusgs", "dplur"):
             raise ValueError(inner_solver)
         self.inner_solver = inner_solver
         params = build_ref.params_for(ch)
         if build:
-            path = build_ref.build(params, ch.name)
+            path = build_ref.build(params, ch.name, flavor=flavor)
         else:
-            path = os.path.join(os.path.dirname(__file__), "_ref", ch.name, "libref.so")
+            path = build_ref.lib_path(ch.name, flavor)
+        self.path = path
         self.lib = ctypes.CDLL(path)
         L = self.lib
         L.ref_array.restype = ctypes.POINTER(ctypes.c_double)

@@ -176,6 +176,33 @@ def test_c1_twenty_steps_match_reference_build(lib):
     assert max(errs) <= STEP_TOL
 
 
+@pytest.mark.skipif(not _ref_lib_present(Channel(256, 192, 192)),
+                    reason="reference build for 256x192x192 not present")
+def test_c2_twenty_steps_match_reference_build(lib):
+    """The plain-FP64-at-scale channel at its own size, 256 x 192 x 192
+    cells: 20 physical steps x 10 inner iterations on the GPU against the
+    reference's own CPU build (OpenMP on every host core, several minutes).
+    At this size the wavefront runs 32 x 12 tiles of 8 x 16 columns and the
+    channel's per-row metric tables are in use, as in the benchmark."""
+    from cgli_fu_flow_b200.solver import Solver
+    from oracle.refrun import RefSolver
+    ch = Channel(256, 192, 192)
+    g = Solver(ch)
+    g.init()
+    r = RefSolver(ch, threads=os.cpu_count() or 1, build=False)
+    r.init()
+    for _ in range(20):
+        g.step(10)
+        r.step(10)
+    reg = regions(ch)
+    sl = (slice(None),) + reg["cell"]
+    qg, qr = g.q()[sl], r.q()[sl]
+    errs = [rel_l2(qg[v], qr[v]) for v in range(5)]
+    print("C2 20-step relative L2 per variable:", errs)
+    g.close()
+    assert max(errs) <= STEP_TOL
+
+
 def test_extrapolated_predictor_matches_oracle(lib):
     """Second-order extrapolated initial guess: same states as the oracle
     with the same predictor."""

@@ -127,10 +127,21 @@ def test_force_controller_steers_toward_target():
 
 
 def test_wavefront_step_count():
-    """Hyperplane steps of one wavefront pass of 8 x 16 tiles (the profiling
-    runner's per-step figure): nz + 22 for one tile, plus 8 per extra tile
-    in x and 16 per extra tile in y (ragged tiles count whole)."""
+    """Dependent steps of one wavefront pass of ti x tj tiles (the profiling
+    runner's per-step figure): nz + ti + tj - 2 for one tile, plus ti per
+    extra tile in x and tj per extra tile in y (ragged tiles count whole)."""
     from cgli_fu_flow_b200.run import wavefront_steps
-    assert wavefront_steps(8, 16, 192) == 214
-    assert wavefront_steps(256, 192, 192) == 256 + 192 + 192 - 2
-    assert wavefront_steps(9, 17, 10) == 10 + 22 + 8 + 16
+    assert wavefront_steps(8, 16, 192, 8, 16) == 214
+    assert wavefront_steps(256, 192, 192, 8, 16) == 256 + 192 + 192 - 2
+    assert wavefront_steps(9, 17, 10, 8, 16) == 10 + 22 + 8 + 16
+    # other tile shapes the library can be built with
+    assert wavefront_steps(256, 192, 192, 16, 16) == 256 + 192 + 192 - 2
+    assert wavefront_steps(20, 20, 8, 16, 16) == 8 + 30 + 16 + 16
+    assert wavefront_steps(9, 40, 10, 8, 32) == 10 + 38 + 8 + 32
+
+
+def test_library_reports_its_tile_shape(cuda_lib):
+    """The tile shape comes from the library itself (set at build time)."""
+    from cgli_fu_flow_b200.solver import sweep_tile_shape
+    ti, tj = sweep_tile_shape()
+    assert ti >= 1 and tj >= 1 and (ti * tj) % 32 == 0
