@@ -72,7 +72,7 @@ struct cgli_ctx {
   long long sweep_passes = 0;
   cgli_cnn *cnn = nullptr;            // learned initial guess (not owned)
   std::vector<double> step_norms;     // the five norms of every inner iteration of the last step
-  double *stats = nullptr;            // [11][nx][ny] running sums (allocated on first use)
+  double *stats = nullptr;            // [CGLI_NSTATS][nx][ny] running sums and samples (allocated on first use)
   long long stat_samples = 0;
   cgli::FilterBufs fb;                // allocated on first use of the filter
   bool have_filter = false, have_ypoint = false;
@@ -844,7 +844,7 @@ int cgli_step_norms(cgli_ctx *c, double *norms, int max_iters, int *iters) {
 int cgli_statistics_accumulate(cgli_ctx *c) {
   int rc = check(c); if (rc) return rc;
   rc = need_ready(c); if (rc) return rc;
-  const size_t bytes = (size_t)11 * c->p.nx * c->p.ny * sizeof(double);
+  const size_t bytes = (size_t)CGLI_NSTATS * c->p.nx * c->p.ny * sizeof(double);
   if (!c->stats) { rc = alloc(c, bytes, (void **)&c->stats); if (rc) return rc; }
   cgli::launch_statistics(c->d, c->stream, c->stats);
   rc = last_launch("statistics"); if (rc) return rc;
@@ -856,7 +856,7 @@ int cgli_statistics_accumulate(cgli_ctx *c) {
 int cgli_statistics_get(cgli_ctx *c, double *sums, long long *samples) {
   int rc = check(c); if (rc) return rc;
   if (!sums || !samples) return fail(CGLI_EINVAL, "null argument");
-  const size_t bytes = (size_t)11 * c->p.nx * c->p.ny * sizeof(double);
+  const size_t bytes = (size_t)CGLI_NSTATS * c->p.nx * c->p.ny * sizeof(double);
   if (!c->stats) memset(sums, 0, bytes);
   else {
     CUDA_TRY(cudaMemcpyAsync(sums, c->stats, bytes, cudaMemcpyDeviceToHost, c->stream));
@@ -869,7 +869,7 @@ int cgli_statistics_get(cgli_ctx *c, double *sums, long long *samples) {
 int cgli_statistics_reset(cgli_ctx *c) {
   int rc = check(c); if (rc) return rc;
   if (c->stats) {
-    CUDA_TRY(cudaMemsetAsync(c->stats, 0, (size_t)11 * c->p.nx * c->p.ny * sizeof(double), c->stream));
+    CUDA_TRY(cudaMemsetAsync(c->stats, 0, (size_t)CGLI_NSTATS * c->p.nx * c->p.ny * sizeof(double), c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
   }
   c->stat_samples = 0;

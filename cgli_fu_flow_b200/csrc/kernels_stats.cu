@@ -1,14 +1,17 @@
 // Running statistics of Statistic.cpp:120-160: per (i, j) sums over k of
 // U, V, W, T, UU, VV, WW, TT, UV, UT, VT of the current U_, accumulated once
-// per call (once per physical step).  One CTA per (i, j) row, a fixed-order
-// reduction over k, so repeated runs give identical sums.
+// per call (once per physical step), and the instantaneous U and T of cell
+// k = 150 (:155-158; kept only when the row has that cell).  One CTA per
+// (i, j) row, a fixed-order reduction over k, so repeated runs give
+// identical sums.
 #include "cgli_dev.cuh"
 #include "cgli_launch.h"
 
 namespace cgli {
 namespace {
 
-constexpr int NSTAT = 11;
+constexpr int NSTAT = 11;   // accumulated quantities; two sampled ones follow
+constexpr int KSAMPLE = 150;  // reference k index of the instantaneous sample
 
 __global__ void k_statistics(Dev d, double *sums) {
   const int jl = blockIdx.x, il = blockIdx.y;     // interior row (0-based)
@@ -26,6 +29,10 @@ __global__ void k_statistics(Dev d, double *sums) {
     a[0] += U; a[1] += V; a[2] += W; a[3] += T;
     a[4] += U * U; a[5] += V * V; a[6] += W * W; a[7] += T * T;
     a[8] += U * V; a[9] += U * T; a[10] += V * T;
+    if (kl + 2 == KSAMPLE) {
+      sums[((long long)NSTAT * d.nx + il) * d.ny + jl] = U;
+      sums[((long long)(NSTAT + 1) * d.nx + il) * d.ny + jl] = T;
+    }
   }
   __shared__ double red[NSTAT][128];
 #pragma unroll

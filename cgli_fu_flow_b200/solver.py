@@ -379,14 +379,16 @@ class Solver:
             self.ctrl = dict(ctrl)
 
     STATS = ("U", "V", "W", "T", "UU", "VV", "WW", "TT", "UV", "UT", "VT")
+    SAMPLES = ("UI", "TI")      # instantaneous U and T at reference index k = 150
 
     def accumulate_statistics(self) -> None:
         """Adds the current level to the running sums (Statistic.cpp:120-160)."""
         self._rc(self.L.cgli_statistics_accumulate(self.h))
 
     def statistics(self) -> tuple[np.ndarray, int]:
-        """The running sums (11, Nx, Ny) and the number of accumulated steps."""
-        out = np.zeros((11, self.ch.nx, self.ch.ny))
+        """The running sums (11, Nx, Ny) followed by the two instantaneous
+        samples (13 rows in all), and the number of accumulated steps."""
+        out = np.zeros((len(self.STATS) + len(self.SAMPLES), self.ch.nx, self.ch.ny))
         n = ctypes.c_longlong()
         self._rc(self.L.cgli_statistics_get(self.h, out.ctypes.data, ctypes.byref(n)))
         return out, int(n.value)
@@ -398,7 +400,7 @@ class Solver:
         """Means over x, z and the accumulated steps, per wall-normal cell:
         the reference's (i, j) means (sums / (steps Nz)) averaged over i."""
         sums, n = self.statistics()
-        m = sums.mean(axis=1) / (max(n, 1) * self.ch.nz)
+        m = sums[:len(self.STATS)].mean(axis=1) / (max(n, 1) * self.ch.nz)
         return dict(zip(self.STATS, m))
 
     def copy_state_from(self, other: "Solver") -> None:

@@ -276,10 +276,14 @@ int cgli_set_learned_guess(cgli_ctx *ctx, cgli_cnn *cnn);
 
 /* ---- running statistics (replaces the accumulation of Statistic.cpp:120-160).
  * Each call adds, for every interior (i, j), the sums over k of U, V, W, T,
- * UU, VV, WW, TT, UV, UT, VT of the current U_ (call after each cgli_step);
- * cgli_statistics_get copies the sums [11][Nx][Ny] (quantity-major, i then j)
- * and the number of accumulated calls; the reference's means are the sums
- * divided by calls * Nz (Statistic.cpp:162-190). */
+ * UU, VV, WW, TT, UV, UT, VT of the current U_ (call after each cgli_step),
+ * and records the instantaneous U and T of the cell at reference index
+ * k = 150 (Statistic.cpp:155-158; zero where Nz < 149);
+ * cgli_statistics_get copies the [CGLI_NSTATS][Nx][Ny] values
+ * (quantity-major, i then j: the 11 sums, then U and T at k = 150) and the
+ * number of accumulated calls; the reference's means are the sums divided
+ * by calls * Nz (Statistic.cpp:162-190). */
+#define CGLI_NSTATS 13
 int cgli_statistics_accumulate(cgli_ctx *ctx);
 int cgli_statistics_get(cgli_ctx *ctx, double *sums, long long *samples);
 int cgli_statistics_reset(cgli_ctx *ctx);

@@ -44,7 +44,7 @@ SOURCES = [
     "Initial_condition.cpp", "X_boundary_condition.cpp", "Y_boundary_condition.cpp",
     "Z_boundary_condition.cpp", "Flux_X.cpp", "Flux_Y.cpp", "Flux_Z.cpp",
     "Viscous_terms.cpp", "Dual_time_stepping.cpp", "Driven_force.cpp", "Hyperplane.cpp",
-    "Filter.cpp", "DPLUSGS.cpp",
+    "Filter.cpp", "DPLUSGS.cpp", "Statistic.cpp",
 ]
 
 PATCHES = {

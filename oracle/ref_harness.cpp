@@ -82,6 +82,9 @@ void DPLUSGS(int, double, double *, double *, double *, double *, double *, doub
 void Driven_force(int, A3, A3);
 void Hyperplane(int, int (*)[2], int (*)[3]);
 void Filter(int, double, double, double, A3, A3, A3, A3, A3, A3, A3, A3, A3, A3);
+void Statistic(int, int, int, int, double, double, double, double, double, double,
+               A3, A3, A3, A3, A3, A3, A3, A3, A3, A3, A3, A3, A3, A3, A3, A3,
+               A3, A3, A3, A3, A3, A3, A3, A3, A3, A3, A3);
 
 namespace {
 
@@ -391,6 +394,18 @@ void ref_end_step(void) {
 void ref_filter(double roe_criterion, double e_high, double e_low) {
   A3 *q = A.U_;
   Filter(MYID, roe_criterion, e_high, e_low, q[0], q[1], q[2], q[3], q[4], A.Yp, A.EpX, A.EpY, A.EpZ, A.J);
+}
+
+/* Statistic.cpp:12-506 as main.cpp:334-342 calls it after a step: adds U_
+ * to the per-(i, j) sums over k; every statistic_step-th step it writes the
+ * means of the planes at x positions obs[0..4] to st_obs<n>_<step>.dat in the
+ * current directory (Statistic.cpp:120-331) and clears the sums. */
+void ref_statistic(int step, int statistic_step, const double *obs) {
+  A3 *q = A.U_, *mv = A.mv;
+  Statistic(MYID, step, 0, statistic_step, obs[0], obs[1], obs[2], obs[3], obs[4], g_e,
+            q[0], q[1], q[2], q[3], q[4], A.J, A.Jv,
+            mv[0], mv[1], mv[2], mv[3], mv[4], mv[5], mv[6], mv[7], mv[8],
+            A.MR[0], A.MR[1], A.MR[2], A.MR[3], A.MR[4], A.ML[0], A.ML[1], A.ML[2], A.ML[3], A.ML[4], A.EpY);
 }
 
 }  // extern "C"

@@ -46,6 +46,7 @@ class RefSolver:
         L.ref_bulk_flux.restype = ctypes.c_double
         L.ref_check_hyperplanes.restype = ctypes.c_long
         L.ref_filter.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        L.ref_statistic.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
         self.ch = ch
         dims = (ctypes.c_int * 6)()
         L.ref_dims(dims)
@@ -122,6 +123,32 @@ class RefSolver:
         self.array("Y_point")[...] = y_point
         self.lib.ref_filter(roe_criterion, e_high, e_low)
         return [self.array(n).copy() for n in ("EpX", "EpY", "EpZ")]
+
+    def statistic(self, step: int, statistic_step: int, planes: list[int]) -> dict | None:
+        """Statistic.cpp on the current U_ (call after each step).  On every
+        statistic_step-th step the reference writes, for up to five x planes,
+        the means over k and the accumulated steps of U, V, W, T, UU, VV, WW,
+        TT, UV, UT, VT and the instantaneous U, T at k = 150; returns
+        {plane i: array (13, Ny)} then, None otherwise.  Planes are the
+        slab's interior indices i = 3 .. Nx+2 (periodic slab only)."""
+        assert not self.ch.x_open and len(planes) <= 5
+        nx, ny = self.ch.nx, self.ch.ny
+        # the reference finds plane i where (ii-2) dx <= obs <= (ii-1) dx with
+        # ii = i + gstart of this rank (rank 1 of 3 equal slabs: gstart = Nx)
+        obs = [(i + nx - 1.5) * self.ch.dxi for i in planes] + [-1e30] * (5 - len(planes))
+        cwd = os.getcwd()
+        with tempfile.TemporaryDirectory() as td:
+            os.chdir(td)
+            try:
+                self.lib.ref_statistic(step, statistic_step, (ctypes.c_double * 5)(*obs))
+            finally:
+                os.chdir(cwd)
+            out = {}
+            for n, i in enumerate(planes, start=1):
+                path = os.path.join(td, f"st_obs{n}_{step:05d}.dat")
+                if os.path.exists(path):
+                    out[i] = np.loadtxt(path).reshape(13, ny)
+        return out or None
 
     def step(self, fixed_iters: int | None = 10, drop: float = 1e-3, cap: int = 30) -> tuple[int, np.ndarray]:
         """One physical step.  fixed_iters=N runs exactly N inner iterations;
