@@ -66,6 +66,16 @@ def parse():
     ap.add_argument("--skip", type=int, default=16, help="first steps (initial transient) not used for training")
     ap.add_argument("--train-steps", type=int, default=600)
     ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--tight-drop", type=float, default=1e-6,
+                    help="stopping rule of the arms' second matrix: the drop under which the converged state no "
+                         "longer depends on the predictor or the sweep precision")
+    ap.add_argument("--tight-cap", type=int, default=60)
+    ap.add_argument("--truth-drop", type=float, default=1e-10, help="the arms' reference run (FP64)")
+    ap.add_argument("--truth-cap", type=int, default=200)
+    ap.add_argument("--extras", action=argparse.BooleanOptionalAction, default=True,
+                    help="after the timed region, also run the 384x256x256 mixed-precision profile check and the "
+                         "wavy-wall workload (the line's `extras`)")
+    ap.add_argument("--extras-steps", type=int, default=100, help="steps of the 384x256x256 profile check")
     ap.add_argument("--profile-check", type=int, default=0, metavar="STEPS",
                     help="instead of timing: run FP64 and mixed STEPS steps each and compare the mean streamwise "
                          "velocity profiles over x, z and the steps (the mixed-precision acceptance criterion of the 384x256x256 channel: 0.5 %%)")
@@ -273,21 +283,31 @@ def run_gpu(a, dist: Dist) -> dict | None:
     return out
 
 
-def _timed_steps(sol, a, dist):
+def _timed_steps(sol, a, dist, drop=None, cap=None):
     iters = []
+    drop = a.drop if drop is None else drop
+    cap = a.cap if cap is None else cap
     dist.barrier()
     sol.event(0)
     for _ in range(a.steps):
-        it, _ = sol.step(None, a.drop, a.cap)
+        it, _ = sol.step(None, drop, cap)
         iters.append(it)
     sol.event(1)
     ms = dist.max(sol.elapsed_ms(0, 1))
     return ms, iters
 
 
+PREDICTORS = ("previous level", "extrapolation", "learned")
+
+
 def run_arms(a, ch, dist) -> dict:
-    """FP64 / mixed + extrapolation / mixed + learned guess from one point of
-    a run (module docstring)."""
+    """Precision x predictor from one common point of a run (module
+    docstring): FP64 and mixed precision, each with the previous-level,
+    extrapolated and learned initial guess, at the headline stopping rule
+    and at the tight rule; plus FP64 with the DP-LUR inner solver.  Every
+    arm runs the same W + K steps from the common point; its state after
+    them is compared with a reference run converged far below either rule
+    (FP64, previous-level guess, `--truth-drop`)."""
     from cgli_fu_flow_b200.cnn import (CNN_FLOP_PER_CELL, CNN_TC_FLOP_PER_CELL, Network, init_params,
                                        physical_levels, scales_from_levels)
     from cgli_fu_flow_b200.solver import FP64, MIXED, Solver
@@ -318,46 +338,65 @@ def run_arms(a, ch, dist) -> dict:
     loss = net.train(a.train_steps, a.lr, 20261203, 0, ntrain)
     train_s = time.perf_counter() - t0
     held = float(np.mean([net.pair_loss(p) for p in range(ntrain, npairs)]))
-    out = {"common_point": f"after {a.collect} steps from the seeded field (mixed precision, extrapolated guess)",
+    out = {"common_point": f"after {a.collect} steps from the seeded field (mixed precision, extrapolated guess, "
+                           f"headline rule)",
+           "steps_per_arm": f"{a.warmup} untimed + {a.steps} timed",
            "learned_guess": {"training_pairs": ntrain, "training_steps_of_run": [a.skip, a.collect],
                              "adam_steps": a.train_steps, "lr": a.lr,
                              "final_mean_loss": round(loss, 5), "held_out_loss_last_4_pairs": round(held, 5),
                              "collect_s": round(collect_s, 2), "train_s": round(train_s, 2),
                              "loss_unit": "mean squared extrapolation correction / its RMS (1.0 = extrapolation)"}}
-    sols = {}
-    for name, prec, pred in (("fp64", FP64, 0), ("mixed_extrapolation", MIXED, 1), ("mixed_learned", MIXED, 2),
-                             ("fp64_dplur", FP64, 0)):
+    sl = (slice(None), slice(3, ch.nx + 3), slice(2, ch.ny + 2), slice(2, ch.nz + 2))
+
+    def run(prec, pred, drop, cap, inner="lusgs"):
         s = Solver(ch, prec)
         s.copy_state_from(base)
         if pred == 2:
             s.set_learned_guess(net)
         s.set_predictor(pred)
-        if name == "fp64_dplur":
+        if inner == "dplur":
             s.set_inner_solver("dplur")
         for _ in range(a.warmup):
-            s.step(None, a.drop, a.cap)
-        ms, iters = _timed_steps(s, a, dist)
+            s.step(None, drop, cap)
+        ms, iters = _timed_steps(s, a, dist, drop, cap)
         value = dist.sum(float(ch.cells) * a.steps) / (ms / 1e3) / 1e6
-        out[name] = {"value": round(value, 3), "unit": "Mcell-steps/s", "ms_per_step": round(ms / a.steps, 3),
-                     "mean_inner_iterations": round(float(np.mean(iters)), 2), "inner_iterations": iters,
-                     "precision": "fp64" if prec == FP64 else "mixed", "predictor": ["previous level", "extrapolation",
-                                                                                     "learned"][pred],
-                     "inner_solver": "DP-LUR (DPLUSGS.cpp: 4 Jacobi relaxations; norms of squared "
-                                     "p, u, v, w, T increments)" if name == "fp64_dplur" else "LU-SGS"}
+        res = {"value": round(value, 3), "unit": "Mcell-steps/s", "ms_per_step": round(ms / a.steps, 3),
+               "mean_inner_iterations": round(float(np.mean(iters)), 2), "inner_iterations": iters,
+               "precision": "fp64" if prec == FP64 else "mixed", "predictor": PREDICTORS[pred],
+               "inner_solver": "DP-LUR (DPLUSGS.cpp: 4 Jacobi relaxations; norms of squared "
+                               "p, u, v, w, T increments)" if inner == "dplur" else "LU-SGS"}
         if pred == 2:
             inf_ms = net.time_inference(s, 3)
-            tf = ch.cells * CNN_TC_FLOP_PER_CELL / (inf_ms / 1e3) / 1e12
-            out[name]["inference"] = {"ms": round(inf_ms, 3), "tensor_tflops": round(tf, 1),
-                                      "real_tflops": round(ch.cells * CNN_FLOP_PER_CELL / (inf_ms / 1e3) / 1e12, 1)}
-        sols[name] = s
-    sl = (slice(None), slice(3, ch.nx + 3), slice(2, ch.ny + 2), slice(2, ch.nz + 2))
-    ref = sols["fp64"].q()[sl]
-    for name in ("mixed_extrapolation", "mixed_learned", "fp64_dplur"):
-        q = sols[name].q()[sl]
-        errs = [float(np.linalg.norm(q[v] - ref[v]) / np.linalg.norm(ref[v])) for v in range(5)]
-        out[name]["state_rel_l2_vs_fp64"] = max(errs)
-    for s in sols.values():
+            res["inference"] = {"ms": round(inf_ms, 3),
+                                "tensor_tflops": round(ch.cells * CNN_TC_FLOP_PER_CELL / (inf_ms / 1e3) / 1e12, 1),
+                                "real_tflops": round(ch.cells * CNN_FLOP_PER_CELL / (inf_ms / 1e3) / 1e12, 1)}
+        q = s.q()[sl]
         s.close()
+        return res, q
+
+    def rel(q, ref):
+        return max(float(np.linalg.norm(q[v] - ref[v]) / np.linalg.norm(ref[v])) for v in range(5))
+
+    truth, q_truth = run(FP64, 0, a.truth_drop, a.truth_cap)
+    out["truth"] = {"rule": f"drop {a.truth_drop:g}, cap {a.truth_cap}", "precision": "fp64",
+                    "predictor": "previous level", "mean_inner_iterations": truth["mean_inner_iterations"],
+                    "inner_iterations": truth["inner_iterations"]}
+    for rule, drop, cap in (("headline", a.drop, a.cap), ("tight", a.tight_drop, a.tight_cap)):
+        arms = {"rule": f"every norm below {drop:g} of its running maximum, cap {cap}"}
+        qs = {}
+        for prec in (FP64, MIXED):
+            for pred in (0, 1, 2):
+                name = f"{'fp64' if prec == FP64 else 'mixed'}_{['previous', 'extrapolation', 'learned'][pred]}"
+                arms[name], qs[name] = run(prec, pred, drop, cap)
+        if rule == "headline":
+            arms["fp64_dplur"], qs["fp64_dplur"] = run(FP64, 0, drop, cap, "dplur")
+        for name, q in qs.items():
+            arms[name]["state_rel_l2_vs_truth"] = rel(q, q_truth)
+            arms[name]["state_rel_l2_vs_fp64_previous"] = rel(q, qs["fp64_previous"])
+        base_v = arms["fp64_previous"]["value"]
+        arms["speedup_vs_fp64_previous"] = {n: round(arms[n]["value"] / base_v, 3)
+                                            for n in qs if n != "fp64_previous"}
+        out[rule] = arms
     base.close()
     net.close()
     return out
@@ -484,35 +523,67 @@ def run_reference(a, dist: Dist) -> dict | None:
                     "d2h_bytes_per_step": 0}}
 
 
-def run_profile_check(a) -> dict:
+def run_profile_check(ch, steps: int, drop: float, cap: int) -> dict:
     """Mean streamwise velocity profile of mixed precision against FP64 on
-    the same workload (each from the seeded field, same stopping rule), and
-    the final states' relative L2 difference."""
+    the same workload (each from the seeded field, same stopping rule, on-
+    device statistics every step), the final states' relative L2 difference
+    and each precision's throughput over the steps (CUDA events)."""
     from cgli_fu_flow_b200.solver import FP64, MIXED, Solver
-    ch = C.workload(a.workload)
-    prof, q, iters, secs = {}, {}, {}, {}
+    prof, q, iters, ms = {}, {}, {}, {}
     for name, prec in (("fp64", FP64), ("mixed", MIXED)):
         g = Solver(ch, prec)
         g.init()
         it = []
-        t0 = time.perf_counter()
-        for _ in range(a.profile_check):
-            n, _ = g.step(None, a.drop, a.cap)
+        g.event(0)
+        for _ in range(steps):
+            n, _ = g.step(None, drop, cap)
             it.append(n)
             g.accumulate_statistics()
-        secs[name] = time.perf_counter() - t0
+        g.event(1)
+        ms[name] = g.elapsed_ms(0, 1)
         prof[name] = g.mean_profiles()["U"]
         sl = (slice(None), slice(3, ch.nx + 3), slice(2, ch.ny + 2), slice(2, ch.nz + 2))
         q[name] = g.q()[sl]
-        iters[name] = float(np.mean(it))
+        iters[name] = it
         g.close()
     diff = float(np.abs(prof["mixed"] - prof["fp64"]).max() / ch.u_b)
     rel = [float(np.linalg.norm(q["mixed"][v] - q["fp64"][v]) / np.linalg.norm(q["fp64"][v])) for v in range(5)]
-    return {"check": "mean streamwise velocity profile over x, z and steps: mixed vs FP64",
-            "workload": f"channel {ch.nx}x{ch.ny}x{ch.nz}", "steps": a.profile_check,
+    return {"check": "mean streamwise velocity profile over x, z and the steps: mixed vs FP64 (criterion 0.5 % "
+                     "of U_b)", "workload": workload_label(ch), "steps": steps,
+            "rule": f"every norm below {drop:g} of its running maximum, cap {cap}",
             "max_profile_difference_over_u_b": diff, "criterion": 0.005, "passed": diff <= 0.005,
-            "state_rel_l2_mixed_vs_fp64": rel, "mean_inner_iterations": iters, "wall_s": secs,
-            "profile_fp64": [round(float(x), 6) for x in prof["fp64"]]}
+            "state_rel_l2_mixed_vs_fp64": max(rel), "state_rel_l2_mixed_vs_fp64_per_variable": rel,
+            "mean_inner_iterations": {k: round(float(np.mean(v)), 2) for k, v in iters.items()},
+            "value": {k: round(ch.cells * steps / (v / 1e3) / 1e6, 3) for k, v in ms.items()},
+            "unit": "Mcell-steps/s (statistics included)"}
+
+
+def run_wavy(a) -> dict:
+    """The curvilinear workload: FP64 and mixed precision on the wavy-wall
+    channel, W + K steps each from the seeded field at the headline rule,
+    throughput over the K timed steps and the final states' difference."""
+    from cgli_fu_flow_b200.solver import FP64, MIXED, Solver
+    ch = C.workload("c4")
+    out, q = {"workload": workload_label(ch)}, {}
+    for name, prec in (("fp64", FP64), ("mixed", MIXED)):
+        g = Solver(ch, prec)
+        g.init()
+        for _ in range(a.warmup):
+            g.step(None, a.drop, a.cap)
+        it = []
+        g.event(0)
+        for _ in range(a.steps):
+            n, _ = g.step(None, a.drop, a.cap)
+            it.append(n)
+        g.event(1)
+        ms = g.elapsed_ms(0, 1)
+        q[name] = g.q()[(slice(None), slice(3, ch.nx + 3), slice(2, ch.ny + 2), slice(2, ch.nz + 2))]
+        g.close()
+        out[name] = {"value": round(ch.cells * a.steps / (ms / 1e3) / 1e6, 3), "unit": "Mcell-steps/s",
+                     "mean_inner_iterations": round(float(np.mean(it)), 2), "inner_iterations": it}
+    out["state_rel_l2_mixed_vs_fp64"] = max(float(np.linalg.norm(q["mixed"][v] - q["fp64"][v]) /
+                                              np.linalg.norm(q["fp64"][v])) for v in range(5))
+    return out
 
 
 def main():
@@ -520,7 +591,7 @@ def main():
     dist = Dist()
     if a.profile_check:
         if dist.rank == 0:
-            print(json.dumps(run_profile_check(a)), flush=True)
+            print(json.dumps(run_profile_check(C.workload(a.workload), a.profile_check, a.drop, a.cap)), flush=True)
         dist.close()
         return
     try:
@@ -544,6 +615,11 @@ def main():
                 else:
                     out["cpu_baseline"] = {"value": None, "unit": "Mcell-steps/s", "cores": 0, "kind": "reference",
                                            "sample": "reference build missing"}
+            if out is not None and a.extras and dist.world == 1:
+                # the other two configurations, after the timed region
+                out["extras"] = {"mixed_384x256x256": run_profile_check(C.workload("c3"), a.extras_steps, a.drop,
+                                                                         a.cap),
+                                 "wavy_256x256x128": run_wavy(a)}
         if out is not None:
             print(json.dumps(out), flush=True)
     finally:

@@ -47,6 +47,16 @@
 #ifndef CGLI_SWEEP_MINBLOCKS
 #define CGLI_SWEEP_MINBLOCKS 1
 #endif
+// steps of records in flight: the ring holds this many steps' blocks, the
+// copy of step s + RING - 1 is issued at step s
+#ifndef CGLI_SWEEP_RING
+#define CGLI_SWEEP_RING 2
+#endif
+// backward pass: bring the forward result dQ of each step in with the
+// records' bulk copy (five 1-value-per-thread rows) instead of plain loads
+#ifndef CGLI_SWEEP_DQ_BULK
+#define CGLI_SWEEP_DQ_BULK 0
+#endif
 
 namespace cgli {
 
@@ -198,7 +208,7 @@ __device__ __forceinline__ void fetch_cell(const Dev &d, const SweepArgs &a, con
   x.slot = slot;
   // the record (and, forward, MR) arrive in shared memory with the CTA's
   // block of the step (k_sweep); backward, this cell's forward result
-  if (BACKWARD)
+  if (BACKWARD && !CGLI_SWEEP_DQ_BULK)
 #pragma unroll
     for (int v = 0; v < 5; v++) x.mr[v] = SweepPtrs<T>::dq(a)[v][slot];
   if (halo_edge) {
@@ -266,12 +276,16 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
   __shared__ T sy[2][TI][TJ][5];   // j-direction products
   __shared__ double s_jt[TJ], s_et[TJ];
   __shared__ int s_tile;
-  __shared__ __align__(8) uint64_t s_bar[2];
-  // the CTA's records of two steps: step s's TI*TJ slots are one contiguous
+  constexpr int RING = CGLI_SWEEP_RING;
+  constexpr bool DQB = BACKWARD && CGLI_SWEEP_DQ_BULK;
+  __shared__ __align__(8) uint64_t s_bar[RING];
+  // the CTA's records of RING steps: step s's TI*TJ slots are one contiguous
   // block of TI*TJ*CR_N words in the tile-skewed layout, brought in with one
-  // bulk copy a step ahead
+  // bulk copy RING - 1 steps ahead (backward, optionally followed by the five
+  // rows of the step's forward result dQ)
   extern __shared__ __align__(128) unsigned char s_dyn[];
   T *const s_rec = reinterpret_cast<T *>(s_dyn);
+  constexpr int kStage = TI * TJ * (CR_N + (DQB ? 5 : 0));   // words per ring stage
   const int il = threadIdx.x / TJ, jl = threadIdx.x % TJ;
   const int nti = (d.nx + TI - 1) / TI, ntj = (d.ny + TJ - 1) / TJ, ntiles = nti * ntj;
   if (threadIdx.x == 0) s_tile = (int)atomicAdd(a.ticket, 1u);
@@ -289,8 +303,8 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
     s_et[threadIdx.x] = (Met::kChannel && jj <= jn) ? a.etdytab[jj] : 0.0;
   }
   if (threadIdx.x == 0) {
-    tc::mbar_init(tc::smem_addr(&s_bar[0]), 1);
-    tc::mbar_init(tc::smem_addr(&s_bar[1]), 1);
+#pragma unroll
+    for (int r = 0; r < RING; r++) tc::mbar_init(tc::smem_addr(&s_bar[r]), 1);
     tc::mbar_fence_init();
   }
   __syncthreads();
@@ -298,15 +312,23 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
   const int S = Nz + TI - 1 + TJ - 1;
   const long long tile_base = (long long)tile * S * (TI * TJ);
   constexpr uint32_t kBlock = TI * TJ * CR_N * sizeof(T);
+  constexpr uint32_t kRow = TI * TJ * sizeof(T);
   const T *const crec = SweepPtrs<T>::cellrec(a);
   auto issue = [&](int step) {   // one thread
     const int sf = BACKWARD ? S - 1 - step : step;
-    const uint32_t bar = tc::smem_addr(&s_bar[step & 1]);
-    tc::mbar_expect_tx(bar, kBlock);
-    tc::bulk_load(tc::smem_addr(s_rec + (step & 1) * (TI * TJ * CR_N)), crec + (tile_base + (long long)sf * (TI * TJ)) * CR_N,
-                  kBlock, bar);
+    const int b = step % RING;
+    const uint32_t bar = tc::smem_addr(&s_bar[b]);
+    T *const dst = s_rec + b * kStage;
+    const long long slot0 = tile_base + (long long)sf * (TI * TJ);
+    tc::mbar_expect_tx(bar, kBlock + (DQB ? 5 * kRow : 0));
+    tc::bulk_load(tc::smem_addr(dst), crec + slot0 * CR_N, kBlock, bar);
+    if (DQB)
+#pragma unroll
+      for (int v = 0; v < 5; v++)
+        tc::bulk_load(tc::smem_addr(dst + TI * TJ * CR_N + v * TI * TJ), SweepPtrs<T>::dq(a)[v] + slot0, kRow, bar);
   };
-  if (threadIdx.x == 0) issue(0);
+  if (threadIdx.x == 0)
+    for (int r = 0; r < RING - 1 && r < S; r++) issue(r);
   const int pa = BACKWARD ? ta + 1 : ta - 1, pb = BACKWARD ? tb + 1 : tb - 1;
   const int tile_pa = pa * ntj + tb, tile_pb = ta * ntj + pb;
   const bool halo_edge = BACKWARD ? (i == ie) : (i == 3);
@@ -355,17 +377,23 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
     const int rel = BACKWARD ? s - (TI - 1 - il) - (TJ - 1 - jl) : s - il - jl;
     const int kl = BACKWARD ? Nz - 1 - rel : rel;
     // loads of the next cell go out first and land during the dependent part
-    if (threadIdx.x == 0 && s + 1 < S) issue(s + 1);   // buffer (s+1)&1 was last read before the previous barrier
+    // stage (s + RING - 1) % RING was last read at step s - 1, before the previous barrier
+    if (threadIdx.x == 0 && s + RING - 1 < S) issue(s + RING - 1);
     if (s + 1 < S) fetch_cell<TI, TJ, Met, BACKWARD, T>(d, a, s_et, il, jl, j, s + 1, S, tile_base, inside, halo_edge, nxt);
     else nxt.active = false;
     // this step's records (bounded wait; a timeout is reported like a tile's)
     int gave_up = 0;
-    if (!tc::mbar_wait(tc::smem_addr(&s_bar[s & 1]), (s >> 1) & 1, a.spin_limit)) {
+    if (!tc::mbar_wait(tc::smem_addr(&s_bar[s % RING]), (s / RING) & 1, a.spin_limit)) {
       atomicExch(d.status, CGLI_TIMEOUT_CODE);
       gave_up = 1;
     }
-    if (cur.active)
-      load_cellrec(s_rec + (s & 1) * (TI * TJ * CR_N) + threadIdx.x * CR_N, cur.rec, BACKWARD ? (T *)nullptr : cur.mr);
+    if (cur.active) {
+      const T *st = s_rec + (s % RING) * kStage;
+      load_cellrec(st + threadIdx.x * CR_N, cur.rec, BACKWARD ? (T *)nullptr : cur.mr);
+      if (DQB)
+#pragma unroll
+        for (int v = 0; v < 5; v++) cur.mr[v] = st[TI * TJ * CR_N + v * TI * TJ + threadIdx.x];
+    }
     if (cur.active) {
       const int pbuf = (s - 1) & 1;
       T tx[5], ty[5];
@@ -479,10 +507,8 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
       // a wait of this step gave up: wait (bounded) for the record copies
       // still in flight into this CTA's shared memory, then stop; the
       // consumers of this tile's products give up on it in turn
-      if (threadIdx.x == 0) {
-        tc::mbar_wait(tc::smem_addr(&s_bar[s & 1]), (s >> 1) & 1, kDrainPolls);
-        if (s + 1 < S) tc::mbar_wait(tc::smem_addr(&s_bar[(s + 1) & 1]), ((s + 1) >> 1) & 1, kDrainPolls);
-      }
+      if (threadIdx.x == 0)
+        for (int r = s; r < s + RING && r < S; r++) tc::mbar_wait(tc::smem_addr(&s_bar[r % RING]), (r / RING) & 1, kDrainPolls);
       return;
     }
   }
@@ -528,6 +554,12 @@ __global__ void __launch_bounds__(128) k_update_skewed(Dev d, SweepArgs a) {
   block_sum5(acc, d.partial + 5 * ((long long)blockIdx.y * gridDim.x + blockIdx.x));
 }
 
+// dynamic shared memory of a wavefront pass: the ring of record stages
+template <int TI, int TJ, typename T>
+constexpr int sweep_smem_bytes(bool backward) {
+  return CGLI_SWEEP_RING * TI * TJ * (CR_N + (backward && CGLI_SWEEP_DQ_BULK ? 5 : 0)) * (int)sizeof(T);
+}
+
 // tickets follow the anti-diagonals ta + tb of the tile grid
 void sweep_tile_order(int nti, int ntj, std::vector<int> &order) {
   order.clear();
@@ -554,10 +586,10 @@ static void run_sweeps(const Dev &d, const SweepArgs &a, cudaStream_t s) {
       const dim3 hg((d.nz + 63) / 64, d.ny);
       if (pass == 0) {
         k_halo_products<Met, false, T><<<hg, 64, 0, s>>>(d, f);
-        k_sweep<TI, TJ, Met, false, T><<<ntiles, TI * TJ, 2 * TI * TJ * CR_N * sizeof(T), s>>>(d, f);
+        k_sweep<TI, TJ, Met, false, T><<<ntiles, TI * TJ, sweep_smem_bytes<TI, TJ, T>(false), s>>>(d, f);
       } else {
         k_halo_products<Met, true, T><<<hg, 64, 0, s>>>(d, b);
-        k_sweep<TI, TJ, Met, true, T><<<ntiles, TI * TJ, 2 * TI * TJ * CR_N * sizeof(T), s>>>(d, b);
+        k_sweep<TI, TJ, Met, true, T><<<ntiles, TI * TJ, sweep_smem_bytes<TI, TJ, T>(true), s>>>(d, b);
       }
     }
   }
@@ -576,10 +608,10 @@ static void run_one_pass(const Dev &d, const SweepArgs &a, cudaStream_t s, bool 
   const dim3 hg((d.nz + 63) / 64, d.ny);
   if (!backward) {
     k_halo_products<Met, false, T><<<hg, 64, 0, s>>>(d, b);
-    k_sweep<TI, TJ, Met, false, T><<<ntiles, TI * TJ, 2 * TI * TJ * CR_N * sizeof(T), s>>>(d, b);
+    k_sweep<TI, TJ, Met, false, T><<<ntiles, TI * TJ, sweep_smem_bytes<TI, TJ, T>(false), s>>>(d, b);
   } else {
     k_halo_products<Met, true, T><<<hg, 64, 0, s>>>(d, b);
-    k_sweep<TI, TJ, Met, true, T><<<ntiles, TI * TJ, 2 * TI * TJ * CR_N * sizeof(T), s>>>(d, b);
+    k_sweep<TI, TJ, Met, true, T><<<ntiles, TI * TJ, sweep_smem_bytes<TI, TJ, T>(true), s>>>(d, b);
   }
   if (final_pass) k_update_skewed<T><<<dim3(d.ny, d.nx), 128, 0, s>>>(d, a);
 }
@@ -598,11 +630,12 @@ void launch_sweep_pass(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mi
 // two-step record buffer) exceeds 48 KB: opt in once, outside any capture
 template <class Met, typename T>
 static cudaError_t opt_in() {
-  const int dyn = 2 * SWEEP_TI * SWEEP_TJ * CR_N * sizeof(T);   // two steps' records
   cudaError_t e = cudaFuncSetAttribute(k_sweep<SWEEP_TI, SWEEP_TJ, Met, false, T>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       sweep_smem_bytes<SWEEP_TI, SWEEP_TJ, T>(false));
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_sweep<SWEEP_TI, SWEEP_TJ, Met, true, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+    e = cudaFuncSetAttribute(k_sweep<SWEEP_TI, SWEEP_TJ, Met, true, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             sweep_smem_bytes<SWEEP_TI, SWEEP_TJ, T>(true));
   return e;
 }
 cudaError_t sweep_kernel_attributes() {

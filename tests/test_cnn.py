@@ -153,21 +153,23 @@ def _lockstep_channel():
 
 @pytest.mark.gpu
 def test_training_on_solver_levels_and_ab_against_extrapolation():
-    """Two identical FP64 solvers step the seeded channel with second-order
-    extrapolation while the network stores the converged levels; the
-    network is trained on the GPU (Adam, own kernels) on those pairs; then
-    solver B switches to the learned guess.  On the held-out steps the
-    learned guess must be closer to the converged Q^(n+1) than
-    extrapolation; the inner-iteration counts of both are reported."""
+    """Solver A steps the seeded channel with second-order extrapolation
+    while the network stores its converged levels; the network is trained
+    on the GPU (Adam, own kernels) on those pairs.  Then, on held-out steps,
+    a second solver B is set to A's state before every step (same levels,
+    norm maxima and force) and takes the same step with the learned guess:
+    an A/B test of the initial guess alone.  The learned guess must be
+    closer to the converged Q^(n+1) than extrapolation and must need fewer
+    inner iterations in total to reach the same stopping rule (every norm
+    below 1e-3 of its running maximum)."""
     from cgli_fu_flow_b200 import build
     from cgli_fu_flow_b200.cnn import Network, init_params, physical_levels, scales_from_levels
     from cgli_fu_flow_b200.solver import Solver
     build.build()
     ch = _lockstep_channel()
     A, B = Solver(ch), Solver(ch)
-    for s in (A, B):
-        s.init()
-        s.set_predictor(1)
+    A.init()
+    A.set_predictor(1)
     net = Network(ch.nx, ch.ny, ch.nz)
     net.reserve_levels(64)
     net.set_params(init_params(0))
@@ -175,7 +177,6 @@ def test_training_on_solver_levels_and_ab_against_extrapolation():
     warm, train_steps = 8, 48
     for k in range(warm + train_steps):
         A.step(None, 1e-3, 30)
-        B.step(None, 1e-3, 30)
         if k >= warm:
             net.push_level(A)
             host_levels.append(physical_levels(A))
@@ -187,18 +188,14 @@ def test_training_on_solver_levels_and_ab_against_extrapolation():
     print(f"training pairs {npairs}: loss {loss0:.4f} -> {loss1:.4f} (last mean {loss:.4f})")
     assert loss1 < 0.7 * loss0
     B.set_learned_guess(net)
-    B.set_predictor(2)
-    it_a, it_b, held_cnn, held_ext, saved = [], [], [], [], []
+    it_a, it_b, held_cnn, held_ext = [], [], [], []
     for k in range(12):
-        na, _ = A.step(None, 1e-3, 30)
+        B.copy_state_from(A)
+        B.set_predictor(2)
         nb, _ = B.step(None, 1e-3, 30)
+        na, _ = A.step(None, 1e-3, 30)
         it_a.append(na)
         it_b.append(nb)
-        # iterations the learned guess needs to reach the accuracy (all five
-        # update norms) that extrapolation reached at its last iteration
-        ea, eb = A.step_norms(), B.step_norms()
-        reach = np.nonzero(np.all(eb <= ea[-1] * (1 + 1e-12), axis=1))[0]
-        saved.append(len(ea) - (reach[0] + 1) if reach.size else 0)
         net.push_level(A)
         p = net.levels - 4
         held_cnn.append(net.pair_loss(p))
@@ -208,7 +205,9 @@ def test_training_on_solver_levels_and_ab_against_extrapolation():
         r = (q[3] - (3 * q[2] - 3 * q[1] + q[0])) / osc[:, None, None, None]
         held_ext.append(float(np.mean(r * r)))
     print("held-out guess MSE (normalised): learned", np.mean(held_cnn), "extrapolation", np.mean(held_ext))
-    print("inner iterations: extrapolation", it_a, "learned", it_b)
-    print("iterations saved at equal update norms:", saved)
+    print("inner iterations from the same states: extrapolation", it_a, "learned", it_b)
     assert np.mean(held_cnn) < 0.9 * np.mean(held_ext)
-    assert sum(saved) >= 0
+    assert sum(it_b) < sum(it_a), (it_a, it_b)
+    for s in (A, B):
+        s.close()
+    net.close()
