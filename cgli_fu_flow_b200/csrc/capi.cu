@@ -352,12 +352,6 @@ int cgli_create(const cgli_params *p, cgli_ctx **out) {
     if (rc == CGLI_OK) rc = alloc(c, xb, mixed ? (void **)&a.xbuff : (void **)&a.xbuf);
     if (rc == CGLI_OK) rc = alloc(c, yb, mixed ? (void **)&a.ybuff : (void **)&a.ybuf);
     if (rc == CGLI_OK) rc = alloc(c, 64, (void **)&a.ticket);
-    std::vector<int> order;
-    cgli::sweep_tile_order(nti, ntj, order);
-    int *dorder = nullptr;
-    if (rc == CGLI_OK) rc = alloc(c, sizeof(int) * order.size(), (void **)&dorder);
-    if (rc == CGLI_OK) cudaMemcpy(dorder, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice);
-    a.order = dorder;
     double *jt = nullptr, *et = nullptr;
     if (rc == CGLI_OK) rc = alloc(c, sizeof(double) * d.Y, (void **)&jt);
     if (rc == CGLI_OK) rc = alloc(c, sizeof(double) * d.Y, (void **)&et);
@@ -367,6 +361,19 @@ int cgli_create(const cgli_params *p, cgli_ctx **out) {
   if (rc == CGLI_OK) {
     cudaError_t e = cgli::sweep_kernel_attributes();
     if (e != cudaSuccess) rc = fail(CGLI_ECUDA, std::string("sweep kernel attributes: ") + cudaGetErrorString(e));
+  }
+  if (rc == CGLI_OK) {
+    // wavefront clusters along x, and the tickets' order of the cluster
+    // rows (anti-diagonals of the grid of clusters)
+    const int nti = (p->nx + cgli::SWEEP_TI - 1) / cgli::SWEEP_TI, ntj = (p->ny + cgli::SWEEP_TJ - 1) / cgli::SWEEP_TJ;
+    cgli::SweepArgs &a = c->sw;
+    a.cluster_x = cgli::sweep_cluster_x(nti, ntj, CGLI_SWEEP_CLUSTER_MAX);
+    std::vector<int> order;
+    cgli::sweep_tile_order(nti / a.cluster_x, ntj, order);
+    int *dorder = nullptr;
+    rc = alloc(c, sizeof(int) * order.size(), (void **)&dorder);
+    if (rc == CGLI_OK) cudaMemcpy(dorder, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice);
+    a.order = dorder;
   }
   if (rc == CGLI_OK && cudaMallocHost(&c->h_norms, 16 * sizeof(double)) != cudaSuccess)
     rc = fail(CGLI_ENOMEM, "cudaMallocHost");

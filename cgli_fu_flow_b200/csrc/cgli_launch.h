@@ -15,6 +15,10 @@ constexpr int CR_MR = REC_N;
 
 // tile shape of the wavefront sweeps: TI x TJ (i, j) columns per CTA (one
 // thread each, so TI * TJ <= 1024 and a multiple of 32)
+// largest cluster of wavefront CTAs along x (1: no clusters)
+#ifndef CGLI_SWEEP_CLUSTER_MAX
+#define CGLI_SWEEP_CLUSTER_MAX 1
+#endif
 #ifndef CGLI_SWEEP_TI
 #define CGLI_SWEEP_TI 8
 #endif
@@ -52,6 +56,7 @@ struct SweepArgs {
   const double *Jtab, *etdytab;   // per-j metrics of a grid uniform in x and z
   int channel_metrics;            // 1: use Jtab / etdytab instead of the 3-D arrays
   int spin_limit;                 // bounded wait (polls) for a neighbouring tile
+  int cluster_x;                  // wavefront CTAs per cluster along x (1: no clusters)
 };
 
 // slot of cell (i, j, k) in the tile-skewed layout
@@ -71,6 +76,7 @@ __host__ __device__ __forceinline__ long long skew_size(const Dev &d) {
 void sweep_tile_order(int nti, int ntj, std::vector<int> &order);
 // shared-memory opt-in of the wavefront kernels (once per process and device)
 cudaError_t sweep_kernel_attributes();
+int sweep_cluster_x(int nti, int ntj, int max_cx);
 // the four wavefront passes (two sweeps) of one inner iteration
 void launch_sweeps(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed);
 // the update and norm partials after the last pass (k_update_skewed)

@@ -30,6 +30,16 @@
 // Tiles take tickets in an order where every dependency holds a smaller
 // ticket, so a waiting CTA only ever waits on CTAs that are already running.
 //
+// Thread-block clusters (SweepArgs::cluster_x > 1): the CTAs of a cluster
+// are consecutive tiles along x, launched together.  Inside a cluster the
+// x hand-over is pushed, not pulled: the producing tile stores the products
+// of its edge row straight into the consuming tile's shared-memory ring
+// (distributed shared memory) and arrives on that slot's mbarrier there;
+// the consumer waits on its own barrier and gives the slot back with an
+// arrival on the producer's "empty" barrier.  The first (last) tile of a
+// cluster still receives (sends) through the global buffers.  A cluster
+// takes one ticket for its whole row of tiles.
+//
 // The periodic x halo keeps the reference's lag: the forward pass at i = 3
 // uses dQ of plane Nx+2 as it was at the start of the sweep (halo_f), the
 // backward pass at i = Nx+2 uses dQ of plane 3 (halo_b).  The backward pass of
@@ -276,6 +286,9 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
   __shared__ T sy[2][TI][TJ][5];   // j-direction products
   __shared__ double s_jt[TJ], s_et[TJ];
   __shared__ int s_tile;
+  // x hand-over ring inside a cluster: RX steps x TJ lanes x XW words
+  constexpr int RX = 8, XW = sizeof(T) == 8 ? 6 : 8;
+  __shared__ __align__(8) uint64_t s_full[RX], s_empty[RX];
   constexpr int RING = CGLI_SWEEP_RING;
   constexpr bool DQB = BACKWARD && CGLI_SWEEP_DQ_BULK;
   __shared__ __align__(8) uint64_t s_bar[RING];
@@ -286,14 +299,36 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
   extern __shared__ __align__(128) unsigned char s_dyn[];
   T *const s_rec = reinterpret_cast<T *>(s_dyn);
   constexpr int kStage = TI * TJ * (CR_N + (DQB ? 5 : 0));   // words per ring stage
+  T *const s_rx = s_rec + RING * kStage;   // the cluster ring follows the record ring
   const int il = threadIdx.x / TJ, jl = threadIdx.x % TJ;
-  const int nti = (d.nx + TI - 1) / TI, ntj = (d.ny + TJ - 1) / TJ, ntiles = nti * ntj;
-  if (threadIdx.x == 0) s_tile = (int)atomicAdd(a.ticket, 1u);
-  __syncthreads();
+  const int nti = (d.nx + TI - 1) / TI, ntj = (d.ny + TJ - 1) / TJ;
+  // cluster of ncl consecutive x tiles (1 without clusters): one ticket per
+  // cluster, taken by its first CTA and written into every CTA's s_tile
+  const uint32_t ncl = tc::cluster_nctarank(), crank = tc::cluster_ctarank();
+  const int nunits = (nti / (int)ncl) * ntj;
+  if (threadIdx.x == 0) {
+    if (ncl == 1) {
+      s_tile = (int)atomicAdd(a.ticket, 1u);
+    } else if (crank == 0) {
+      const uint32_t t = atomicAdd(a.ticket, 1u);
+      for (uint32_t r = 0; r < ncl; r++) tc::st_cluster_u32(tc::mapa(tc::smem_addr(&s_tile), r), t);
+    }
+#pragma unroll
+    for (int r = 0; r < RX; r++) {
+      tc::mbar_init(tc::smem_addr(&s_full[r]), TJ);
+      tc::mbar_init(tc::smem_addr(&s_empty[r]), 1);
+    }
+#pragma unroll
+    for (int r = 0; r < RING; r++) tc::mbar_init(tc::smem_addr(&s_bar[r]), 1);
+    tc::mbar_fence_init();
+  }
+  // tickets and barriers visible cluster-wide before any remote access
+  if (ncl > 1) tc::cluster_sync(); else __syncthreads();
   const int ticket = s_tile;
-  if (ticket >= ntiles) return;
-  const int tile = a.order[BACKWARD ? ntiles - 1 - ticket : ticket];
-  const int ta = tile / ntj, tb = tile % ntj;
+  if (ncl == 1 && ticket >= nunits) return;   // (a cluster's ticket is always in range)
+  const int unit = a.order[BACKWARD ? nunits - 1 - ticket : ticket];
+  const int ta = (unit / ntj) * (int)ncl + (int)crank, tb = unit % ntj;
+  const int tile = ta * ntj + tb;
   const int ie = d.nx + 2, jn = d.ny + 1;
   const int i = 3 + ta * TI + il, j = 2 + tb * TJ + jl;
   const bool inside = (i <= ie) && (j <= jn);
@@ -301,11 +336,6 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
     int jj = 2 + tb * TJ + threadIdx.x;
     s_jt[threadIdx.x] = (Met::kChannel && jj <= jn) ? a.Jtab[jj] : 1.0;
     s_et[threadIdx.x] = (Met::kChannel && jj <= jn) ? a.etdytab[jj] : 0.0;
-  }
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int r = 0; r < RING; r++) tc::mbar_init(tc::smem_addr(&s_bar[r]), 1);
-    tc::mbar_fence_init();
   }
   __syncthreads();
   const int Nz = d.nz;
@@ -337,6 +367,13 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
   const bool wall_y = BACKWARD ? (j == jn) : (j == 2);
   const bool send_x = BACKWARD ? (il == 0) : (il == TI - 1);
   const bool send_y = BACKWARD ? (jl == 0) : (jl == TJ - 1);
+  // x hand-over inside the cluster: received from / sent to the neighbouring
+  // CTA's shared memory; at the cluster's ends through the global buffers
+  const bool dsm_recv = ncl > 1 && (BACKWARD ? crank + 1 < ncl : crank > 0);
+  const bool dsm_send = ncl > 1 && (BACKWARD ? crank > 0 : crank + 1 < ncl);
+  const uint32_t producer = BACKWARD ? crank + 1 : crank - 1, consumer = BACKWARD ? crank - 1 : crank + 1;
+  // the step q of the consumer's wait is the producer's step q + TI - 1
+  const int QN = S - TI + 1;   // hand-over steps per pass
   const T rdx = (T)(1.0 / d.dxi), rdy = (T)(1.0 / d.det), rdz = (T)(1.0 / d.dzt);
   T *xb = SweepPtrs<T>::xb(a), *yb = SweepPtrs<T>::yb(a);
   T *const *dq = SweepPtrs<T>::dq(a);
@@ -353,7 +390,7 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
   };
   const T *xsrc = xb + ((long long)tile_pa * TJ + jl) * Nz * 5;
   const T *ysrc = yb + ((long long)tile_pb * TI + il) * Nz * 5;
-  const bool pre_x = recv_x, pre_y = recv_y && !wall_y;
+  const bool pre_x = recv_x && !dsm_recv, pre_y = recv_y && !wall_y;
   T px0[5], px1[5], py0[5], py1[5];
   auto preload = [&](int step, T *px, T *py) {
     const int k2 = kl_of(step);
@@ -376,6 +413,10 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
   for (int s = 0; s < S; s++) {
     const int rel = BACKWARD ? s - (TI - 1 - il) - (TJ - 1 - jl) : s - il - jl;
     const int kl = BACKWARD ? Nz - 1 - rel : rel;
+    // the slot read in step s - 1 is free again (every receiving lane read it
+    // before the barrier that ended that step)
+    if (dsm_recv && threadIdx.x == 0 && s >= 1 && s - 1 < QN)
+      tc::mbar_arrive_cluster(tc::mapa(tc::smem_addr(&s_empty[(s - 1) % RX]), producer));
     // loads of the next cell go out first and land during the dependent part
     // stage (s + RING - 1) % RING was last read at step s - 1, before the previous barrier
     if (threadIdx.x == 0 && s + RING - 1 < S) issue(s + RING - 1);
@@ -394,6 +435,7 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
 #pragma unroll
         for (int v = 0; v < 5; v++) cur.mr[v] = st[TI * TJ * CR_N + v * TI * TJ + threadIdx.x];
     }
+    T ox[5];
     if (cur.active) {
       const int pbuf = (s - 1) & 1;
       T tx[5], ty[5];
@@ -404,6 +446,15 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
         const int sil = BACKWARD ? il + 1 : il - 1;
 #pragma unroll
         for (int v = 0; v < 5; v++) tx[v] = sx[pbuf][sil][jl][v];
+      } else if (dsm_recv) {
+        // pushed by the producing CTA of the cluster (step s < QN here)
+        if (!tc::mbar_wait_cluster(tc::smem_addr(&s_full[s % RX]), (s / RX) & 1, a.spin_limit)) {
+          atomicExch(d.status, CGLI_TIMEOUT_CODE);
+          gave_up = 1;
+        }
+        const T *src = s_rx + ((s % RX) * TJ + jl) * XW;
+#pragma unroll
+        for (int v = 0; v < 5; v++) tx[v] = src[v];
       } else {
         bool ok = true;
 #pragma unroll
@@ -448,7 +499,7 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
       const long long c = Met::kChannel ? 0 : ix(d, i, j, 2 + kl);
       T mm[9];
       Met::template dirs<T>(d, s_et, c, jl, mm);
-      T ox[5], oy[5];
+      T oy[5];
       if (Met::kChannel) {
         // the channel's face metrics have one nonzero component per
         // direction (1, etdy, 1 on the x, y, z components), so only the
@@ -473,7 +524,7 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
       const int cb = s & 1;
 #pragma unroll
       for (int v = 0; v < 5; v++) { sx[cb][il][jl][v] = ox[v]; sy[cb][il][jl][v] = oy[v]; }
-      if (send_x) {
+      if (send_x && !dsm_send) {
         T *dst = xb + (((long long)tile * TJ + jl) * Nz + kl) * 5;
 #pragma unroll
         for (int v = 0; v < 5; v++) __stcg(dst + v, ox[v]);
@@ -497,6 +548,27 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
         }
       }
     }
+    if (dsm_send && send_x && s >= TI - 1) {
+      const int q = s - (TI - 1);
+      // the slot's previous use must have been read by the consumer
+      if (q >= RX && !tc::mbar_wait_cluster(tc::smem_addr(&s_empty[q % RX]), ((q / RX) - 1) & 1, a.spin_limit)) {
+        atomicExch(d.status, CGLI_TIMEOUT_CODE);
+        gave_up = 1;
+      } else {
+        if (cur.active) {
+          const uint32_t dst = tc::mapa(tc::smem_addr(s_rx + ((q % RX) * TJ + jl) * XW), consumer);
+          if (sizeof(T) == 8) {
+            tc::st_cluster_v2(dst, (double)ox[0], (double)ox[1]);
+            tc::st_cluster_v2(dst + 16, (double)ox[2], (double)ox[3]);
+            tc::st_cluster(dst + 32, (double)ox[4]);
+          } else {
+            tc::st_cluster_v4(dst, (float)ox[0], (float)ox[1], (float)ox[2], (float)ox[3]);
+            tc::st_cluster(dst + 16, (float)ox[4]);
+          }
+        }
+        tc::mbar_arrive_cluster(tc::mapa(tc::smem_addr(&s_full[q % RX]), consumer));
+      }
+    }
     if (pre_x || pre_y) {
 #pragma unroll
       for (int v = 0; v < 5; v++) { px0[v] = px1[v]; py0[v] = py1[v]; }
@@ -509,9 +581,13 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
       // consumers of this tile's products give up on it in turn
       if (threadIdx.x == 0)
         for (int r = s; r < s + RING && r < S; r++) tc::mbar_wait(tc::smem_addr(&s_bar[r % RING]), (r / RING) & 1, kDrainPolls);
+      // the cluster's CTAs leave together: none may leave while another
+      // can still write into its shared memory
+      if (ncl > 1) tc::cluster_sync();
       return;
     }
   }
+  if (ncl > 1) tc::cluster_sync();
 }
 
 // Dual_time_stepping.cpp:1702-1743 after the last backward pass: the
@@ -557,7 +633,8 @@ __global__ void __launch_bounds__(128) k_update_skewed(Dev d, SweepArgs a) {
 // dynamic shared memory of a wavefront pass: the ring of record stages
 template <int TI, int TJ, typename T>
 constexpr int sweep_smem_bytes(bool backward) {
-  return CGLI_SWEEP_RING * TI * TJ * (CR_N + (backward && CGLI_SWEEP_DQ_BULK ? 5 : 0)) * (int)sizeof(T);
+  return CGLI_SWEEP_RING * TI * TJ * (CR_N + (backward && CGLI_SWEEP_DQ_BULK ? 5 : 0)) * (int)sizeof(T) +
+         8 * TJ * (sizeof(T) == 8 ? 6 : 8) * (int)sizeof(T);   // the cluster's x hand-over ring
 }
 
 // tickets follow the anti-diagonals ta + tb of the tile grid
@@ -570,50 +647,44 @@ void sweep_tile_order(int nti, int ntj, std::vector<int> &order) {
     }
 }
 
-template <int TI, int TJ, class Met, typename T>
-static void run_sweeps(const Dev &d, const SweepArgs &a, cudaStream_t s) {
-  const int nti = (d.nx + TI - 1) / TI, ntj = (d.ny + TJ - 1) / TJ, ntiles = nti * ntj;
-  const size_t xbytes = (size_t)ntiles * TJ * d.nz * 5 * sizeof(T), ybytes = (size_t)ntiles * TI * d.nz * 5 * sizeof(T);
-  T *xb = sizeof(T) == 8 ? (T *)a.xbuf : (T *)a.xbuff;
-  T *yb = sizeof(T) == 8 ? (T *)a.ybuf : (T *)a.ybuff;
-  for (int sweep = 0; sweep < 2; sweep++) {
-    const SweepArgs &f = a, &b = a;
-    for (int pass = 0; pass < 2; pass++) {
-      // ticket reset and sentinel fill of the hand-over buffers
-      cudaMemsetAsync(a.ticket, 0, sizeof(unsigned int), s);
-      cudaMemsetAsync(xb, 0xff, xbytes, s);
-      cudaMemsetAsync(yb, 0xff, ybytes, s);
-      const dim3 hg((d.nz + 63) / 64, d.ny);
-      if (pass == 0) {
-        k_halo_products<Met, false, T><<<hg, 64, 0, s>>>(d, f);
-        k_sweep<TI, TJ, Met, false, T><<<ntiles, TI * TJ, sweep_smem_bytes<TI, TJ, T>(false), s>>>(d, f);
-      } else {
-        k_halo_products<Met, true, T><<<hg, 64, 0, s>>>(d, b);
-        k_sweep<TI, TJ, Met, true, T><<<ntiles, TI * TJ, sweep_smem_bytes<TI, TJ, T>(true), s>>>(d, b);
-      }
-    }
-  }
-}
-
+// One wavefront pass: ticket reset and sentinel fill of the hand-over
+// buffers, the halo products, then the pass itself (with the cluster
+// dimension a.cluster_x along x when it is above 1).
 template <int TI, int TJ, class Met, typename T>
 static void run_one_pass(const Dev &d, const SweepArgs &a, cudaStream_t s, bool backward, bool final_pass) {
   const int nti = (d.nx + TI - 1) / TI, ntj = (d.ny + TJ - 1) / TJ, ntiles = nti * ntj;
   const size_t xbytes = (size_t)ntiles * TJ * d.nz * 5 * sizeof(T), ybytes = (size_t)ntiles * TI * d.nz * 5 * sizeof(T);
   T *xb = sizeof(T) == 8 ? (T *)a.xbuf : (T *)a.xbuff;
   T *yb = sizeof(T) == 8 ? (T *)a.ybuf : (T *)a.ybuff;
-  const SweepArgs &b = a;
   cudaMemsetAsync(a.ticket, 0, sizeof(unsigned int), s);
   cudaMemsetAsync(xb, 0xff, xbytes, s);
   cudaMemsetAsync(yb, 0xff, ybytes, s);
   const dim3 hg((d.nz + 63) / 64, d.ny);
-  if (!backward) {
-    k_halo_products<Met, false, T><<<hg, 64, 0, s>>>(d, b);
-    k_sweep<TI, TJ, Met, false, T><<<ntiles, TI * TJ, sweep_smem_bytes<TI, TJ, T>(false), s>>>(d, b);
-  } else {
-    k_halo_products<Met, true, T><<<hg, 64, 0, s>>>(d, b);
-    k_sweep<TI, TJ, Met, true, T><<<ntiles, TI * TJ, sweep_smem_bytes<TI, TJ, T>(true), s>>>(d, b);
+  if (!backward) k_halo_products<Met, false, T><<<hg, 64, 0, s>>>(d, a);
+  else k_halo_products<Met, true, T><<<hg, 64, 0, s>>>(d, a);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(ntiles);
+  cfg.blockDim = dim3(TI * TJ);
+  cfg.dynamicSmemBytes = sweep_smem_bytes<TI, TJ, T>(backward);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  if (a.cluster_x > 1) {
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = a.cluster_x;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
   }
+  if (!backward) cudaLaunchKernelEx(&cfg, k_sweep<TI, TJ, Met, false, T>, d, a);
+  else cudaLaunchKernelEx(&cfg, k_sweep<TI, TJ, Met, true, T>, d, a);
   if (final_pass) k_update_skewed<T><<<dim3(d.ny, d.nx), 128, 0, s>>>(d, a);
+}
+
+template <int TI, int TJ, class Met, typename T>
+static void run_sweeps(const Dev &d, const SweepArgs &a, cudaStream_t s) {
+  for (int sweep = 0; sweep < 2; sweep++)
+    for (int pass = 0; pass < 2; pass++) run_one_pass<TI, TJ, Met, T>(d, a, s, pass == 1, false);
 }
 
 void launch_sweep_pass(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed, bool backward, bool final_pass) {
@@ -644,6 +715,35 @@ cudaError_t sweep_kernel_attributes() {
   if (e == cudaSuccess) e = opt_in<MetricsChannel, float>();
   if (e == cudaSuccess) e = opt_in<MetricsGeneral, float>();
   return e;
+}
+
+// The cluster size along x for a grid of nti x ntj tiles: the largest of
+// max_cx, max_cx/2, ... (at least 2) that divides nti and of which the
+// device can hold at least `need` clusters of the largest wavefront kernel
+// at once; 1 (no clusters) otherwise.
+int sweep_cluster_x(int nti, int ntj, int max_cx) {
+  for (int cx = max_cx; cx >= 2; cx /= 2) {
+    if (nti % cx) continue;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(nti * ntj);
+    cfg.blockDim = dim3(SWEEP_TI * SWEEP_TJ);
+    cfg.dynamicSmemBytes = sweep_smem_bytes<SWEEP_TI, SWEEP_TJ, double>(true);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cx;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, k_sweep<SWEEP_TI, SWEEP_TJ, MetricsGeneral, true, double>, &cfg) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    if (n >= 1) return cx;
+  }
+  return 1;
 }
 
 void launch_sweep_update(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed) {

@@ -44,6 +44,70 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int lim
   return false;
 }
 
+// ------------------------------------------- thread-block clusters (DSMEM)
+// A CTA's rank in its cluster and the cluster's size (1 without clusters).
+__device__ __forceinline__ uint32_t cluster_ctarank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t cluster_nctarank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+  return r;
+}
+// The shared::cluster address of the variable at shared::cta address `local`
+// in the shared memory of cluster CTA `rank`.
+__device__ __forceinline__ uint32_t mapa(uint32_t local, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(local), "r"(rank));
+  return r;
+}
+// Stores into another cluster CTA's shared memory (16-byte and 8 / 4-byte).
+__device__ __forceinline__ void st_cluster_v2(uint32_t addr, double x, double y) {
+  asm volatile("st.shared::cluster.v2.f64 [%0], {%1, %2};" ::"r"(addr), "d"(x), "d"(y) : "memory");
+}
+__device__ __forceinline__ void st_cluster(uint32_t addr, double x) {
+  asm volatile("st.shared::cluster.f64 [%0], %1;" ::"r"(addr), "d"(x) : "memory");
+}
+__device__ __forceinline__ void st_cluster_v4(uint32_t addr, float x, float y, float z, float w) {
+  asm volatile("st.shared::cluster.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "f"(x), "f"(y), "f"(z), "f"(w)
+               : "memory");
+}
+__device__ __forceinline__ void st_cluster(uint32_t addr, float x) {
+  asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(addr), "f"(x) : "memory");
+}
+// Arrival on an mbarrier in another cluster CTA's shared memory, releasing
+// this thread's earlier writes (its stores into that CTA included) at
+// cluster scope.
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t remote_bar) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(remote_bar) : "memory");
+}
+// Bounded wait on a local mbarrier whose arrivals come from other CTAs of the
+// cluster (acquire at cluster scope); false after `limit` polls.
+__device__ __forceinline__ bool mbar_wait_cluster(uint32_t bar, uint32_t parity, int limit) {
+  for (int n = 0; n < limit; n++) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if (n > 32) __nanosleep(64);
+  }
+  return false;
+}
+// The cluster-wide barrier (every thread of every CTA of the cluster).
+__device__ __forceinline__ void cluster_sync() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void st_cluster_u32(uint32_t addr, uint32_t v) {
+  asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+}
+
 // ------------------------------------------------------------------ TMA
 // Tiled 2-D / 4-D loads into this CTA's shared memory, completing on an
 // mbarrier; `map` is the generic address of a __grid_constant__ CUtensorMap.

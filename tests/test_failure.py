@@ -34,10 +34,13 @@ def lib(cuda_lib):
     return cuda_lib
 
 
-def test_wait_that_runs_out_reports_timeout_and_keeps_the_state(lib):
+@pytest.mark.parametrize("dims", [(24, 40, 16), (32, 40, 16)])
+def test_wait_that_runs_out_reports_timeout_and_keeps_the_state(lib, dims):
     from cgli_fu_flow_b200.solver import CgliError, Solver
-    # 3 x 3 tiles of the 8 x 16 wavefront: every kind of wait occurs
-    ch = Channel(24, 40, 16)
+    # 3 x 3 and 4 x 3 tiles of the 8 x 16 wavefront: every kind of wait
+    # occurs (with four tiles along x, also the waits inside a cluster of
+    # tiles when the library is built with clusters)
+    ch = Channel(*dims)
     g = Solver(ch)
     g.init()
     sl = interior(ch)
@@ -66,7 +69,7 @@ def test_wait_that_runs_out_reports_timeout_and_keeps_the_state(lib):
 
 def test_timeout_in_mixed_precision(lib):
     from cgli_fu_flow_b200.solver import MIXED, CgliError, Solver
-    ch = Channel(24, 40, 16)
+    ch = Channel(32, 40, 16)
     g = Solver(ch, MIXED)
     g.init()
     g.set_wait_limit(0)
