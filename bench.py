@@ -66,12 +66,12 @@ def parse():
     ap.add_argument("--skip", type=int, default=16, help="first steps (initial transient) not used for training")
     ap.add_argument("--train-steps", type=int, default=600)
     ap.add_argument("--lr", type=float, default=1e-3)
-    ap.add_argument("--tight-drop", type=float, default=1e-6,
+    ap.add_argument("--tight-drop", type=float, default=1e-9,
                     help="stopping rule of the arms' second matrix: the drop under which the converged state no "
                          "longer depends on the predictor or the sweep precision")
-    ap.add_argument("--tight-cap", type=int, default=60)
-    ap.add_argument("--truth-drop", type=float, default=1e-10, help="the arms' reference run (FP64)")
-    ap.add_argument("--truth-cap", type=int, default=200)
+    ap.add_argument("--tight-cap", type=int, default=200)
+    ap.add_argument("--truth-drop", type=float, default=1e-11, help="the arms' reference run (FP64)")
+    ap.add_argument("--truth-cap", type=int, default=250)
     ap.add_argument("--extras", action=argparse.BooleanOptionalAction, default=True,
                     help="after the timed region, also run the 384x256x256 mixed-precision profile check and the "
                          "wavy-wall workload (the line's `extras`)")
@@ -384,10 +384,13 @@ def run_arms(a, ch, dist) -> dict:
     for rule, drop, cap in (("headline", a.drop, a.cap), ("tight", a.tight_drop, a.tight_cap)):
         arms = {"rule": f"every norm below {drop:g} of its running maximum, cap {cap}"}
         qs = {}
-        for prec in (FP64, MIXED):
-            for pred in (0, 1, 2):
-                name = f"{'fp64' if prec == FP64 else 'mixed'}_{['previous', 'extrapolation', 'learned'][pred]}"
-                arms[name], qs[name] = run(prec, pred, drop, cap)
+        # the full matrix at the headline rule; at the tight rule the FP64
+        # path and the mixed path with either guess
+        matrix = [(p, g) for p in (FP64, MIXED) for g in (0, 1, 2)] if rule == "headline" else \
+            [(FP64, 0), (MIXED, 1), (MIXED, 2)]
+        for prec, pred in matrix:
+            name = f"{'fp64' if prec == FP64 else 'mixed'}_{['previous', 'extrapolation', 'learned'][pred]}"
+            arms[name], qs[name] = run(prec, pred, drop, cap)
         if rule == "headline":
             arms["fp64_dplur"], qs["fp64_dplur"] = run(FP64, 0, drop, cap, "dplur")
         for name, q in qs.items():

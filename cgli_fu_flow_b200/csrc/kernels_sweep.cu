@@ -30,15 +30,17 @@
 // Tiles take tickets in an order where every dependency holds a smaller
 // ticket, so a waiting CTA only ever waits on CTAs that are already running.
 //
-// Thread-block clusters (SweepArgs::cluster_x > 1): the CTAs of a cluster
-// are consecutive tiles along x, launched together.  Inside a cluster the
-// x hand-over is pushed, not pulled: the producing tile stores the products
-// of its edge row straight into the consuming tile's shared-memory ring
-// (distributed shared memory) and arrives on that slot's mbarrier there;
-// the consumer waits on its own barrier and gives the slot back with an
-// arrival on the producer's "empty" barrier.  The first (last) tile of a
-// cluster still receives (sends) through the global buffers.  A cluster
-// takes one ticket for its whole row of tiles.
+// Thread-block clusters (SweepArgs::cluster_x > 1, the CL instantiation):
+// the CTAs of a cluster are consecutive tiles along x, launched together.
+// Inside a cluster the x hand-over is pushed, not pulled: the producing
+// tile writes the products of its edge row straight into the consuming
+// tile's shared-memory ring with st.async, which counts the bytes on that
+// slot's mbarrier in the consumer (armed by the consumer with the bytes it
+// expects); the consumer waits on its own barrier and gives the slot back
+// with a relaxed arrival on the producer's "empty" barrier.  No fence is on
+// either path.  The first (last) tile of a cluster still receives (sends)
+// through the global buffers.  A cluster takes one ticket for its whole row
+// of tiles.
 //
 // The periodic x halo keeps the reference's lag: the forward pass at i = 3
 // uses dQ of plane Nx+2 as it was at the start of the sweep (halo_f), the
@@ -280,15 +282,16 @@ __device__ __forceinline__ void channel_products(const T r[REC_N], T m, const T 
   }
 }
 
-template <int TI, int TJ, class Met, bool BACKWARD, typename T>
+template <int TI, int TJ, class Met, bool BACKWARD, typename T, bool CL>
 __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, SweepArgs a) {
   __shared__ T sx[2][TI][TJ][5];   // i-direction products, double-buffered by step parity
   __shared__ T sy[2][TI][TJ][5];   // j-direction products
   __shared__ double s_jt[TJ], s_et[TJ];
   __shared__ int s_tile;
+  __shared__ int s_abort[2];   // a wait of step s gave up (slot s & 1)
   // x hand-over ring inside a cluster: RX steps x TJ lanes x XW words
   constexpr int RX = 8, XW = sizeof(T) == 8 ? 6 : 8;
-  __shared__ __align__(8) uint64_t s_full[RX], s_empty[RX];
+  __shared__ __align__(8) uint64_t s_full[CL ? RX : 1], s_empty[CL ? RX : 1];
   constexpr int RING = CGLI_SWEEP_RING;
   constexpr bool DQB = BACKWARD && CGLI_SWEEP_DQ_BULK;
   __shared__ __align__(8) uint64_t s_bar[RING];
@@ -304,28 +307,37 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
   const int nti = (d.nx + TI - 1) / TI, ntj = (d.ny + TJ - 1) / TJ;
   // cluster of ncl consecutive x tiles (1 without clusters): one ticket per
   // cluster, taken by its first CTA and written into every CTA's s_tile
-  const uint32_t ncl = tc::cluster_nctarank(), crank = tc::cluster_ctarank();
+  const uint32_t ncl = CL ? tc::cluster_nctarank() : 1u, crank = CL ? tc::cluster_ctarank() : 0u;
   const int nunits = (nti / (int)ncl) * ntj;
   if (threadIdx.x == 0) {
-    if (ncl == 1) {
+    if (!CL) {
       s_tile = (int)atomicAdd(a.ticket, 1u);
     } else if (crank == 0) {
       const uint32_t t = atomicAdd(a.ticket, 1u);
       for (uint32_t r = 0; r < ncl; r++) tc::st_cluster_u32(tc::mapa(tc::smem_addr(&s_tile), r), t);
     }
+    s_abort[0] = 0;
+    s_abort[1] = 0;
+    if (CL) {
 #pragma unroll
-    for (int r = 0; r < RX; r++) {
-      tc::mbar_init(tc::smem_addr(&s_full[r]), TJ);
-      tc::mbar_init(tc::smem_addr(&s_empty[r]), 1);
+      for (int r = 0; r < RX; r++) {
+        tc::mbar_init(tc::smem_addr(&s_full[r]), 1);    // the consumer's own arm per use
+        tc::mbar_init(tc::smem_addr(&s_empty[r]), 1);   // the consumer's release per use
+      }
+      // a receiving CTA arms its first RX slots with the bytes of one push
+      // before its producer can start (the cluster barrier below)
+      if (ncl > 1 && (BACKWARD ? crank + 1 < ncl : crank > 0))
+        for (int r = 0; r < RX && r < d.nz + TJ - 1; r++)
+          tc::mbar_expect_tx(tc::smem_addr(&s_full[r]), TJ * 5 * sizeof(T));
     }
 #pragma unroll
     for (int r = 0; r < RING; r++) tc::mbar_init(tc::smem_addr(&s_bar[r]), 1);
     tc::mbar_fence_init();
   }
   // tickets and barriers visible cluster-wide before any remote access
-  if (ncl > 1) tc::cluster_sync(); else __syncthreads();
+  if (CL) tc::cluster_sync(); else __syncthreads();
   const int ticket = s_tile;
-  if (ncl == 1 && ticket >= nunits) return;   // (a cluster's ticket is always in range)
+  if (!CL && ticket >= nunits) return;   // (a cluster's ticket is always in range)
   const int unit = a.order[BACKWARD ? nunits - 1 - ticket : ticket];
   const int ta = (unit / ntj) * (int)ncl + (int)crank, tb = unit % ntj;
   const int tile = ta * ntj + tb;
@@ -369,11 +381,12 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
   const bool send_y = BACKWARD ? (jl == 0) : (jl == TJ - 1);
   // x hand-over inside the cluster: received from / sent to the neighbouring
   // CTA's shared memory; at the cluster's ends through the global buffers
-  const bool dsm_recv = ncl > 1 && (BACKWARD ? crank + 1 < ncl : crank > 0);
-  const bool dsm_send = ncl > 1 && (BACKWARD ? crank > 0 : crank + 1 < ncl);
+  const bool dsm_recv = CL && ncl > 1 && (BACKWARD ? crank + 1 < ncl : crank > 0);
+  const bool dsm_send = CL && ncl > 1 && (BACKWARD ? crank > 0 : crank + 1 < ncl);
   const uint32_t producer = BACKWARD ? crank + 1 : crank - 1, consumer = BACKWARD ? crank - 1 : crank + 1;
   // the step q of the consumer's wait is the producer's step q + TI - 1
   const int QN = S - TI + 1;   // hand-over steps per pass
+  constexpr uint32_t kPush = TJ * 5 * sizeof(T);   // bytes pushed per hand-over step (armed above for the first RX)
   const T rdx = (T)(1.0 / d.dxi), rdy = (T)(1.0 / d.det), rdz = (T)(1.0 / d.dzt);
   T *xb = SweepPtrs<T>::xb(a), *yb = SweepPtrs<T>::yb(a);
   T *const *dq = SweepPtrs<T>::dq(a);
@@ -414,9 +427,13 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
     const int rel = BACKWARD ? s - (TI - 1 - il) - (TJ - 1 - jl) : s - il - jl;
     const int kl = BACKWARD ? Nz - 1 - rel : rel;
     // the slot read in step s - 1 is free again (every receiving lane read it
-    // before the barrier that ended that step)
-    if (dsm_recv && threadIdx.x == 0 && s >= 1 && s - 1 < QN)
-      tc::mbar_arrive_cluster(tc::mapa(tc::smem_addr(&s_empty[(s - 1) % RX]), producer));
+    // before the barrier that ended that step): arm it for its next use, then
+    // give it back to the producer
+    if (dsm_recv && threadIdx.x == 0 && s >= 1 && s - 1 < QN) {
+      if (s - 1 + RX < QN) tc::mbar_expect_tx(tc::smem_addr(&s_full[(s - 1) % RX]), kPush);
+      tc::mbar_arrive_cluster_relaxed(tc::mapa(tc::smem_addr(&s_empty[(s - 1) % RX]), producer));
+    }
+    if (threadIdx.x == 0) s_abort[(s + 1) & 1] = 0;   // read last after step s - 1 (it held 0)
     // loads of the next cell go out first and land during the dependent part
     // stage (s + RING - 1) % RING was last read at step s - 1, before the previous barrier
     if (threadIdx.x == 0 && s + RING - 1 < S) issue(s + RING - 1);
@@ -555,18 +572,21 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
         atomicExch(d.status, CGLI_TIMEOUT_CODE);
         gave_up = 1;
       } else {
-        if (cur.active) {
-          const uint32_t dst = tc::mapa(tc::smem_addr(s_rx + ((q % RX) * TJ + jl) * XW), consumer);
-          if (sizeof(T) == 8) {
-            tc::st_cluster_v2(dst, (double)ox[0], (double)ox[1]);
-            tc::st_cluster_v2(dst + 16, (double)ox[2], (double)ox[3]);
-            tc::st_cluster(dst + 32, (double)ox[4]);
-          } else {
-            tc::st_cluster_v4(dst, (float)ox[0], (float)ox[1], (float)ox[2], (float)ox[3]);
-            tc::st_cluster(dst + 16, (float)ox[4]);
-          }
+        // every lane pushes its five words each step (zeros for a cell
+        // outside the slab), so the consumer's byte count always completes
+        T o5[5];
+#pragma unroll
+        for (int v = 0; v < 5; v++) o5[v] = cur.active ? ox[v] : (T)0;
+        const uint32_t dst = tc::mapa(tc::smem_addr(s_rx + ((q % RX) * TJ + jl) * XW), consumer);
+        const uint32_t bar = tc::mapa(tc::smem_addr(&s_full[q % RX]), consumer);
+        if (sizeof(T) == 8) {
+          tc::st_async_v2(dst, (double)o5[0], (double)o5[1], bar);
+          tc::st_async_v2(dst + 16, (double)o5[2], (double)o5[3], bar);
+          tc::st_async(dst + 32, (double)o5[4], bar);
+        } else {
+          tc::st_async_v4(dst, (float)o5[0], (float)o5[1], (float)o5[2], (float)o5[3], bar);
+          tc::st_async(dst + 16, (float)o5[4], bar);
         }
-        tc::mbar_arrive_cluster(tc::mapa(tc::smem_addr(&s_full[q % RX]), consumer));
       }
     }
     if (pre_x || pre_y) {
@@ -575,19 +595,27 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
       if (s + 2 < S) preload(s + 2, px1, py1);
     }
     cur = nxt;
-    if (__syncthreads_or(gave_up)) {
+    if (gave_up) s_abort[s & 1] = 1;
+    __syncthreads();
+    if (*(volatile int *)&s_abort[s & 1]) {
       // a wait of this step gave up: wait (bounded) for the record copies
       // still in flight into this CTA's shared memory, then stop; the
       // consumers of this tile's products give up on it in turn
       if (threadIdx.x == 0)
         for (int r = s; r < s + RING && r < S; r++) tc::mbar_wait(tc::smem_addr(&s_bar[r % RING]), (r / RING) & 1, kDrainPolls);
-      // the cluster's CTAs leave together: none may leave while another
-      // can still write into its shared memory
-      if (ncl > 1) tc::cluster_sync();
+      if (CL) {
+        // the cluster's CTAs leave together, none while another can still
+        // write into its shared memory; a push issued just before a
+        // neighbour stopped lands within a microsecond: wait that out
+        tc::cluster_sync();
+        if (threadIdx.x == 0)
+          for (int n = 0; n < 100; n++) __nanosleep(200);
+        __syncthreads();
+      }
       return;
     }
   }
-  if (ncl > 1) tc::cluster_sync();
+  if (CL) tc::cluster_sync();
 }
 
 // Dual_time_stepping.cpp:1702-1743 after the last backward pass: the
@@ -632,9 +660,9 @@ __global__ void __launch_bounds__(128) k_update_skewed(Dev d, SweepArgs a) {
 
 // dynamic shared memory of a wavefront pass: the ring of record stages
 template <int TI, int TJ, typename T>
-constexpr int sweep_smem_bytes(bool backward) {
+constexpr int sweep_smem_bytes(bool backward, bool cluster) {
   return CGLI_SWEEP_RING * TI * TJ * (CR_N + (backward && CGLI_SWEEP_DQ_BULK ? 5 : 0)) * (int)sizeof(T) +
-         8 * TJ * (sizeof(T) == 8 ? 6 : 8) * (int)sizeof(T);   // the cluster's x hand-over ring
+         (cluster ? 8 * TJ * (sizeof(T) == 8 ? 6 : 8) * (int)sizeof(T) : 0);   // the cluster's x hand-over ring
 }
 
 // tickets follow the anti-diagonals ta + tb of the tile grid
@@ -665,7 +693,7 @@ static void run_one_pass(const Dev &d, const SweepArgs &a, cudaStream_t s, bool 
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(ntiles);
   cfg.blockDim = dim3(TI * TJ);
-  cfg.dynamicSmemBytes = sweep_smem_bytes<TI, TJ, T>(backward);
+  cfg.dynamicSmemBytes = sweep_smem_bytes<TI, TJ, T>(backward, a.cluster_x > 1);
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
   if (a.cluster_x > 1) {
@@ -676,8 +704,13 @@ static void run_one_pass(const Dev &d, const SweepArgs &a, cudaStream_t s, bool 
     cfg.attrs = attr;
     cfg.numAttrs = 1;
   }
-  if (!backward) cudaLaunchKernelEx(&cfg, k_sweep<TI, TJ, Met, false, T>, d, a);
-  else cudaLaunchKernelEx(&cfg, k_sweep<TI, TJ, Met, true, T>, d, a);
+  if (a.cluster_x > 1) {
+    if (!backward) cudaLaunchKernelEx(&cfg, k_sweep<TI, TJ, Met, false, T, true>, d, a);
+    else cudaLaunchKernelEx(&cfg, k_sweep<TI, TJ, Met, true, T, true>, d, a);
+  } else {
+    if (!backward) cudaLaunchKernelEx(&cfg, k_sweep<TI, TJ, Met, false, T, false>, d, a);
+    else cudaLaunchKernelEx(&cfg, k_sweep<TI, TJ, Met, true, T, false>, d, a);
+  }
   if (final_pass) k_update_skewed<T><<<dim3(d.ny, d.nx), 128, 0, s>>>(d, a);
 }
 
@@ -699,21 +732,27 @@ void launch_sweep_pass(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mi
 
 // the wavefront kernels' shared memory (static products plus the dynamic
 // two-step record buffer) exceeds 48 KB: opt in once, outside any capture
-template <class Met, typename T>
+template <class Met, typename T, bool CL>
 static cudaError_t opt_in() {
-  cudaError_t e = cudaFuncSetAttribute(k_sweep<SWEEP_TI, SWEEP_TJ, Met, false, T>,
+  cudaError_t e = cudaFuncSetAttribute(k_sweep<SWEEP_TI, SWEEP_TJ, Met, false, T, CL>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       sweep_smem_bytes<SWEEP_TI, SWEEP_TJ, T>(false));
+                                       sweep_smem_bytes<SWEEP_TI, SWEEP_TJ, T>(false, CL));
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_sweep<SWEEP_TI, SWEEP_TJ, Met, true, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             sweep_smem_bytes<SWEEP_TI, SWEEP_TJ, T>(true));
+    e = cudaFuncSetAttribute(k_sweep<SWEEP_TI, SWEEP_TJ, Met, true, T, CL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             sweep_smem_bytes<SWEEP_TI, SWEEP_TJ, T>(true, CL));
   return e;
 }
 cudaError_t sweep_kernel_attributes() {
-  cudaError_t e = opt_in<MetricsChannel, double>();
-  if (e == cudaSuccess) e = opt_in<MetricsGeneral, double>();
-  if (e == cudaSuccess) e = opt_in<MetricsChannel, float>();
-  if (e == cudaSuccess) e = opt_in<MetricsGeneral, float>();
+  cudaError_t e = opt_in<MetricsChannel, double, false>();
+  if (e == cudaSuccess) e = opt_in<MetricsGeneral, double, false>();
+  if (e == cudaSuccess) e = opt_in<MetricsChannel, float, false>();
+  if (e == cudaSuccess) e = opt_in<MetricsGeneral, float, false>();
+#if CGLI_SWEEP_CLUSTER_MAX > 1
+  if (e == cudaSuccess) e = opt_in<MetricsChannel, double, true>();
+  if (e == cudaSuccess) e = opt_in<MetricsGeneral, double, true>();
+  if (e == cudaSuccess) e = opt_in<MetricsChannel, float, true>();
+  if (e == cudaSuccess) e = opt_in<MetricsGeneral, float, true>();
+#endif
   return e;
 }
 
@@ -727,7 +766,7 @@ int sweep_cluster_x(int nti, int ntj, int max_cx) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(nti * ntj);
     cfg.blockDim = dim3(SWEEP_TI * SWEEP_TJ);
-    cfg.dynamicSmemBytes = sweep_smem_bytes<SWEEP_TI, SWEEP_TJ, double>(true);
+    cfg.dynamicSmemBytes = sweep_smem_bytes<SWEEP_TI, SWEEP_TJ, double>(true, true);
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = cx;
@@ -736,7 +775,7 @@ int sweep_cluster_x(int nti, int ntj, int max_cx) {
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     int n = 0;
-    if (cudaOccupancyMaxActiveClusters(&n, k_sweep<SWEEP_TI, SWEEP_TJ, MetricsGeneral, true, double>, &cfg) !=
+    if (cudaOccupancyMaxActiveClusters(&n, k_sweep<SWEEP_TI, SWEEP_TJ, MetricsGeneral, true, double, true>, &cfg) !=
         cudaSuccess) {
       cudaGetLastError();
       continue;

@@ -100,6 +100,35 @@ __device__ __forceinline__ bool mbar_wait_cluster(uint32_t bar, uint32_t parity,
   }
   return false;
 }
+// Asynchronous stores into another cluster CTA's shared memory that count
+// their bytes on that CTA's mbarrier (complete_tx): the consumer arms the
+// barrier with the bytes it expects and waits on it; no fence is needed on
+// the producing side.
+__device__ __forceinline__ void st_async_v2(uint32_t addr, double x, double y, uint32_t remote_bar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f64 [%0], {%1, %2}, [%3];" ::"r"(addr),
+               "d"(x), "d"(y), "r"(remote_bar)
+               : "memory");
+}
+__device__ __forceinline__ void st_async(uint32_t addr, double x, uint32_t remote_bar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.f64 [%0], %1, [%2];" ::"r"(addr), "d"(x),
+               "r"(remote_bar)
+               : "memory");
+}
+__device__ __forceinline__ void st_async_v4(uint32_t addr, float x, float y, float z, float w, uint32_t remote_bar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.f32 [%0], {%1, %2, %3, %4}, [%5];" ::"r"(addr),
+               "f"(x), "f"(y), "f"(z), "f"(w), "r"(remote_bar)
+               : "memory");
+}
+__device__ __forceinline__ void st_async(uint32_t addr, float x, uint32_t remote_bar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.f32 [%0], %1, [%2];" ::"r"(addr), "f"(x),
+               "r"(remote_bar)
+               : "memory");
+}
+// Arrival on another cluster CTA's mbarrier without ordering this thread's
+// earlier memory operations (a flow-control signal that carries no data).
+__device__ __forceinline__ void mbar_arrive_cluster_relaxed(uint32_t remote_bar) {
+  asm volatile("mbarrier.arrive.relaxed.cluster.shared::cluster.b64 _, [%0];" ::"r"(remote_bar) : "memory");
+}
 // The cluster-wide barrier (every thread of every CTA of the cluster).
 __device__ __forceinline__ void cluster_sync() {
   asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");

@@ -146,9 +146,7 @@ def test_training_reduces_loss_on_a_fixed_pair():
     assert l1 < 0.75 * l0
 
 
-def _lockstep_channel():
-    from cgli_fu_flow_b200.channel import Channel
-    return Channel(16, 16, 32)
+CAP = 200
 
 
 @pytest.mark.gpu
@@ -161,12 +159,14 @@ def test_training_on_solver_levels_and_ab_against_extrapolation():
     an A/B test of the initial guess alone.  The learned guess must be
     closer to the converged Q^(n+1) than extrapolation and must need fewer
     inner iterations in total to reach the same stopping rule (every norm
-    below 1e-3 of its running maximum)."""
+    below 1e-3 of its running maximum; the cap of 200 is not reached on
+    this 64^3 channel, unlike the reference's 30 on the smallest grids)."""
     from cgli_fu_flow_b200 import build
+    from cgli_fu_flow_b200.channel import Channel
     from cgli_fu_flow_b200.cnn import Network, init_params, physical_levels, scales_from_levels
     from cgli_fu_flow_b200.solver import Solver
     build.build()
-    ch = _lockstep_channel()
+    ch = Channel(64, 64, 64)
     A, B = Solver(ch), Solver(ch)
     A.init()
     A.set_predictor(1)
@@ -176,7 +176,7 @@ def test_training_on_solver_levels_and_ab_against_extrapolation():
     host_levels = []
     warm, train_steps = 8, 48
     for k in range(warm + train_steps):
-        A.step(None, 1e-3, 30)
+        A.step(None, 1e-3, CAP)
         if k >= warm:
             net.push_level(A)
             host_levels.append(physical_levels(A))
@@ -192,8 +192,8 @@ def test_training_on_solver_levels_and_ab_against_extrapolation():
     for k in range(12):
         B.copy_state_from(A)
         B.set_predictor(2)
-        nb, _ = B.step(None, 1e-3, 30)
-        na, _ = A.step(None, 1e-3, 30)
+        nb, _ = B.step(None, 1e-3, CAP)
+        na, _ = A.step(None, 1e-3, CAP)
         it_a.append(na)
         it_b.append(nb)
         net.push_level(A)
@@ -210,4 +210,59 @@ def test_training_on_solver_levels_and_ab_against_extrapolation():
     assert sum(it_b) < sum(it_a), (it_a, it_b)
     for s in (A, B):
         s.close()
+    net.close()
+
+
+TIGHT_DROP = 1e-8      # every norm below 1e-8 of its running maximum
+STATE_TOL = 1e-6       # relative L2 per conserved variable after 100 steps
+
+
+@pytest.mark.gpu
+def test_mixed_learned_converges_to_the_fp64_answer_under_a_tight_rule():
+    """The solution the mixed-precision + learned-guess path converges to is
+    the FP64 path's: both run the same 100 physical steps from one state
+    with the same stopping rule, tight enough that the stopping point no
+    longer depends on the initial guess, and end within 1e-6 relative L2 of
+    each other in every conserved variable.  (At the reference's loose 1e-3
+    drop the two stop at different points of the inner iteration, and their
+    states differ by far more: the iteration count, not the answer, is what
+    the learned guess is allowed to change.)"""
+    from cgli_fu_flow_b200 import build
+    from cgli_fu_flow_b200.channel import Channel
+    from cgli_fu_flow_b200.cnn import Network, init_params, physical_levels, scales_from_levels
+    from cgli_fu_flow_b200.solver import MIXED, Solver
+    build.build()
+    ch = Channel(16, 16, 32)
+    A = Solver(ch)
+    A.init()
+    A.set_predictor(1)
+    net = Network(ch.nx, ch.ny, ch.nz)
+    net.reserve_levels(64)
+    net.set_params(init_params(0))
+    host = []
+    for k in range(8 + 48):
+        A.step(None, 1e-3, 30)
+        if k >= 8:
+            net.push_level(A)
+            host.append(physical_levels(A))
+    net.set_scales(*scales_from_levels(host))
+    net.train(600, 1e-3, 1234, 0, net.levels - 3)
+    sl = np.s_[:, 3:ch.nx + 3, 2:ch.ny + 2, 2:ch.nz + 2]
+    runs = {}
+    for name, prec, pred in (("fp64", 0, 0), ("mixed_learned", MIXED, 2)):
+        s = Solver(ch, prec)
+        s.copy_state_from(A)
+        if pred == 2:
+            s.set_learned_guess(net)
+        s.set_predictor(pred)
+        its = [s.step(None, TIGHT_DROP, 400)[0] for _ in range(100)]
+        runs[name] = (s.q()[sl], its)
+        s.close()
+    (qf, itf), (qm, itm) = runs["fp64"], runs["mixed_learned"]
+    errs = [float(np.linalg.norm(qm[v] - qf[v]) / np.linalg.norm(qf[v])) for v in range(5)]
+    print("mean inner iterations: fp64", np.mean(itf), "mixed + learned", np.mean(itm))
+    print("state relative L2, mixed + learned vs fp64, per variable:", errs)
+    assert max(itf) < 400 and max(itm) < 400, "the tight rule must be met, not capped"
+    assert max(errs) <= STATE_TOL
+    A.close()
     net.close()
