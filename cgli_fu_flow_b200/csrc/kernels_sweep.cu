@@ -21,12 +21,15 @@
 // column through global buffers filled with a sentinel bit pattern before the
 // pass; the consumer spins (bounded) on the values themselves until none is
 // the sentinel, so a hand-over needs no fence and no counter (4- and 8-byte
-// stores are single-copy atomic).  When a wait gives up (the hand-over poll or
-// the record copy's mbarrier, SweepArgs::spin_limit polls) the tile records
-// the timeout code in the status word, waits (bounded) for its own bulk
-// copies still in flight and returns; the tiles downstream then give up on
-// it in turn, the update kernel leaves the state alone, and the host reports
-// CGLI_ETIMEOUT.
+// stores are single-copy atomic).  A wait on another tile gives up after
+// SweepArgs::spin_limit polls, or at once when its CTA or any tile has
+// already given up (the CTA's dead flag, the status word): it records the
+// timeout code in the status word and the tile carries on to the end of the
+// pass without waiting, computing values nobody will use.  So no wait is
+// ever repeated at full length, every bulk copy is still awaited in order
+// (those waits have a fixed bound: the copies complete on their own), the
+// fast path carries no exit test, the update kernel leaves the state alone
+// and the host reports CGLI_ETIMEOUT.
 // Tiles take tickets in an order where every dependency holds a smaller
 // ticket, so a waiting CTA only ever waits on CTAs that are already running.
 //
@@ -127,10 +130,20 @@ __device__ __forceinline__ float ld_gpu(const float *p) {
 __device__ __forceinline__ bool is_sentinel(double v) { return __double_as_longlong(v) == -1ll; }
 __device__ __forceinline__ bool is_sentinel(float v) { return __float_as_int(v) == -1; }
 
-// bounded spin on five values handed over by a neighbouring tile; false
-// (and the timeout code in the status word) when it gives up
+// a wait on another tile has given up somewhere: this CTA's dead flag or
+// the grid's status word
+__device__ __forceinline__ bool given_up(const volatile int *dead, const int *status) {
+  return *dead || *(const volatile int *)status;
+}
+__device__ __forceinline__ void give_up(volatile int *dead, int *status) {
+  atomicExch(status, CGLI_TIMEOUT_CODE);
+  *dead = 1;
+}
+
+// bounded spin on five values handed over by a neighbouring tile; false when
+// it gives up (after `limit` polls, or at once once anything gave up)
 template <typename T>
-__device__ __forceinline__ bool recv5(const T *src, T out[5], int *status, int limit) {
+__device__ __forceinline__ bool recv5(const T *src, T out[5], int *status, int limit, volatile int *dead) {
   for (int it = 0;; it++) {
     bool ok = true;
 #pragma unroll
@@ -139,17 +152,17 @@ __device__ __forceinline__ bool recv5(const T *src, T out[5], int *status, int l
       ok = ok && !is_sentinel(out[v]);
     }
     if (ok) return true;
-    if (it >= limit) {
-      atomicExch(status, CGLI_TIMEOUT_CODE);
+    if (it >= limit || given_up(dead, status)) {
+      give_up(dead, status);
       return false;
     }
     __nanosleep(20);
   }
 }
 
-// polls for the wait on a tile's own bulk copies before it returns after a
-// timeout (the copies complete on their own; this only bounds the wait)
-constexpr int kDrainPolls = 1 << 20;
+// polls of the wait on a tile's own bulk copy of records (the copies complete
+// on their own; this only bounds the wait against a failing device)
+constexpr int kCopyPolls = 1 << 20;
 
 // REC_N record words and (mr non-null) the 5 MR words of one slot, through
 // the read-only path (CGLI_SWEEP_LDG) or plain loads
@@ -288,7 +301,7 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
   __shared__ T sy[2][TI][TJ][5];   // j-direction products
   __shared__ double s_jt[TJ], s_et[TJ];
   __shared__ int s_tile;
-  __shared__ int s_abort[2];   // a wait of step s gave up (slot s & 1)
+  __shared__ int s_dead;       // a wait of this CTA gave up: no more waiting
   // x hand-over ring inside a cluster: RX steps x TJ lanes x XW words
   constexpr int RX = 8, XW = sizeof(T) == 8 ? 6 : 8;
   __shared__ __align__(8) uint64_t s_full[CL ? RX : 1], s_empty[CL ? RX : 1];
@@ -316,8 +329,7 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
       const uint32_t t = atomicAdd(a.ticket, 1u);
       for (uint32_t r = 0; r < ncl; r++) tc::st_cluster_u32(tc::mapa(tc::smem_addr(&s_tile), r), t);
     }
-    s_abort[0] = 0;
-    s_abort[1] = 0;
+    s_dead = 0;
     if (CL) {
 #pragma unroll
       for (int r = 0; r < RX; r++) {
@@ -433,18 +445,13 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
       if (s - 1 + RX < QN) tc::mbar_expect_tx(tc::smem_addr(&s_full[(s - 1) % RX]), kPush);
       tc::mbar_arrive_cluster_relaxed(tc::mapa(tc::smem_addr(&s_empty[(s - 1) % RX]), producer));
     }
-    if (threadIdx.x == 0) s_abort[(s + 1) & 1] = 0;   // read last after step s - 1 (it held 0)
     // loads of the next cell go out first and land during the dependent part
     // stage (s + RING - 1) % RING was last read at step s - 1, before the previous barrier
     if (threadIdx.x == 0 && s + RING - 1 < S) issue(s + RING - 1);
     if (s + 1 < S) fetch_cell<TI, TJ, Met, BACKWARD, T>(d, a, s_et, il, jl, j, s + 1, S, tile_base, inside, halo_edge, nxt);
     else nxt.active = false;
     // this step's records (bounded wait; a timeout is reported like a tile's)
-    int gave_up = 0;
-    if (!tc::mbar_wait(tc::smem_addr(&s_bar[s % RING]), (s / RING) & 1, a.spin_limit)) {
-      atomicExch(d.status, CGLI_TIMEOUT_CODE);
-      gave_up = 1;
-    }
+    if (!tc::mbar_wait(tc::smem_addr(&s_bar[s % RING]), (s / RING) & 1, kCopyPolls)) give_up(&s_dead, d.status);
     if (cur.active) {
       const T *st = s_rec + (s % RING) * kStage;
       load_cellrec(st + threadIdx.x * CR_N, cur.rec, BACKWARD ? (T *)nullptr : cur.mr);
@@ -465,10 +472,10 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
         for (int v = 0; v < 5; v++) tx[v] = sx[pbuf][sil][jl][v];
       } else if (dsm_recv) {
         // pushed by the producing CTA of the cluster (step s < QN here)
-        if (!tc::mbar_wait_cluster(tc::smem_addr(&s_full[s % RX]), (s / RX) & 1, a.spin_limit)) {
-          atomicExch(d.status, CGLI_TIMEOUT_CODE);
-          gave_up = 1;
-        }
+        const uint32_t fb = tc::smem_addr(&s_full[s % RX]);
+        if (!tc::mbar_wait_cluster(fb, (s / RX) & 1, 1) &&
+            !tc::mbar_wait_cluster(fb, (s / RX) & 1, given_up(&s_dead, d.status) ? 0 : a.spin_limit))
+          give_up(&s_dead, d.status);
         const T *src = s_rx + ((s % RX) * TJ + jl) * XW;
 #pragma unroll
         for (int v = 0; v < 5; v++) tx[v] = src[v];
@@ -476,7 +483,7 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
         bool ok = true;
 #pragma unroll
         for (int v = 0; v < 5; v++) { tx[v] = px0[v]; ok = ok && !is_sentinel(px0[v]); }
-        if (!ok && !recv5<T>(xsrc + (long long)kl * 5, tx, d.status, a.spin_limit)) gave_up = 1;
+        if (!ok) recv5<T>(xsrc + (long long)kl * 5, tx, d.status, a.spin_limit, &s_dead);
       }
       if (!recv_y) {
         const int sjl = BACKWARD ? jl + 1 : jl - 1;
@@ -486,7 +493,7 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
         bool ok = true;
 #pragma unroll
         for (int v = 0; v < 5; v++) { ty[v] = py0[v]; ok = ok && !is_sentinel(py0[v]); }
-        if (!ok && !recv5<T>(ysrc + (long long)kl * 5, ty, d.status, a.spin_limit)) gave_up = 1;
+        if (!ok) recv5<T>(ysrc + (long long)kl * 5, ty, d.status, a.spin_limit, &s_dead);
       } else {
 #pragma unroll
         for (int v = 0; v < 5; v++) ty[v] = 0;  // wall ghost row: dQ = 0 there
@@ -567,11 +574,13 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
     }
     if (dsm_send && send_x && s >= TI - 1) {
       const int q = s - (TI - 1);
-      // the slot's previous use must have been read by the consumer
-      if (q >= RX && !tc::mbar_wait_cluster(tc::smem_addr(&s_empty[q % RX]), ((q / RX) - 1) & 1, a.spin_limit)) {
-        atomicExch(d.status, CGLI_TIMEOUT_CODE);
-        gave_up = 1;
-      } else {
+      // the slot's previous use must have been read by the consumer (after
+      // a give-up the push goes ahead regardless: its values are unused)
+      const uint32_t eb = tc::smem_addr(&s_empty[q % RX]);
+      if (q >= RX && !tc::mbar_wait_cluster(eb, ((q / RX) - 1) & 1, 1) &&
+          !tc::mbar_wait_cluster(eb, ((q / RX) - 1) & 1, given_up(&s_dead, d.status) ? 0 : a.spin_limit))
+        give_up(&s_dead, d.status);
+      {
         // every lane pushes its five words each step (zeros for a cell
         // outside the slab), so the consumer's byte count always completes
         T o5[5];
@@ -595,26 +604,10 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
       if (s + 2 < S) preload(s + 2, px1, py1);
     }
     cur = nxt;
-    if (gave_up) s_abort[s & 1] = 1;
     __syncthreads();
-    if (*(volatile int *)&s_abort[s & 1]) {
-      // a wait of this step gave up: wait (bounded) for the record copies
-      // still in flight into this CTA's shared memory, then stop; the
-      // consumers of this tile's products give up on it in turn
-      if (threadIdx.x == 0)
-        for (int r = s; r < s + RING && r < S; r++) tc::mbar_wait(tc::smem_addr(&s_bar[r % RING]), (r / RING) & 1, kDrainPolls);
-      if (CL) {
-        // the cluster's CTAs leave together, none while another can still
-        // write into its shared memory; a push issued just before a
-        // neighbour stopped lands within a microsecond: wait that out
-        tc::cluster_sync();
-        if (threadIdx.x == 0)
-          for (int n = 0; n < 100; n++) __nanosleep(200);
-        __syncthreads();
-      }
-      return;
-    }
   }
+  // the cluster's CTAs leave together: none while another can still write
+  // into its shared memory
   if (CL) tc::cluster_sync();
 }
 

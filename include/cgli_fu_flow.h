@@ -218,14 +218,14 @@ int cgli_step_norms(cgli_ctx *ctx, double *norms, int max_iters, int *iters);
  * cell where the network's output is not finite). */
 int cgli_set_predictor(cgli_ctx *ctx, int mode);
 
-/* Bound of every device-side wait of the LU-SGS wavefront passes (the
- * reference has none: its OpenMP barriers wait without limit): a tile
- * waiting for its neighbour's products or for its own record copy polls at
- * most `polls` times (default CGLI_WAIT_LIMIT_DEFAULT, well over a second),
- * then records a timeout, finishes its copies in flight and stops; the
- * update leaves U_ unchanged, the call returns CGLI_ETIMEOUT and the next
- * call runs normally.  0 makes every wait give up at once (for tests of the
- * timeout path). */
+/* Bound of the device-side waits of the LU-SGS wavefront passes on other
+ * tiles (the reference has none: its OpenMP barriers wait without limit): a
+ * tile waiting for its neighbour's products polls at most `polls` times
+ * (default CGLI_WAIT_LIMIT_DEFAULT, well over a second), then records a
+ * timeout; from then on no wait of the pass waits again, the pass runs to
+ * its end computing values that are discarded, the update leaves U_
+ * unchanged, the call returns CGLI_ETIMEOUT and the next call runs normally.
+ * 0 makes those waits give up at once (for tests of the timeout path). */
 #define CGLI_WAIT_LIMIT_DEFAULT 4194304
 int cgli_set_wait_limit(cgli_ctx *ctx, int polls);
 /* The (i, j) column tile of the wavefront passes this library was built

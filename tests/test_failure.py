@@ -5,10 +5,10 @@ a diverging run just prints non-finite norms (Dual_time_stepping.cpp:1761-1791,
 main.cpp:313).  The library bounds every device-side wait of the wavefront
 passes and turns both conditions into return codes:
 
-* a wait that runs out (here forced with a wait limit of 0 polls, so that
-  every wait gives up at once) makes the tile record a timeout, finish its
-  own copies in flight and stop; the update leaves the state alone, the call
-  returns CGLI_ETIMEOUT and the context keeps working;
+* a wait on another tile that runs out (here forced with a wait limit of 0
+  polls, so that such waits give up at once) records a timeout; the pass
+  then runs to its end without waiting, the update leaves the state alone,
+  the call returns CGLI_ETIMEOUT and the context keeps working;
 * a non-finite state (NaN in Q) or a degenerate metric (J = 0 in one cell)
   gives non-finite update norms: CGLI_EDIVERGED.
 
