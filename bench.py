@@ -66,6 +66,10 @@ def parse():
     ap.add_argument("--skip", type=int, default=16, help="first steps (initial transient) not used for training")
     ap.add_argument("--train-steps", type=int, default=600)
     ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--subbox-pairs", type=int, default=2000,
+                    help="also train the learned guess on this many (history, converged level) pairs of a seeded run of "
+                         "a 64 x Ny x 64 sub-box of the channel with its cell sizes (0: off), and add arms with it")
+    ap.add_argument("--subbox-train-steps", type=int, default=2000)
     ap.add_argument("--tight-drop", type=float, default=1e-9,
                     help="stopping rule of the arms' second matrix: the drop under which the converged state no "
                          "longer depends on the predictor or the sweep precision")
@@ -347,12 +351,15 @@ def run_arms(a, ch, dist) -> dict:
                              "collect_s": round(collect_s, 2), "train_s": round(train_s, 2),
                              "loss_unit": "mean squared extrapolation correction / its RMS (1.0 = extrapolation)"}}
     sl = (slice(None), slice(3, ch.nx + 3), slice(2, ch.ny + 2), slice(2, ch.nz + 2))
+    net_box = None
+    if a.subbox_pairs > 0 and ch.nx % 64 == 0 and ch.nz % 64 == 0:
+        net_box, out["learned_guess_subbox"] = train_on_subbox(a, ch)
 
-    def run(prec, pred, drop, cap, inner="lusgs"):
+    def run(prec, pred, drop, cap, inner="lusgs", learned=None):
         s = Solver(ch, prec)
         s.copy_state_from(base)
         if pred == 2:
-            s.set_learned_guess(net)
+            s.set_learned_guess(learned or net)
         s.set_predictor(pred)
         if inner == "dplur":
             s.set_inner_solver("dplur")
@@ -366,7 +373,7 @@ def run_arms(a, ch, dist) -> dict:
                "inner_solver": "DP-LUR (DPLUSGS.cpp: 4 Jacobi relaxations; norms of squared "
                                "p, u, v, w, T increments)" if inner == "dplur" else "LU-SGS"}
         if pred == 2:
-            inf_ms = net.time_inference(s, 3)
+            inf_ms = (learned or net).time_inference(s, 3)
             res["inference"] = {"ms": round(inf_ms, 3),
                                 "tensor_tflops": round(ch.cells * CNN_TC_FLOP_PER_CELL / (inf_ms / 1e3) / 1e12, 1),
                                 "real_tflops": round(ch.cells * CNN_FLOP_PER_CELL / (inf_ms / 1e3) / 1e12, 1)}
@@ -393,6 +400,9 @@ def run_arms(a, ch, dist) -> dict:
             arms[name], qs[name] = run(prec, pred, drop, cap)
         if rule == "headline":
             arms["fp64_dplur"], qs["fp64_dplur"] = run(FP64, 0, drop, cap, "dplur")
+        if net_box is not None:
+            arms["mixed_learned_subbox"], qs["mixed_learned_subbox"] = run(MIXED, 2, drop, cap, learned=net_box)
+            arms["mixed_learned_subbox"]["predictor"] = "learned (trained on the sub-box run)"
         for name, q in qs.items():
             arms[name]["state_rel_l2_vs_truth"] = rel(q, q_truth)
             arms[name]["state_rel_l2_vs_fp64_previous"] = rel(q, qs["fp64_previous"])
@@ -402,7 +412,59 @@ def run_arms(a, ch, dist) -> dict:
         out[rule] = arms
     base.close()
     net.close()
+    if net_box is not None:
+        net_box.close()
     return out
+
+
+def train_on_subbox(a, ch):
+    """The learned guess trained on `a.subbox_pairs` pairs: a seeded run of a
+    periodic 64 x Ny x 64 sub-box of the channel with the same cell sizes and
+    time step (mixed precision, extrapolated guess, headline rule) stores
+    skip + pairs + 3 converged levels on the device, the network of the
+    sub-box trains on all its pairs, and its parameters and scales go to a
+    network of the full grid (the network is convolutional: its weights do
+    not depend on the grid).  Returns (network, training record)."""
+    from cgli_fu_flow_b200.cnn import Network, init_params, physical_levels, scales_from_levels
+    from cgli_fu_flow_b200.solver import MIXED, Solver
+    sub = C.Channel(64, ch.ny, 64, lx_scale=64 / ch.nx, lz_scale=64 / ch.nz)
+    s = Solver(sub, MIXED)
+    s.init(sub.initial_conserved())
+    s.set_predictor(1)
+    nlev = a.subbox_pairs + 3
+    nb = Network(sub.nx, sub.ny, sub.nz)
+    nb.reserve_levels(nlev)
+    nb.set_params(init_params(0))
+    quads = [a.skip, a.skip + nlev // 2, a.skip + nlev - 4]
+    keep = {k for q in quads for k in range(q, q + 4)}
+    host, iters = {}, []
+    t0 = time.perf_counter()
+    for k in range(a.skip + nlev):
+        it, _ = s.step(None, a.drop, a.cap)
+        iters.append(it)
+        if k >= a.skip:
+            nb.push_level(s)
+            if k in keep:
+                host[k] = physical_levels(s, np.float32)
+    collect_s = time.perf_counter() - t0
+    sc = [scales_from_levels([host[k] for k in range(q, q + 4)]) for q in quads]
+    scales = [np.mean([x[i] for x in sc], axis=0) for i in range(3)]
+    nb.set_scales(*scales)
+    t0 = time.perf_counter()
+    loss = nb.train(a.subbox_train_steps, a.lr, 20261204, 0, a.subbox_pairs)
+    train_s = time.perf_counter() - t0
+    theta = nb.get_params()
+    s.close()
+    nb.close()
+    full = Network(ch.nx, ch.ny, ch.nz)
+    full.set_params(theta)
+    full.set_scales(*scales)
+    return full, {"workload": f"periodic sub-box {sub.nx}x{sub.ny}x{sub.nz} cells with the channel's cell sizes "
+                              f"(Lx x {64 / ch.nx:g}, Lz x {64 / ch.nz:g})",
+                  "training_pairs": a.subbox_pairs, "training_steps_of_run": [a.skip, a.skip + nlev],
+                  "adam_steps": a.subbox_train_steps, "lr": a.lr, "final_mean_loss": round(float(loss), 5),
+                  "mean_inner_iterations_of_run": round(float(np.mean(iters)), 2),
+                  "collect_s": round(collect_s, 2), "train_s": round(train_s, 2)}
 
 
 def run_e2e(a, ch, prec, dist: Dist) -> dict:

@@ -86,6 +86,11 @@ class Channel:
     buoyancy: bool = False
     twall_lo: float = T0                  # lower / upper wall temperature (K)
     twall_hi: float = T0
+    # a periodic sub-box of the channel: Lx and Lz scaled by these factors
+    # (1: the full 2 pi h x 2h x pi h channel), e.g. a smaller domain with
+    # the full channel's cell sizes for the learned guess's training data
+    lx_scale: float = 1.0
+    lz_scale: float = 1.0
     # derived (filled in __post_init__)
     rho0: float = field(init=False)
     c0: float = field(init=False)
@@ -106,8 +111,8 @@ class Channel:
         self.u_b = MACH_B * self.c0
         self.h = 0.5 * RE_B * MU0 / (self.rho0 * self.u_b)
         self.high = 2.0 * self.h                          # prm.h:16 (channel height)
-        self.lx = 2.0 * math.pi * self.h
-        self.lz = math.pi * self.h
+        self.lx = 2.0 * math.pi * self.h * self.lx_scale
+        self.lz = math.pi * self.h * self.lz_scale
         self.dxi = self.lx / self.nx                      # deltaXI, metres (xidx = 1)
         self.det = 1.0 / self.ny                          # deltaET, normalised eta
         self.dzt = self.lz / self.nz                      # deltaZT, metres (ztdz = 1)
@@ -118,7 +123,8 @@ class Channel:
     def name(self) -> str:
         if self.x_open:
             return f"open_{self.nx}x{self.ny}x{self.nz}_{self.nx_inlet}_{self.nx_outlet}"
-        return f"{'wavy' if self.wavy else 'channel'}_{self.nx}x{self.ny}x{self.nz}"
+        box = "" if self.lx_scale == 1.0 and self.lz_scale == 1.0 else f"_box{self.lx_scale:g}x{self.lz_scale:g}"
+        return f"{'wavy' if self.wavy else 'channel'}_{self.nx}x{self.ny}x{self.nz}{box}"
 
     @property
     def amplitude(self) -> float:

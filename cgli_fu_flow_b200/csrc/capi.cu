@@ -312,7 +312,12 @@ int cgli_create(const cgli_params *p, cgli_ctx **out) {
   if (rc == CGLI_OK) rc = alloc(c, 16 * sizeof(int), (void **)&d.status);
   if (rc == CGLI_OK) rc = alloc(c, 3 * 2 * sizeof(double) * d.Y, (void **)&d.ftab);
   c->update_blocks = p->nx * p->ny;
-  const int nti = (p->nx + cgli::SWEEP_TI - 1) / cgli::SWEEP_TI, ntj = (p->ny + cgli::SWEEP_TJ - 1) / cgli::SWEEP_TJ;
+  // the wavefront's tile grid for this context's precision
+  const bool mixed_passes = p->precision == CGLI_MIXED;
+  const int nti = mixed_passes ? cgli::sweep_tiles_x<float>(p->nx) : cgli::sweep_tiles_x<double>(p->nx);
+  const int ntj = mixed_passes ? cgli::sweep_tiles_y<float>(p->ny) : cgli::sweep_tiles_y<double>(p->ny);
+  const int tile_i = mixed_passes ? cgli::SweepTile<float>::TI : cgli::SweepTile<double>::TI;
+  const int tile_j = mixed_passes ? cgli::SweepTile<float>::TJ : cgli::SweepTile<double>::TJ;
   c->sweep_tiles = nti * ntj;
   size_t nblk = (size_t)std::max(c->update_blocks, c->sweep_tiles);
   if (rc == CGLI_OK) rc = alloc(c, 5 * sizeof(double) * nblk, (void **)&d.partial);
@@ -321,7 +326,7 @@ int cgli_create(const cgli_params *p, cgli_ctx **out) {
     memset(&a, 0, sizeof a);
     const bool mixed = p->precision == CGLI_MIXED;
     const size_t es = mixed ? sizeof(float) : sizeof(double);
-    const size_t nsk = (size_t)cgli::skew_size(d);
+    const size_t nsk = (size_t)(mixed ? cgli::skew_size<float>(d) : cgli::skew_size<double>(d));
     const size_t plane = (size_t)d.Y * d.Z;
     for (int v = 0; v < 5; v++) {
       if (mixed) {
@@ -347,8 +352,8 @@ int cgli_create(const cgli_params *p, cgli_ctx **out) {
         if (rc == CGLI_OK) rc = alloc(c, plane * es, (void **)&a.hrec_b[v]);
       }
     }
-    size_t xb = (size_t)c->sweep_tiles * cgli::SWEEP_TJ * p->nz * 5 * es;
-    size_t yb = (size_t)c->sweep_tiles * cgli::SWEEP_TI * p->nz * 5 * es;
+    size_t xb = (size_t)c->sweep_tiles * tile_j * p->nz * 5 * es;
+    size_t yb = (size_t)c->sweep_tiles * tile_i * p->nz * 5 * es;
     if (rc == CGLI_OK) rc = alloc(c, xb, mixed ? (void **)&a.xbuff : (void **)&a.xbuf);
     if (rc == CGLI_OK) rc = alloc(c, yb, mixed ? (void **)&a.ybuff : (void **)&a.ybuf);
     if (rc == CGLI_OK) rc = alloc(c, 64, (void **)&a.ticket);
@@ -365,9 +370,8 @@ int cgli_create(const cgli_params *p, cgli_ctx **out) {
   if (rc == CGLI_OK) {
     // wavefront clusters along x, and the tickets' order of the cluster
     // rows (anti-diagonals of the grid of clusters)
-    const int nti = (p->nx + cgli::SWEEP_TI - 1) / cgli::SWEEP_TI, ntj = (p->ny + cgli::SWEEP_TJ - 1) / cgli::SWEEP_TJ;
     cgli::SweepArgs &a = c->sw;
-    a.cluster_x = cgli::sweep_cluster_x(nti, ntj, CGLI_SWEEP_CLUSTER_MAX);
+    a.cluster_x = cgli::sweep_cluster_x(nti, ntj, mixed_passes);
     std::vector<int> order;
     cgli::sweep_tile_order(nti / a.cluster_x, ntj, order);
     int *dorder = nullptr;
@@ -814,10 +818,12 @@ int cgli_set_predictor(cgli_ctx *c, int mode) {
   return CGLI_OK;
 }
 
-int cgli_sweep_tile_shape(int *ti, int *tj) {
+int cgli_sweep_tile_shape(int precision, int *ti, int *tj) {
   if (!ti || !tj) return fail(CGLI_EINVAL, "null argument");
-  *ti = cgli::SWEEP_TI;
-  *tj = cgli::SWEEP_TJ;
+  if (precision != CGLI_FP64 && precision != CGLI_MIXED)
+    return fail(CGLI_EINVAL, "precision must be CGLI_FP64 or CGLI_MIXED");
+  *ti = precision == CGLI_MIXED ? cgli::SweepTile<float>::TI : cgli::SweepTile<double>::TI;
+  *tj = precision == CGLI_MIXED ? cgli::SweepTile<float>::TJ : cgli::SweepTile<double>::TJ;
   return CGLI_OK;
 }
 

@@ -13,21 +13,49 @@ namespace cgli {
 constexpr int CR_N = REC_N + 5 + 1;
 constexpr int CR_MR = REC_N;
 
-// tile shape of the wavefront sweeps: TI x TJ (i, j) columns per CTA (one
-// thread each, so TI * TJ <= 1024 and a multiple of 32)
-// largest cluster of wavefront CTAs along x (1: no clusters)
-#ifndef CGLI_SWEEP_CLUSTER_MAX
-#define CGLI_SWEEP_CLUSTER_MAX 1
-#endif
+// Wavefront geometry per arithmetic type of the passes: TI x TJ (i, j)
+// columns per CTA (one thread each, so TI * TJ <= 1024 and a multiple of
+// 32), the depth of the ring of record stages in shared memory, and the
+// largest cluster of CTAs along x (1: no clusters).  Measured at
+// 256x192x192: the FP64 passes are fastest on 16 x 16 tiles with a 3-step
+// ring, the FP32 passes on 8 x 16 tiles in clusters of 8.
 #ifndef CGLI_SWEEP_TI
-#define CGLI_SWEEP_TI 8
+#define CGLI_SWEEP_TI 16
 #endif
 #ifndef CGLI_SWEEP_TJ
 #define CGLI_SWEEP_TJ 16
 #endif
-constexpr int SWEEP_TI = CGLI_SWEEP_TI;
-constexpr int SWEEP_TJ = CGLI_SWEEP_TJ;
-static_assert(SWEEP_TI * SWEEP_TJ <= 1024 && (SWEEP_TI * SWEEP_TJ) % 32 == 0, "sweep tile shape");
+#ifndef CGLI_SWEEP_RING
+#define CGLI_SWEEP_RING 3
+#endif
+#ifndef CGLI_SWEEP_CLUSTER_MAX
+#define CGLI_SWEEP_CLUSTER_MAX 1
+#endif
+#ifndef CGLI_SWEEP_TI_F32
+#define CGLI_SWEEP_TI_F32 8
+#endif
+#ifndef CGLI_SWEEP_TJ_F32
+#define CGLI_SWEEP_TJ_F32 16
+#endif
+#ifndef CGLI_SWEEP_RING_F32
+#define CGLI_SWEEP_RING_F32 2
+#endif
+#ifndef CGLI_SWEEP_CLUSTER_MAX_F32
+#define CGLI_SWEEP_CLUSTER_MAX_F32 8
+#endif
+template <typename T> struct SweepTile;
+template <> struct SweepTile<double> {
+  static constexpr int TI = CGLI_SWEEP_TI, TJ = CGLI_SWEEP_TJ, RING = CGLI_SWEEP_RING;
+  static constexpr int CLUSTER_MAX = CGLI_SWEEP_CLUSTER_MAX;
+};
+template <> struct SweepTile<float> {
+  static constexpr int TI = CGLI_SWEEP_TI_F32, TJ = CGLI_SWEEP_TJ_F32, RING = CGLI_SWEEP_RING_F32;
+  static constexpr int CLUSTER_MAX = CGLI_SWEEP_CLUSTER_MAX_F32;
+};
+static_assert(SweepTile<double>::TI * SweepTile<double>::TJ <= 1024 &&
+                  (SweepTile<double>::TI * SweepTile<double>::TJ) % 32 == 0, "FP64 sweep tile shape");
+static_assert(SweepTile<float>::TI * SweepTile<float>::TJ <= 1024 &&
+                  (SweepTile<float>::TI * SweepTile<float>::TJ) % 32 == 0, "FP32 sweep tile shape");
 constexpr int CGLI_TIMEOUT_CODE = 6;
 
 // buffers of the tile-wavefront sweeps (kernels_sweep.cu)
@@ -59,24 +87,31 @@ struct SweepArgs {
   int cluster_x;                  // wavefront CTAs per cluster along x (1: no clusters)
 };
 
-// slot of cell (i, j, k) in the tile-skewed layout
+// slot of cell (i, j, k) in the tile-skewed layout of the passes in type T
+template <typename T>
 __host__ __device__ __forceinline__ long long skew_slot(const Dev &d, int i, int j, int k) {
-  const int ntj = (d.ny + SWEEP_TJ - 1) / SWEEP_TJ;
-  const int S = d.nz + SWEEP_TI + SWEEP_TJ - 2;
-  const int il = (i - 3) % SWEEP_TI, jl = (j - 2) % SWEEP_TJ;
-  const int tile = ((i - 3) / SWEEP_TI) * ntj + (j - 2) / SWEEP_TJ;
+  constexpr int TI = SweepTile<T>::TI, TJ = SweepTile<T>::TJ;
+  const int ntj = (d.ny + TJ - 1) / TJ;
+  const int S = d.nz + TI + TJ - 2;
+  const int il = (i - 3) % TI, jl = (j - 2) % TJ;
+  const int tile = ((i - 3) / TI) * ntj + (j - 2) / TJ;
   const int s = (k - 2) + il + jl;
-  return ((long long)tile * S + s) * (SWEEP_TI * SWEEP_TJ) + il * SWEEP_TJ + jl;
+  return ((long long)tile * S + s) * (TI * TJ) + il * TJ + jl;
 }
+template <typename T>
 __host__ __device__ __forceinline__ long long skew_size(const Dev &d) {
-  const long long ntiles = (long long)((d.nx + SWEEP_TI - 1) / SWEEP_TI) * ((d.ny + SWEEP_TJ - 1) / SWEEP_TJ);
-  return ntiles * (d.nz + SWEEP_TI + SWEEP_TJ - 2) * (SWEEP_TI * SWEEP_TJ);
+  constexpr int TI = SweepTile<T>::TI, TJ = SweepTile<T>::TJ;
+  const long long ntiles = (long long)((d.nx + TI - 1) / TI) * ((d.ny + TJ - 1) / TJ);
+  return ntiles * (d.nz + TI + TJ - 2) * (TI * TJ);
 }
+// tiles of the wavefront in x and y for the passes in type T
+template <typename T> inline int sweep_tiles_x(int nx) { return (nx + SweepTile<T>::TI - 1) / SweepTile<T>::TI; }
+template <typename T> inline int sweep_tiles_y(int ny) { return (ny + SweepTile<T>::TJ - 1) / SweepTile<T>::TJ; }
 
 void sweep_tile_order(int nti, int ntj, std::vector<int> &order);
 // shared-memory opt-in of the wavefront kernels (once per process and device)
 cudaError_t sweep_kernel_attributes();
-int sweep_cluster_x(int nti, int ntj, int max_cx);
+int sweep_cluster_x(int nti, int ntj, bool mixed);
 // the four wavefront passes (two sweeps) of one inner iteration
 void launch_sweeps(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed);
 // the update and norm partials after the last pass (k_update_skewed)

@@ -1,6 +1,8 @@
 // Fast path of one inner iteration: halo and boundaries, fluxes, viscous
 // terms, residual assembly, four wavefront sweep passes with the update
 // fused into the last one.
+#include <type_traits>
+
 #include "cgli_dev.cuh"
 #include "cgli_launch.h"
 
@@ -39,7 +41,7 @@ __global__ void __launch_bounds__(64, CGLI_RESIDUAL_MINBLOCKS) k_residual_fast(D
 
   const int ie = d.nx + 2;
   const bool halo_plane = (i == 2 || i == ie + 1);
-  const long long slot = halo_plane ? 0 : skew_slot(d, i, j, k);
+  const long long slot = halo_plane ? 0 : skew_slot<typename std::conditional<MIXED, float, double>::type>(d, i, j, k);
   {
     // the cell's sweep record; planes 2 and ie+1 (the periodic halo copies)
     // go to the per-(j,k) halo records

@@ -62,18 +62,13 @@
 #ifndef CGLI_SWEEP_MINBLOCKS
 #define CGLI_SWEEP_MINBLOCKS 1
 #endif
-// steps of records in flight: the ring holds this many steps' blocks, the
-// copy of step s + RING - 1 is issued at step s
-#ifndef CGLI_SWEEP_RING
-#define CGLI_SWEEP_RING 2
-#endif
-// backward pass: bring the forward result dQ of each step in with the
-// records' bulk copy (five 1-value-per-thread rows) instead of plain loads
-#ifndef CGLI_SWEEP_DQ_BULK
-#define CGLI_SWEEP_DQ_BULK 0
-#endif
+// backward pass: the forward result dQ of each step arrives with the
+// records' bulk copy (five rows of one value per thread)
 
 namespace cgli {
+
+using F64 = SweepTile<double>;
+using F32 = SweepTile<float>;
 
 template <typename T> struct SweepPtrs;
 template <> struct SweepPtrs<double> {
@@ -209,44 +204,6 @@ __device__ __forceinline__ void load_cellrec(const float *p, float rec[REC_N], f
   }
 }
 
-// one cell's sweep inputs
-template <typename T>
-struct Cell {
-  bool active;
-  long long slot;   // tile-skewed slot
-  T rec[REC_N];     // split-Jacobian / diagonal record
-  T mr[5];          // forward: MR; backward: this cell's forward result
-  T hx[5];          // product from the periodic lagged halo (x edge of the slab)
-  bool has_hx;
-};
-
-template <int TI, int TJ, class Met, bool BACKWARD, typename T>
-__device__ __forceinline__ void fetch_cell(const Dev &d, const SweepArgs &a, const double *et, int il, int jl,
-                                           int j, int s, int S, long long tile_base, bool inside, bool halo_edge,
-                                           Cell<T> &x) {
-  const int rel = BACKWARD ? s - (TI - 1 - il) - (TJ - 1 - jl) : s - il - jl;
-  x.active = inside && rel >= 0 && rel < d.nz;
-  x.has_hx = false;
-  if (!x.active) return;
-  const int sf = BACKWARD ? S - 1 - s : s;   // forward step of this cell
-  const long long slot = tile_base + (long long)sf * (TI * TJ) + threadIdx.x;
-  x.slot = slot;
-  // the record (and, forward, MR) arrive in shared memory with the CTA's
-  // block of the step (k_sweep); backward, this cell's forward result
-  if (BACKWARD && !CGLI_SWEEP_DQ_BULK)
-#pragma unroll
-    for (int v = 0; v < 5; v++) x.mr[v] = SweepPtrs<T>::dq(a)[v][slot];
-  if (halo_edge) {
-    // periodic lagged halo: the x neighbour's product, formed before the
-    // pass (k_halo_products)
-    const int kl = BACKWARD ? d.nz - 1 - rel : rel;
-    const long long h = (long long)j * d.dj + 2 + kl;
-#pragma unroll
-    for (int v = 0; v < 5; v++) x.hx[v] = SweepPtrs<T>::hxp(a)[v][h];
-    x.has_hx = true;
-  }
-}
-
 // The x neighbour of the slab's first plane (forward) / last plane
 // (backward) is the periodic halo plane 2 / ie+1, a copy of plane ie / 3 made
 // by the Q halo exchange; its record and the lagged dQ are kept per (j, k).
@@ -305,8 +262,10 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
   // x hand-over ring inside a cluster: RX steps x TJ lanes x XW words
   constexpr int RX = 8, XW = sizeof(T) == 8 ? 6 : 8;
   __shared__ __align__(8) uint64_t s_full[CL ? RX : 1], s_empty[CL ? RX : 1];
-  constexpr int RING = CGLI_SWEEP_RING;
-  constexpr bool DQB = BACKWARD && CGLI_SWEEP_DQ_BULK;
+  // steps of records in flight: the ring holds RING steps' blocks, the copy
+  // of step s + RING - 1 is issued at step s
+  constexpr int RING = SweepTile<T>::RING;
+  constexpr bool DQB = BACKWARD;
   __shared__ __align__(8) uint64_t s_bar[RING];
   // the CTA's records of RING steps: step s's TI*TJ slots are one contiguous
   // block of TI*TJ*CR_N words in the tile-skewed layout, brought in with one
@@ -432,12 +391,29 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
   preload(0, px0, py0);
   preload(1, px1, py1);
 
-  Cell<T> cur, nxt;
-  fetch_cell<TI, TJ, Met, BACKWARD, T>(d, a, s_et, il, jl, j, 0, S, tile_base, inside, halo_edge, cur);
+  // the periodic lagged halo of the slab's x edge: the x neighbour's product,
+  // formed before the pass (k_halo_products), loaded a step ahead by the
+  // edge lanes
+  T hx_cur[5], hx_nxt[5];
+  auto load_hx = [&](int step, T *out) {
+    const int k2 = kl_of(step);
+    if (k2 < 0) return;
+    const long long h = (long long)j * d.dj + 2 + k2;
+#pragma unroll
+    for (int v = 0; v < 5; v++) out[v] = SweepPtrs<T>::hxp(a)[v][h];
+  };
+  if (halo_edge) load_hx(0, hx_cur);
+  // this thread's slot of step s: slot0 + (forward step) * TI * TJ
+  const long long slot0 = tile_base + threadIdx.x;
+  const int rel0 = BACKWARD ? -(TI - 1 - il) - (TJ - 1 - jl) : -il - jl;
 
+  // unrolled twice: the ring and buffer indices of the two halves are
+  // constants, and the compiler overlaps the halves' independent work
+#pragma unroll 2
   for (int s = 0; s < S; s++) {
-    const int rel = BACKWARD ? s - (TI - 1 - il) - (TJ - 1 - jl) : s - il - jl;
+    const int rel = rel0 + s;
     const int kl = BACKWARD ? Nz - 1 - rel : rel;
+    const bool active = inside && rel >= 0 && rel < Nz;
     // the slot read in step s - 1 is free again (every receiving lane read it
     // before the barrier that ended that step): arm it for its next use, then
     // give it back to the producer
@@ -448,24 +424,25 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
     // loads of the next cell go out first and land during the dependent part
     // stage (s + RING - 1) % RING was last read at step s - 1, before the previous barrier
     if (threadIdx.x == 0 && s + RING - 1 < S) issue(s + RING - 1);
-    if (s + 1 < S) fetch_cell<TI, TJ, Met, BACKWARD, T>(d, a, s_et, il, jl, j, s + 1, S, tile_base, inside, halo_edge, nxt);
-    else nxt.active = false;
+    if (halo_edge && s + 1 < S) load_hx(s + 1, hx_nxt);
     // this step's records (bounded wait; a timeout is reported like a tile's)
     if (!tc::mbar_wait(tc::smem_addr(&s_bar[s % RING]), (s / RING) & 1, kCopyPolls)) give_up(&s_dead, d.status);
-    if (cur.active) {
+    // the record and MR (forward) or this cell's forward result (backward)
+    T rec[REC_N], mr[5];
+    if (active) {
       const T *st = s_rec + (s % RING) * kStage;
-      load_cellrec(st + threadIdx.x * CR_N, cur.rec, BACKWARD ? (T *)nullptr : cur.mr);
+      load_cellrec(st + threadIdx.x * CR_N, rec, BACKWARD ? (T *)nullptr : mr);
       if (DQB)
 #pragma unroll
-        for (int v = 0; v < 5; v++) cur.mr[v] = st[TI * TJ * CR_N + v * TI * TJ + threadIdx.x];
+        for (int v = 0; v < 5; v++) mr[v] = st[TI * TJ * CR_N + v * TI * TJ + threadIdx.x];
     }
     T ox[5];
-    if (cur.active) {
+    if (active) {
       const int pbuf = (s - 1) & 1;
       T tx[5], ty[5];
-      if (cur.has_hx) {
+      if (halo_edge) {
 #pragma unroll
-        for (int v = 0; v < 5; v++) tx[v] = cur.hx[v];
+        for (int v = 0; v < 5; v++) tx[v] = hx_cur[v];
       } else if (!recv_x) {
         const int sil = BACKWARD ? il + 1 : il - 1;
 #pragma unroll
@@ -502,23 +479,23 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
       T L[5];
 #pragma unroll
       for (int v = 0; v < 5; v++) L[v] = tx[v] * rdx + ty[v] * rdy + (zedge ? (T)0 : carry_z[v]) * rdz;
-      const T d11 = cur.rec[R_D11], d22 = cur.rec[R_D22], d51 = cur.rec[R_D51];
+      const T d11 = rec[R_D11], d22 = rec[R_D22], d51 = rec[R_D51];
       T n[5];
       if (!BACKWARD) {
         // Dual_time_stepping.cpp:1289-1293
-        T r1 = cur.mr[0] - L[0];
+        T r1 = mr[0] - L[0];
         n[0] = d11 * r1;
-        n[1] = d22 * (cur.mr[1] - L[1]);
-        n[2] = d22 * (cur.mr[2] - L[2]);
-        n[3] = d22 * (cur.mr[3] - L[3]);
-        n[4] = d51 * r1 + d22 * (cur.mr[4] - L[4]);
+        n[1] = d22 * (mr[1] - L[1]);
+        n[2] = d22 * (mr[2] - L[2]);
+        n[3] = d22 * (mr[3] - L[3]);
+        n[4] = d51 * r1 + d22 * (mr[4] - L[4]);
       } else {
         // Dual_time_stepping.cpp:1651-1655 (mr holds this cell's forward result)
-        n[0] = cur.mr[0] - d11 * L[0];
-        n[1] = cur.mr[1] - d22 * L[1];
-        n[2] = cur.mr[2] - d22 * L[2];
-        n[3] = cur.mr[3] - d22 * L[3];
-        n[4] = cur.mr[4] - (d51 * L[0] + d22 * L[4]);
+        n[0] = mr[0] - d11 * L[0];
+        n[1] = mr[1] - d22 * L[1];
+        n[2] = mr[2] - d22 * L[2];
+        n[3] = mr[3] - d22 * L[3];
+        n[4] = mr[4] - (d51 * L[0] + d22 * L[4]);
       }
       const long long c = Met::kChannel ? 0 : ix(d, i, j, 2 + kl);
       T mm[9];
@@ -528,13 +505,13 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
         // the channel's face metrics have one nonzero component per
         // direction (1, etdy, 1 on the x, y, z components), so only the
         // nonzero split entries are formed and applied
-        channel_products<T, 0, BACKWARD>(cur.rec, (T)1, n, ox);
-        channel_products<T, 1, BACKWARD>(cur.rec, mm[4], n, oy);
-        channel_products<T, 2, BACKWARD>(cur.rec, (T)1, n, carry_z);
+        channel_products<T, 0, BACKWARD>(rec, (T)1, n, ox);
+        channel_products<T, 1, BACKWARD>(rec, mm[4], n, oy);
+        channel_products<T, 2, BACKWARD>(rec, (T)1, n, carry_z);
       } else {
-        Split<T> Ax = split_from_record<T>(cur.rec, 0, mm[0], mm[1], mm[2]);
-        Split<T> Ay = split_from_record<T>(cur.rec, 1, mm[3], mm[4], mm[5]);
-        Split<T> Az = split_from_record<T>(cur.rec, 2, mm[6], mm[7], mm[8]);
+        Split<T> Ax = split_from_record<T>(rec, 0, mm[0], mm[1], mm[2]);
+        Split<T> Ay = split_from_record<T>(rec, 1, mm[3], mm[4], mm[5]);
+        Split<T> Az = split_from_record<T>(rec, 2, mm[6], mm[7], mm[8]);
         if (BACKWARD) {
           upper_terms<T>(Ax, n, ox);
           upper_terms<T>(Ay, n, oy);
@@ -560,7 +537,7 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
       }
       {
 #pragma unroll
-        for (int v = 0; v < 5; v++) dq[v][cur.slot] = n[v];
+        for (int v = 0; v < 5; v++) dq[v][slot0 + (long long)(BACKWARD ? S - 1 - s : s) * (TI * TJ)] = n[v];
         if (BACKWARD && !d.x_open) {
           // lagged halos of the next sweep: plane ie feeds its forward pass,
           // plane 3 its backward pass (an open slab's halos stay zero)
@@ -585,7 +562,7 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
         // outside the slab), so the consumer's byte count always completes
         T o5[5];
 #pragma unroll
-        for (int v = 0; v < 5; v++) o5[v] = cur.active ? ox[v] : (T)0;
+        for (int v = 0; v < 5; v++) o5[v] = active ? ox[v] : (T)0;
         const uint32_t dst = tc::mapa(tc::smem_addr(s_rx + ((q % RX) * TJ + jl) * XW), consumer);
         const uint32_t bar = tc::mapa(tc::smem_addr(&s_full[q % RX]), consumer);
         if (sizeof(T) == 8) {
@@ -603,7 +580,9 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
       for (int v = 0; v < 5; v++) { px0[v] = px1[v]; py0[v] = py1[v]; }
       if (s + 2 < S) preload(s + 2, px1, py1);
     }
-    cur = nxt;
+    if (halo_edge)
+#pragma unroll
+      for (int v = 0; v < 5; v++) hx_cur[v] = hx_nxt[v];
     __syncthreads();
   }
   // the cluster's CTAs leave together: none while another can still write
@@ -625,7 +604,7 @@ __global__ void __launch_bounds__(128) k_update_skewed(Dev d, SweepArgs a) {
   T *const *dq = SweepPtrs<T>::dq(a);
   double acc[5] = {0, 0, 0, 0, 0};
   for (int k = 2 + threadIdx.x; k <= d.nz + 1; k += blockDim.x) {
-    const long long c = ix(d, i, j, k), slot = skew_slot(d, i, j, k);
+    const long long c = ix(d, i, j, k), slot = skew_slot<T>(d, i, j, k);
     const double J = d.J[c], iJ = d.iJ[c];
     const double q1 = d.U_[0][c], iq1 = 1 / q1;
     const double rhoold = q1 * J;
@@ -654,7 +633,7 @@ __global__ void __launch_bounds__(128) k_update_skewed(Dev d, SweepArgs a) {
 // dynamic shared memory of a wavefront pass: the ring of record stages
 template <int TI, int TJ, typename T>
 constexpr int sweep_smem_bytes(bool backward, bool cluster) {
-  return CGLI_SWEEP_RING * TI * TJ * (CR_N + (backward && CGLI_SWEEP_DQ_BULK ? 5 : 0)) * (int)sizeof(T) +
+  return SweepTile<T>::RING * TI * TJ * (CR_N + (backward ? 5 : 0)) * (int)sizeof(T) +
          (cluster ? 8 * TJ * (sizeof(T) == 8 ? 6 : 8) * (int)sizeof(T) : 0);   // the cluster's x hand-over ring
 }
 
@@ -715,11 +694,11 @@ static void run_sweeps(const Dev &d, const SweepArgs &a, cudaStream_t s) {
 
 void launch_sweep_pass(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed, bool backward, bool final_pass) {
   if (mixed) {
-    if (a.channel_metrics) run_one_pass<SWEEP_TI, SWEEP_TJ, MetricsChannel, float>(d, a, s, backward, final_pass);
-    else run_one_pass<SWEEP_TI, SWEEP_TJ, MetricsGeneral, float>(d, a, s, backward, final_pass);
+    if (a.channel_metrics) run_one_pass<F32::TI, F32::TJ, MetricsChannel, float>(d, a, s, backward, final_pass);
+    else run_one_pass<F32::TI, F32::TJ, MetricsGeneral, float>(d, a, s, backward, final_pass);
   } else {
-    if (a.channel_metrics) run_one_pass<SWEEP_TI, SWEEP_TJ, MetricsChannel, double>(d, a, s, backward, final_pass);
-    else run_one_pass<SWEEP_TI, SWEEP_TJ, MetricsGeneral, double>(d, a, s, backward, final_pass);
+    if (a.channel_metrics) run_one_pass<F64::TI, F64::TJ, MetricsChannel, double>(d, a, s, backward, final_pass);
+    else run_one_pass<F64::TI, F64::TJ, MetricsGeneral, double>(d, a, s, backward, final_pass);
   }
 }
 
@@ -727,12 +706,12 @@ void launch_sweep_pass(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mi
 // two-step record buffer) exceeds 48 KB: opt in once, outside any capture
 template <class Met, typename T, bool CL>
 static cudaError_t opt_in() {
-  cudaError_t e = cudaFuncSetAttribute(k_sweep<SWEEP_TI, SWEEP_TJ, Met, false, T, CL>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       sweep_smem_bytes<SWEEP_TI, SWEEP_TJ, T>(false, CL));
+  constexpr int TI = SweepTile<T>::TI, TJ = SweepTile<T>::TJ;
+  cudaError_t e = cudaFuncSetAttribute(k_sweep<TI, TJ, Met, false, T, CL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       sweep_smem_bytes<TI, TJ, T>(false, CL));
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_sweep<SWEEP_TI, SWEEP_TJ, Met, true, T, CL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             sweep_smem_bytes<SWEEP_TI, SWEEP_TJ, T>(true, CL));
+    e = cudaFuncSetAttribute(k_sweep<TI, TJ, Met, true, T, CL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             sweep_smem_bytes<TI, TJ, T>(true, CL));
   return e;
 }
 cudaError_t sweep_kernel_attributes() {
@@ -740,26 +719,30 @@ cudaError_t sweep_kernel_attributes() {
   if (e == cudaSuccess) e = opt_in<MetricsGeneral, double, false>();
   if (e == cudaSuccess) e = opt_in<MetricsChannel, float, false>();
   if (e == cudaSuccess) e = opt_in<MetricsGeneral, float, false>();
-#if CGLI_SWEEP_CLUSTER_MAX > 1
-  if (e == cudaSuccess) e = opt_in<MetricsChannel, double, true>();
-  if (e == cudaSuccess) e = opt_in<MetricsGeneral, double, true>();
-  if (e == cudaSuccess) e = opt_in<MetricsChannel, float, true>();
-  if (e == cudaSuccess) e = opt_in<MetricsGeneral, float, true>();
-#endif
+  if (SweepTile<double>::CLUSTER_MAX > 1) {
+    if (e == cudaSuccess) e = opt_in<MetricsChannel, double, true>();
+    if (e == cudaSuccess) e = opt_in<MetricsGeneral, double, true>();
+  }
+  if (SweepTile<float>::CLUSTER_MAX > 1) {
+    if (e == cudaSuccess) e = opt_in<MetricsChannel, float, true>();
+    if (e == cudaSuccess) e = opt_in<MetricsGeneral, float, true>();
+  }
   return e;
 }
 
-// The cluster size along x for a grid of nti x ntj tiles: the largest of
-// max_cx, max_cx/2, ... (at least 2) that divides nti and of which the
-// device can hold at least `need` clusters of the largest wavefront kernel
-// at once; 1 (no clusters) otherwise.
-int sweep_cluster_x(int nti, int ntj, int max_cx) {
-  for (int cx = max_cx; cx >= 2; cx /= 2) {
+// The cluster size along x of the passes in type T for a grid of nti x ntj
+// tiles: the largest of CLUSTER_MAX, CLUSTER_MAX/2, ... (at least 2) that
+// divides nti and of which the device can hold at least one cluster of the
+// largest wavefront kernel; 1 (no clusters) otherwise.
+template <typename T>
+static int cluster_x_for(int nti, int ntj) {
+  constexpr int TI = SweepTile<T>::TI, TJ = SweepTile<T>::TJ;
+  for (int cx = SweepTile<T>::CLUSTER_MAX; cx >= 2; cx /= 2) {
     if (nti % cx) continue;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(nti * ntj);
-    cfg.blockDim = dim3(SWEEP_TI * SWEEP_TJ);
-    cfg.dynamicSmemBytes = sweep_smem_bytes<SWEEP_TI, SWEEP_TJ, double>(true, true);
+    cfg.blockDim = dim3(TI * TJ);
+    cfg.dynamicSmemBytes = sweep_smem_bytes<TI, TJ, T>(true, true);
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = cx;
@@ -768,14 +751,16 @@ int sweep_cluster_x(int nti, int ntj, int max_cx) {
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     int n = 0;
-    if (cudaOccupancyMaxActiveClusters(&n, k_sweep<SWEEP_TI, SWEEP_TJ, MetricsGeneral, true, double, true>, &cfg) !=
-        cudaSuccess) {
+    if (cudaOccupancyMaxActiveClusters(&n, k_sweep<TI, TJ, MetricsGeneral, true, T, true>, &cfg) != cudaSuccess) {
       cudaGetLastError();
       continue;
     }
     if (n >= 1) return cx;
   }
   return 1;
+}
+int sweep_cluster_x(int nti, int ntj, bool mixed) {
+  return mixed ? cluster_x_for<float>(nti, ntj) : cluster_x_for<double>(nti, ntj);
 }
 
 void launch_sweep_update(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed) {
@@ -785,11 +770,11 @@ void launch_sweep_update(const Dev &d, const SweepArgs &a, cudaStream_t s, bool 
 
 void launch_sweeps(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed) {
   if (mixed) {
-    if (a.channel_metrics) run_sweeps<SWEEP_TI, SWEEP_TJ, MetricsChannel, float>(d, a, s);
-    else run_sweeps<SWEEP_TI, SWEEP_TJ, MetricsGeneral, float>(d, a, s);
+    if (a.channel_metrics) run_sweeps<F32::TI, F32::TJ, MetricsChannel, float>(d, a, s);
+    else run_sweeps<F32::TI, F32::TJ, MetricsGeneral, float>(d, a, s);
   } else {
-    if (a.channel_metrics) run_sweeps<SWEEP_TI, SWEEP_TJ, MetricsChannel, double>(d, a, s);
-    else run_sweeps<SWEEP_TI, SWEEP_TJ, MetricsGeneral, double>(d, a, s);
+    if (a.channel_metrics) run_sweeps<F64::TI, F64::TJ, MetricsChannel, double>(d, a, s);
+    else run_sweeps<F64::TI, F64::TJ, MetricsGeneral, double>(d, a, s);
   }
 }
 

@@ -59,7 +59,7 @@ def main(argv=None) -> None:
         for _ in range(2):
             sol.inner_iteration()
         st = sol.profile_stages(a.stages)
-        ti, tj = sweep_tile_shape()
+        ti, tj = sweep_tile_shape(FP64 if a.precision == "fp64" else MIXED)
         nsteps = wavefront_steps(ch.nx, ch.ny, ch.nz, ti, tj)
         print(json.dumps({"cells": [ch.nx, ch.ny, ch.nz], "stage_ms": {k: round(v, 4) for k, v in st.items()},
                           "tile": [ti, tj], "wavefront_steps": nsteps,

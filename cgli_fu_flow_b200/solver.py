@@ -100,7 +100,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cgli_profile_stages.argtypes = [P, ctypes.c_int, DP]
     L.cgli_set_predictor.argtypes = [P, ctypes.c_int]
     L.cgli_set_wait_limit.argtypes = [P, ctypes.c_int]
-    L.cgli_sweep_tile_shape.argtypes = [ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+    L.cgli_sweep_tile_shape.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
     L.cgli_filter.argtypes = [P, D, D, D]
     F = ctypes.c_float
     FP = ctypes.POINTER(ctypes.c_float)
@@ -444,11 +444,12 @@ class Solver:
         return it.value, np.array(er[:])
 
 
-def sweep_tile_shape() -> tuple[int, int]:
-    """(ti, tj): the wavefront tile the loaded library was built with."""
+def sweep_tile_shape(precision: int = FP64) -> tuple[int, int]:
+    """(ti, tj): the wavefront tile the loaded library was built with for
+    passes of the given precision."""
     L = load_library()
     ti, tj = ctypes.c_int(), ctypes.c_int()
-    rc = L.cgli_sweep_tile_shape(ctypes.byref(ti), ctypes.byref(tj))
+    rc = L.cgli_sweep_tile_shape(precision, ctypes.byref(ti), ctypes.byref(tj))
     if rc:
         raise CgliError(rc, L.cgli_last_error().decode())
     return ti.value, tj.value

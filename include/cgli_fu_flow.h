@@ -229,10 +229,11 @@ int cgli_set_predictor(cgli_ctx *ctx, int mode);
 #define CGLI_WAIT_LIMIT_DEFAULT 4194304
 int cgli_set_wait_limit(cgli_ctx *ctx, int polls);
 /* The (i, j) column tile of the wavefront passes this library was built
- * with (no counterpart in the reference, which sweeps whole hyperplanes):
- * each pass takes Nz + ti + tj - 2 + ti (ceil(Nx/ti) - 1) + tj (ceil(Ny/tj) - 1)
- * dependent steps.  Host only. */
-int cgli_sweep_tile_shape(int *ti, int *tj);
+ * with for CGLI_FP64 or CGLI_MIXED passes (no counterpart in the reference,
+ * which sweeps whole hyperplanes): each pass takes
+ * Nz + ti + tj - 2 + ti (ceil(Nx/ti) - 1) + tj (ceil(Ny/tj) - 1) dependent
+ * steps.  Host only. */
+int cgli_sweep_tile_shape(int precision, int *ti, int *tj);
 
 /* ---- learned initial guess (no counterpart in the reference).  A 3-D
  * convolutional network, 15 -> 32 -> 32 -> 32 -> 32 -> 5 channels, 3x3x3

@@ -142,6 +142,9 @@ def test_wavefront_step_count():
 
 def test_library_reports_its_tile_shape(cuda_lib):
     """The tile shape comes from the library itself (set at build time)."""
-    from cgli_fu_flow_b200.solver import sweep_tile_shape
-    ti, tj = sweep_tile_shape()
-    assert ti >= 1 and tj >= 1 and (ti * tj) % 32 == 0
+    from cgli_fu_flow_b200.solver import FP64, MIXED, CgliError, sweep_tile_shape
+    for precision in (FP64, MIXED):
+        ti, tj = sweep_tile_shape(precision)
+        assert ti >= 1 and tj >= 1 and (ti * tj) % 32 == 0
+    with pytest.raises(CgliError):
+        sweep_tile_shape(7)
