@@ -43,7 +43,14 @@
 // with a relaxed arrival on the producer's "empty" barrier.  No fence is on
 // either path.  The first (last) tile of a cluster still receives (sends)
 // through the global buffers.  A cluster takes one ticket for its whole row
-// of tiles.
+// of tiles.  A CTA must not leave while a push into its shared memory is
+// still in flight, and a slot must not be re-armed before its phase has
+// completed, so the receiving lanes wait on every hand-over step, whether
+// their own cell is inside the slab or not, and these waits do not give up
+// at the tile wait limit or on the dead flag: the producer always pushes
+// every step (it is co-scheduled with the consumer and its own waits are
+// bounded), so they have the fixed bound of a copy wait, scaled by the wait
+// limit because the producer may itself sit in one wait of that length.
 //
 // The periodic x halo keeps the reference's lag: the forward pass at i = 3
 // uses dQ of plane Nx+2 as it was at the start of the sweep (halo_f), the
@@ -358,6 +365,9 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
   // the step q of the consumer's wait is the producer's step q + TI - 1
   const int QN = S - TI + 1;   // hand-over steps per pass
   constexpr uint32_t kPush = TJ * 5 * sizeof(T);   // bytes pushed per hand-over step (armed above for the first RX)
+  // the lanes that wait on the pushes: the tile's receiving edge, all of them
+  const bool wait_x = dsm_recv && (BACKWARD ? il == TI - 1 : il == 0);
+  const int push_polls = a.spin_limit > (0x7fffffff - kCopyPolls) / 64 ? 0x7fffffff : 64 * a.spin_limit + kCopyPolls;
   const T rdx = (T)(1.0 / d.dxi), rdy = (T)(1.0 / d.det), rdz = (T)(1.0 / d.dzt);
   T *xb = SweepPtrs<T>::xb(a), *yb = SweepPtrs<T>::yb(a);
   T *const *dq = SweepPtrs<T>::dq(a);
@@ -427,6 +437,11 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
     if (halo_edge && s + 1 < S) load_hx(s + 1, hx_nxt);
     // this step's records (bounded wait; a timeout is reported like a tile's)
     if (!tc::mbar_wait(tc::smem_addr(&s_bar[s % RING]), (s / RING) & 1, kCopyPolls)) give_up(&s_dead, d.status);
+    // the cluster neighbour's push of this step (every receiving lane, so
+    // that every push has landed before the slot is re-armed or the CTA leaves)
+    if (wait_x && s < QN &&
+        !tc::mbar_wait_cluster(tc::smem_addr(&s_full[s % RX]), (s / RX) & 1, push_polls))
+      give_up(&s_dead, d.status);
     // the record and MR (forward) or this cell's forward result (backward)
     T rec[REC_N], mr[5];
     if (active) {
@@ -448,11 +463,8 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
 #pragma unroll
         for (int v = 0; v < 5; v++) tx[v] = sx[pbuf][sil][jl][v];
       } else if (dsm_recv) {
-        // pushed by the producing CTA of the cluster (step s < QN here)
-        const uint32_t fb = tc::smem_addr(&s_full[s % RX]);
-        if (!tc::mbar_wait_cluster(fb, (s / RX) & 1, 1) &&
-            !tc::mbar_wait_cluster(fb, (s / RX) & 1, given_up(&s_dead, d.status) ? 0 : a.spin_limit))
-          give_up(&s_dead, d.status);
+        // pushed by the producing CTA of the cluster (step s < QN here; the
+        // wait above has seen it land)
         const T *src = s_rx + ((s % RX) * TJ + jl) * XW;
 #pragma unroll
         for (int v = 0; v < 5; v++) tx[v] = src[v];
@@ -552,7 +564,9 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
     if (dsm_send && send_x && s >= TI - 1) {
       const int q = s - (TI - 1);
       // the slot's previous use must have been read by the consumer (after
-      // a give-up the push goes ahead regardless: its values are unused)
+      // a give-up the push goes ahead regardless: its values are unused, and
+      // an early push only counts its bytes ahead on the consumer's next
+      // phase, which the consumer arms once it has seen the previous one)
       const uint32_t eb = tc::smem_addr(&s_empty[q % RX]);
       if (q >= RX && !tc::mbar_wait_cluster(eb, ((q / RX) - 1) & 1, 1) &&
           !tc::mbar_wait_cluster(eb, ((q / RX) - 1) & 1, given_up(&s_dead, d.status) ? 0 : a.spin_limit))
