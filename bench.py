@@ -278,6 +278,7 @@ def run_gpu(a, dist: Dist) -> dict | None:
         "clocks": ck,
         "stage_ms": {k: round(v, 4) for k, v in stages.items()},
         "roofline": roof,
+        "roofline_residual": roofline.residual_roofline(ch, stages),
         "gpu_launches": int(sum(launches_per_iteration(ch) * n + 3 for n in iters)),
     }
     if e2e:

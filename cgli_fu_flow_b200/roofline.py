@@ -48,3 +48,24 @@ def sweep_roofline(ch, pass_ms: float, precision: str) -> dict:
             "achieved": round(achieved, 1), "peak": peak, "peak_kind": kind, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": None if tpc is None else int(tpc * cells),
             "algorithmic_bytes_per_launch": bpc * cells, "launch_ms": round(dur_ms, 4)}
+
+
+# Algorithmic bytes of the residual side of one inner iteration per cell
+# (halo and boundaries, the three flux sweeps, the viscous terms and the
+# residual assembly together), the per-unit figure of the hot-path scope:
+# Q at three time levels (15), J and nine cell metrics (10), three face sets
+# of J_f and nine metrics (30), written MR (5): 60 doubles = 480 B.
+RESIDUAL_BYTES_PER_CELL = 60 * 8
+RESIDUAL_STAGES = ("halo_bc", "flux_x", "flux_y", "flux_z", "viscous", "residual")
+
+
+def residual_roofline(ch, stage_ms: dict) -> dict:
+    """stage_ms: device milliseconds per stage of one inner iteration."""
+    dur_ms = sum(stage_ms[k] for k in RESIDUAL_STAGES)
+    achieved = RESIDUAL_BYTES_PER_CELL * ch.cells / (dur_ms / 1e3) / 1e9
+    peak, kind = hbm_peak()
+    return {"kernels": "halo/boundaries, k_flux_x/y/z, k_vprim + k_viscous_faces + k_viscous_div, k_residual_fast",
+            "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "peak_kind": kind, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "algorithmic_bytes_per_iteration": RESIDUAL_BYTES_PER_CELL * ch.cells,
+            "ms_per_iteration": round(dur_ms, 4)}
+
