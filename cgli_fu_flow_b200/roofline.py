@@ -20,12 +20,13 @@ PEAKS = os.path.join(os.path.dirname(HERE), "MEASURED_PEAKS.json")
 SWEEP_BYTES_PER_CELL = {"fp64": 25 * 8, "mixed": 25 * 4}
 
 # DRAM bytes (read + write) per cell of one sweep pass from an ncu capture of
-# k_sweep (dram__bytes_read.sum + dram__bytes_write.sum, forward and backward
-# averaged), on the 160x128x128 channel; traffic grows with the cell count,
-# so it is scaled to the benchmark grid.  The passes read each cell's
-# 20-word record block (the backward pass also its forward result) and
-# write 5 words.  See profiles/k_sweep_channel_160x128x128.md.
-MEASURED_TRAFFIC_PER_CELL = {"fp64": (236.0 + 278.6) / 2, "mixed": None}
+# the current k_sweep (16 x 16-column FP64 tiles; dram__bytes_read.sum +
+# dram__bytes_write.sum, forward 243 B and backward 291 B per cell, averaged)
+# on the 160x128x128 channel; traffic grows with the cell count, so it is
+# scaled to the benchmark grid.  The passes read each cell's 20-word record
+# block (the backward pass also its forward result) and write 5 words.  See
+# profiles/k_sweep_channel_160x128x128.md.
+MEASURED_TRAFFIC_PER_CELL = {"fp64": (243.3 + 290.6) / 2, "mixed": None}
 
 
 def hbm_peak() -> tuple[float, str]:
