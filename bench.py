@@ -335,7 +335,7 @@ def run_arms(a, ch, dist) -> dict:
                 host[k] = physical_levels(base, np.float32)
     collect_s = time.perf_counter() - t0
     sc = [scales_from_levels([host[k] for k in range(q, q + 4)]) for q in quads]
-    net.set_scales(*[np.mean([x[i] for x in sc], axis=0) for i in range(3)])
+    net.set_scales(*[np.mean([x[i] for x in sc], axis=0) for i in range(len(sc[0]))])
     del host
     npairs = net.levels - 3
     ntrain = max(1, npairs - 4)       # the last four pairs are held out
@@ -449,7 +449,7 @@ def train_on_subbox(a, ch):
                 host[k] = physical_levels(s, np.float32)
     collect_s = time.perf_counter() - t0
     sc = [scales_from_levels([host[k] for k in range(q, q + 4)]) for q in quads]
-    scales = [np.mean([x[i] for x in sc], axis=0) for i in range(3)]
+    scales = [np.mean([x[i] for x in sc], axis=0) for i in range(len(sc[0]))]
     nb.set_scales(*scales)
     t0 = time.perf_counter()
     loss = nb.train(a.subbox_train_steps, a.lr, 20261204, 0, a.subbox_pairs)

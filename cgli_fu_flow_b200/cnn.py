@@ -67,8 +67,10 @@ class Network:
         self._rc(self.L.cgli_cnn_get_params(self.h, t.ctypes.data))
         return t
 
-    def set_scales(self, mean, std, oscale) -> None:
-        a = [np.ascontiguousarray(x, dtype=np.float64) for x in (mean, std, oscale)]
+    def set_scales(self, mean, std, d1, d2, oscale) -> None:
+        """Input scales of the level (mean, std) and of its first and second
+        time differences (RMS d1, d2); output scale of the correction."""
+        a = [np.ascontiguousarray(x, dtype=np.float64) for x in (mean, std, d1, d2, oscale)]
         self._rc(self.L.cgli_cnn_set_scales(self.h, *[x.ctypes.data for x in a]))
 
     # ---- host-data entry points (tests)
@@ -134,14 +136,20 @@ CNN_TC_FLOP_PER_CELL = 2 * 27 * 32 * 32 * 5
 
 
 def scales_from_levels(levels: list[np.ndarray]):
-    """Per-variable input mean / std over the given levels and the output
-    scale: the RMS of the extrapolation residual over consecutive quadruples."""
+    """Per-variable input scales over the given consecutive levels -- the
+    levels' mean and std, the RMS of their first and of their second time
+    differences -- and the output scale: the RMS of the extrapolation
+    residual over consecutive quadruples.  Returns (mean, std, d1, d2, oscale)."""
     q = np.stack(levels)
     mean = q.mean(axis=(0, 2, 3, 4))
     std = q.std(axis=(0, 2, 3, 4))
-    res = [levels[i + 3] - (3 * levels[i + 2] - 3 * levels[i + 1] + levels[i]) for i in range(len(levels) - 3)]
-    r = np.stack(res)
-    osc = np.sqrt((r ** 2).mean(axis=(0, 2, 3, 4)))
-    std = np.where(std > 0, std, 1.0)
-    osc = np.where(osc > 0, osc, 1.0)
-    return mean, std, osc
+
+    def rms(xs):
+        r = np.stack(xs)
+        return np.sqrt((r ** 2).mean(axis=(0, 2, 3, 4)))
+
+    d1 = rms([levels[i + 1] - levels[i] for i in range(len(levels) - 1)])
+    d2 = rms([(levels[i + 2] - levels[i + 1]) - (levels[i + 1] - levels[i]) for i in range(len(levels) - 2)])
+    osc = rms([levels[i + 3] - (3 * levels[i + 2] - 3 * levels[i + 1] + levels[i]) for i in range(len(levels) - 3)])
+    pos = lambda a: np.where(a > 0, a, 1.0)
+    return mean, pos(std), pos(d1), pos(d2), pos(osc)

@@ -5,6 +5,13 @@
 // no counterpart in the reference; this file holds its tensor-core training
 // and inference kernels and their C ABI.
 //
+// Inputs per variable: the level Q^n (less its mean, over its spread), and
+// its first and second time differences Q^n - Q^(n-1) and
+// Q^n - 2 Q^(n-1) + Q^(n-2), each over its own RMS.  A step changes Q by
+// about one part in the grid size of its spatial spread, which is below the
+// resolution of a BF16 level; the differences, formed in FP32 / FP64 before
+// the conversion, keep that information.
+//
 // Data layout.  Activations and gradients are BF16, channel-last, on the
 // interior grid padded by one cell in every direction: [Nx+2][Ny+2][Nz+2][32]
 // (64 bytes per cell; layer inputs with fewer channels are zero padded to
@@ -434,7 +441,9 @@ __global__ void k_halo(bf16 *buf, int nx, int ny, int nz) {
   for (int q = 0; q < 4; q++) dst[q] = src[q];
 }
 
-struct Scales { float mean[5], inv_std[5], oscale[5], inv_oscale[5]; };
+// Input scales: per variable the level's mean and 1/std, and 1/RMS of its
+// first and second time differences; output scale of the correction.
+struct Scales { float mean[5], inv_std[5], inv_d1[5], inv_d2[5], oscale[5], inv_oscale[5]; };
 
 // network input from 15 host-normalised channels [15][cells] (tests)
 __global__ void k_pack_normalised(const float *x0, bf16 *act, int nx, int ny, int nz) {
@@ -478,8 +487,8 @@ __global__ void k_pack_levels(const float *l0, const float *l1, const float *l2,
   for (int v = 0; v < 5; v++) {
     const float qn = l2[v * cells + id], q1 = l1[v * cells + id], q2 = l0[v * cells + id];
     f[v] = (qn - s.mean[v]) * s.inv_std[v];
-    f[5 + v] = (q1 - s.mean[v]) * s.inv_std[v];
-    f[10 + v] = (q2 - s.mean[v]) * s.inv_std[v];
+    f[5 + v] = (qn - q1) * s.inv_d1[v];
+    f[10 + v] = ((qn - q1) - (q1 - q2)) * s.inv_d2[v];
     ex[v] = 3.f * qn - 3.f * q1 + q2;
   }
 #pragma unroll
@@ -514,9 +523,10 @@ __global__ void k_pack_state(Dev d, bf16 *act, Scales s) {
   float f[32];
 #pragma unroll
   for (int v = 0; v < 5; v++) {
-    f[v] = ((float)(d.U[v][o] * J) - s.mean[v]) * s.inv_std[v];
-    f[5 + v] = ((float)(d.Uq[v][o] * J) - s.mean[v]) * s.inv_std[v];
-    f[10 + v] = ((float)(d.Uqq[v][o] * J) - s.mean[v]) * s.inv_std[v];
+    const float qn = (float)(d.U[v][o] * J), q1 = (float)(d.Uq[v][o] * J), q2 = (float)(d.Uqq[v][o] * J);
+    f[v] = (qn - s.mean[v]) * s.inv_std[v];
+    f[5 + v] = (qn - q1) * s.inv_d1[v];
+    f[10 + v] = ((qn - q1) - (q1 - q2)) * s.inv_d2[v];
   }
 #pragma unroll
   for (int c = 15; c < 32; c++) f[c] = 0.f;
@@ -977,7 +987,10 @@ int cgli_cnn_create(int nx, int ny, int nz, cgli_cnn **out) {
         !act_map(&n->act6[l], n->act[l], nx, ny, nz, 6) || !act_map(&n->act7[l], n->act[l], nx, ny, nz, 7))
       rc = cfail(CGLI_ECUDA, "cuTensorMapEncodeTiled failed");
   }
-  for (int v = 0; v < 5; v++) { n->sc.mean[v] = 0.f; n->sc.inv_std[v] = 1.f; n->sc.oscale[v] = 1.f; n->sc.inv_oscale[v] = 1.f; }
+  for (int v = 0; v < 5; v++) {
+    n->sc.mean[v] = 0.f; n->sc.inv_std[v] = 1.f; n->sc.inv_d1[v] = 1.f; n->sc.inv_d2[v] = 1.f;
+    n->sc.oscale[v] = 1.f; n->sc.inv_oscale[v] = 1.f;
+  }
   if (rc) {
     for (void *p : n->allocs) cudaFree(p);
     if (n->h_loss) cudaFreeHost(n->h_loss);
@@ -1037,12 +1050,17 @@ int cgli_cnn_get_params(cgli_cnn *n, float *theta) {
   return copy_out_params(n, n->W, n->b, theta);
 }
 
-int cgli_cnn_set_scales(cgli_cnn *n, const double mean[5], const double stdv[5], const double oscale[5]) {
-  if (!n || !mean || !stdv || !oscale) return cfail(CGLI_EINVAL, "null argument");
+int cgli_cnn_set_scales(cgli_cnn *n, const double mean[5], const double stdv[5], const double d1[5],
+                        const double d2[5], const double oscale[5]) {
+  if (!n || !mean || !stdv || !d1 || !d2 || !oscale) return cfail(CGLI_EINVAL, "null argument");
+  for (int v = 0; v < 5; v++)
+    if (!(stdv[v] > 0) || !(d1[v] > 0) || !(d2[v] > 0) || !(oscale[v] > 0))
+      return cfail(CGLI_EINVAL, "scales must be positive");
   for (int v = 0; v < 5; v++) {
-    if (!(stdv[v] > 0) || !(oscale[v] > 0)) return cfail(CGLI_EINVAL, "scales must be positive");
     n->sc.mean[v] = (float)mean[v];
     n->sc.inv_std[v] = (float)(1.0 / stdv[v]);
+    n->sc.inv_d1[v] = (float)(1.0 / d1[v]);
+    n->sc.inv_d2[v] = (float)(1.0 / d2[v]);
     n->sc.oscale[v] = (float)oscale[v];
     n->sc.inv_oscale[v] = (float)(1.0 / oscale[v]);
   }

@@ -111,7 +111,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.cgli_cnn_last_error.restype = ctypes.c_char_p
     L.cgli_cnn_set_params.argtypes = [P, P]
     L.cgli_cnn_get_params.argtypes = [P, P]
-    L.cgli_cnn_set_scales.argtypes = [P, P, P, P]
+    L.cgli_cnn_set_scales.argtypes = [P, P, P, P, P, P]
     L.cgli_cnn_forward_host.argtypes = [P, P, P]
     L.cgli_cnn_loss_grad_host.argtypes = [P, P, P, FP, P]
     L.cgli_cnn_reserve_levels.argtypes = [P, ctypes.c_int]

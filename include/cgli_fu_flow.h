@@ -239,8 +239,9 @@ int cgli_sweep_tile_shape(int precision, int *ti, int *tj);
  * convolutional network, 15 -> 32 -> 32 -> 32 -> 32 -> 5 channels, 3x3x3
  * kernels, GELU after the first four layers, periodic in x and z, zero
  * padded at the walls, BF16 weights and activations with FP32 accumulation
- * on the tensor cores.  Input: Q = U*J of Q^n, Q^(n-1), Q^(n-2), channel
- * level*5 + v, normalised (Q_v - mean_v) / std_v; output: the correction
+ * on the tensor cores.  Input, from Q = U*J of Q^n, Q^(n-1), Q^(n-2):
+ * channel v (Q^n_v - mean_v) / std_v, channel 5 + v (Q^n - Q^(n-1))_v / d1_v,
+ * channel 10 + v (Q^n - 2Q^(n-1) + Q^(n-2))_v / d2_v; output: the correction
  * (Q^(n+1) - (3Q^n - 3Q^(n-1) + Q^(n-2)))_v / oscale_v.
  * Parameters: a flat float array, per layer W[27][cout][cin] (tap
  * t = (dx*3 + dy)*3 + dz for offsets dx-1, dy-1, dz-1) then b[cout].
@@ -252,7 +253,10 @@ int cgli_cnn_destroy(cgli_cnn *cnn);
 const char *cgli_cnn_last_error(void);
 int cgli_cnn_set_params(cgli_cnn *cnn, const float *theta);   /* also resets Adam */
 int cgli_cnn_get_params(cgli_cnn *cnn, float *theta);
-int cgli_cnn_set_scales(cgli_cnn *cnn, const double mean[5], const double std[5], const double oscale[5]);
+/* mean, std: of the level; d1, d2: RMS of its first and second time
+ * differences; oscale: of the correction (all positive) */
+int cgli_cnn_set_scales(cgli_cnn *cnn, const double mean[5], const double std[5], const double d1[5],
+                        const double d2[5], const double oscale[5]);
 /* x0: [15][Nx][Ny][Nz] already normalised; out: [5][Nx][Ny][Nz] */
 int cgli_cnn_forward_host(cgli_cnn *cnn, const float *x0, float *out);
 /* mean squared error against target [5][Nx][Ny][Nz] and its gradient with

@@ -201,7 +201,7 @@ def test_training_on_solver_levels_and_ab_against_extrapolation():
         held_cnn.append(net.pair_loss(p))
         q = [np.asarray(x) for x in host_levels[-3:]] + [physical_levels(A)]
         host_levels.append(q[-1])
-        mean, std, osc = scales_from_levels(host_levels[:train_steps])
+        osc = scales_from_levels(host_levels[:train_steps])[-1]
         r = (q[3] - (3 * q[2] - 3 * q[1] + q[0])) / osc[:, None, None, None]
         held_ext.append(float(np.mean(r * r)))
     print("held-out guess MSE (normalised): learned", np.mean(held_cnn), "extrapolation", np.mean(held_ext))
