@@ -60,13 +60,25 @@ RESIDUAL_BYTES_PER_CELL = 60 * 8
 RESIDUAL_STAGES = ("halo_bc", "flux_x", "flux_y", "flux_z", "viscous", "residual")
 
 
+# FP64 instructions per cell (thread level) of the residual side's kernels,
+# from ncu (sm__inst_executed_pipe_fp64.sum x 32 / cells) on the
+# 160x128x128 channel: flux 430 per face and direction, viscous faces 980,
+# residual assembly 315.  With the FP64 pipe's measured rate on this GPU
+# (a standalone FMA probe: 34 TFLOP/s = 17 T FP64 instructions/s) this is a
+# lower bound on the side's time that lies above its HBM bound.
+RESIDUAL_FP64_OPS_PER_CELL = 3 * 430 + 980 + 315
+FP64_INST_PER_S = 17.0e12
+
+
 def residual_roofline(ch, stage_ms: dict) -> dict:
     """stage_ms: device milliseconds per stage of one inner iteration."""
     dur_ms = sum(stage_ms[k] for k in RESIDUAL_STAGES)
     achieved = RESIDUAL_BYTES_PER_CELL * ch.cells / (dur_ms / 1e3) / 1e9
+    fp64_ms = RESIDUAL_FP64_OPS_PER_CELL * ch.cells / FP64_INST_PER_S * 1e3
     peak, kind = hbm_peak()
     return {"kernels": "halo/boundaries, k_flux_x/y/z, k_vprim + k_viscous_faces + k_viscous_div, k_residual_fast",
             "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "peak_kind": kind, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "algorithmic_bytes_per_iteration": RESIDUAL_BYTES_PER_CELL * ch.cells,
-            "ms_per_iteration": round(dur_ms, 4)}
+            "ms_per_iteration": round(dur_ms, 4),
+            "fp64_floor_ms": round(fp64_ms, 4), "fp64_frac": round(fp64_ms / dur_ms, 4)}
 
