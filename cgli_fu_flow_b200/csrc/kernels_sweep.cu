@@ -65,6 +65,10 @@
 #include "cgli_launch.h"
 #include "tc_sm100.cuh"
 
+// steps ahead that a tile loads the products its neighbouring tiles hand over
+#ifndef CGLI_SWEEP_PREFETCH
+#define CGLI_SWEEP_PREFETCH 2
+#endif
 // tiles per SM the wavefront kernel is compiled for (a register cap)
 #ifndef CGLI_SWEEP_MINBLOCKS
 #define CGLI_SWEEP_MINBLOCKS 1
@@ -373,11 +377,12 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
   T *const *dq = SweepPtrs<T>::dq(a);
   T carry_z[5] = {0, 0, 0, 0, 0};
 
-  // hand-over values of the next two steps, loaded ahead: a neighbouring
+  // hand-over values of the next PD steps, loaded ahead: a neighbouring
   // tile runs just far enough ahead for its value to exist when needed, so
-  // a load issued then would wait one L2 round trip per step; loaded two
+  // a load issued then would wait one L2 round trip per step; loaded PD
   // steps early it is usually there (a sentinel falls back to the bounded
   // poll)
+  constexpr int PD = CGLI_SWEEP_PREFETCH;
   auto kl_of = [&](int step) {
     const int r = BACKWARD ? step - (TI - 1 - il) - (TJ - 1 - jl) : step - il - jl;
     return (inside && r >= 0 && r < Nz) ? (BACKWARD ? Nz - 1 - r : r) : -1;
@@ -385,21 +390,21 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
   const T *xsrc = xb + ((long long)tile_pa * TJ + jl) * Nz * 5;
   const T *ysrc = yb + ((long long)tile_pb * TI + il) * Nz * 5;
   const bool pre_x = recv_x && !dsm_recv, pre_y = recv_y && !wall_y;
-  T px0[5], px1[5], py0[5], py1[5];
-  auto preload = [&](int step, T *px, T *py) {
+  T px[PD][5], py[PD][5];
+  auto preload = [&](int step, T *qx, T *qy) {
     const int k2 = kl_of(step);
 #pragma unroll
-    for (int v = 0; v < 5; v++) { px[v] = (T)0; py[v] = (T)0; }
+    for (int v = 0; v < 5; v++) { qx[v] = (T)0; qy[v] = (T)0; }
     if (k2 < 0) return;
     if (pre_x)
 #pragma unroll
-      for (int v = 0; v < 5; v++) px[v] = ld_gpu(xsrc + (long long)k2 * 5 + v);
+      for (int v = 0; v < 5; v++) qx[v] = ld_gpu(xsrc + (long long)k2 * 5 + v);
     if (pre_y)
 #pragma unroll
-      for (int v = 0; v < 5; v++) py[v] = ld_gpu(ysrc + (long long)k2 * 5 + v);
+      for (int v = 0; v < 5; v++) qy[v] = ld_gpu(ysrc + (long long)k2 * 5 + v);
   };
-  preload(0, px0, py0);
-  preload(1, px1, py1);
+#pragma unroll
+  for (int p = 0; p < PD; p++) preload(p, px[p], py[p]);
 
   // the periodic lagged halo of the slab's x edge: the x neighbour's product,
   // formed before the pass (k_halo_products), loaded a step ahead by the
@@ -471,7 +476,7 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
       } else {
         bool ok = true;
 #pragma unroll
-        for (int v = 0; v < 5; v++) { tx[v] = px0[v]; ok = ok && !is_sentinel(px0[v]); }
+        for (int v = 0; v < 5; v++) { tx[v] = px[0][v]; ok = ok && !is_sentinel(px[0][v]); }
         if (!ok) recv5<T>(xsrc + (long long)kl * 5, tx, d.status, a.spin_limit, &s_dead);
       }
       if (!recv_y) {
@@ -481,7 +486,7 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
       } else if (!wall_y) {
         bool ok = true;
 #pragma unroll
-        for (int v = 0; v < 5; v++) { ty[v] = py0[v]; ok = ok && !is_sentinel(py0[v]); }
+        for (int v = 0; v < 5; v++) { ty[v] = py[0][v]; ok = ok && !is_sentinel(py[0][v]); }
         if (!ok) recv5<T>(ysrc + (long long)kl * 5, ty, d.status, a.spin_limit, &s_dead);
       } else {
 #pragma unroll
@@ -591,8 +596,10 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
     }
     if (pre_x || pre_y) {
 #pragma unroll
-      for (int v = 0; v < 5; v++) { px0[v] = px1[v]; py0[v] = py1[v]; }
-      if (s + 2 < S) preload(s + 2, px1, py1);
+      for (int p = 0; p + 1 < PD; p++)
+#pragma unroll
+        for (int v = 0; v < 5; v++) { px[p][v] = px[p + 1][v]; py[p][v] = py[p + 1][v]; }
+      if (s + PD < S) preload(s + PD, px[PD - 1], py[PD - 1]);
     }
     if (halo_edge)
 #pragma unroll
