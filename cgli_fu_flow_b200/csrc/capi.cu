@@ -283,6 +283,7 @@ int cgli_create(const cgli_params *p, cgli_ctx **out) {
   d.dj = d.Z; d.di = (long long)d.Y * d.Z;
   d.dxi = p->dxi; d.det = p->det; d.dzt = p->dzt; d.dt = p->dt; d.e = p->e;
   d.mu = p->mu; d.pr = p->pr; d.twl = p->twall_lo; d.twh = p->twall_hi;
+  d.rdxi = 1.0 / p->dxi; d.rdet = 1.0 / p->det; d.rdzt = 1.0 / p->dzt; d.rpr = 1.0 / p->pr;
   d.curved_walls = p->curved_walls ? 1 : 0;
   d.x_open = p->x_open ? 1 : 0;
   d.nx_inlet = p->nx_inlet;
@@ -310,7 +311,7 @@ int cgli_create(const cgli_params *p, cgli_ctx **out) {
   if (rc == CGLI_OK) rc = alloc(c, 16 * sizeof(double), (void **)&d.scal);
   if (rc == CGLI_OK) rc = alloc(c, (8 + 296) * sizeof(double), (void **)&c->d_out);
   if (rc == CGLI_OK) rc = alloc(c, 16 * sizeof(int), (void **)&d.status);
-  if (rc == CGLI_OK) rc = alloc(c, 3 * 2 * sizeof(double) * d.Y, (void **)&d.ftab);
+  if (rc == CGLI_OK) rc = alloc(c, 3 * 4 * sizeof(double) * d.Y, (void **)&d.ftab);
   c->update_blocks = p->nx * p->ny;
   // the wavefront's tile grid for this context's precision
   const bool mixed_passes = p->precision == CGLI_MIXED;

@@ -22,6 +22,7 @@ struct Dev {
   int X, Y, Z;            // X_np, Y_m, Z_m
   long long di, dj;       // strides of i and j (k stride is 1)
   double dxi, det, dzt, dt, e, mu, pr, twl, twh;
+  double rdxi, rdet, rdzt, rpr;   // 1/dxi, 1/det, 1/dzt, 1/pr (formed on the host)
   int curved_walls;       // wall-face pressure force with eta_x, eta_z terms
   int x_open;             // open x ends (single rank 0 of 1), else a periodic slab
   int nx_inlet, nx_outlet;  // sponge layers (open x only)
@@ -32,9 +33,10 @@ struct Dev {
   double *J, *m[9];
   double *iJ;             // 1/J per cell (0 where J = 0), formed when the metrics change
   double *Jf[3], *mf[3][9];
-  // per-row face metrics [3 sets][Y][etdy, J], used when face_tables is set:
-  // every face of each set has the channel's form xi = (1,0,0),
-  // eta = (0,etdy(row),0), zeta = (0,0,1) with J a function of the row
+  // per-row face metrics [3 sets][Y][etdy, J, 1/J, 1/|etdy|], used when
+  // face_tables is set: every face of each set has the channel's form
+  // xi = (1,0,0), eta = (0,etdy(row),0), zeta = (0,0,1) with J a function of
+  // the row
   double *ftab;
   int face_tables;
   double *inF[3][5], *vF[4];
@@ -52,18 +54,77 @@ __host__ __device__ __forceinline__ long long ix(const Dev &d, int i, int j, int
   return (long long)i * d.di + (long long)j * d.dj + k;
 }
 
-// the nine metric terms and J of face set `set` (0 x, 1 y, 2 z faces) at
-// face index f, whose row index is jj: from the per-row tables when the
+// ------------------------------------------ FP64 reciprocal and square root
+// The residual side is bound by FP64 arithmetic, and an IEEE-rounded FP64
+// division or square root is a long instruction sequence with a special-case
+// branch.  These two refine the hardware's approximate seeds (PTX
+// rcp.approx.ftz.f64 and rsqrt.approx.ftz.f64, each good to about 20 bits)
+// by Newton-Raphson iteration with fused multiply-adds:
+//   reciprocal of a:  e = 1 - a y,  y <- y + y e          (twice)
+//   square root of x: g = x y, h = y / 2 (g ~ sqrt x, h ~ 1 / (2 sqrt x)),
+//                     r = 1/2 - g h,  g <- g + g r,  h <- h + h r   (coupled
+//                     Newton step on g and h), then g <- g + h (x - g g)
+// (P. Markstein, "Computation of elementary functions on the IBM RISC
+// System/6000 processor", IBM J. Res. Dev. 34(1), 1990).  Each step roughly
+// squares the relative error, so both results are within one unit in the
+// last place of the rounded value for the positive normal operands the
+// solver forms (densities, pressures, sound speeds, metric norms, face
+// Jacobians); the tests check that bound against CUDA's IEEE results.  Only
+// finite positive operands are meant: a zero or non-finite operand returns
+// NaN (the reciprocal), and x <= 0 returns 0 for x == 0 or NaN.
+__device__ __forceinline__ double nr_rcp(double a) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(a));
+  double e = fma(-a, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-a, y, 1.0);
+  return fma(y, e, y);
+}
+__device__ __forceinline__ double nr_sqrt(double x) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  double g = x * y, h = 0.5 * y;
+  const double r = fma(-g, h, 0.5);
+  g = fma(g, r, g);
+  h = fma(h, r, h);
+  g = fma(fma(-g, g, x), h, g);
+  return x > 0.0 ? g : (x == 0.0 ? 0.0 : __longlong_as_double(0x7ff8000000000000LL));
+}
+
+// the nine metric terms, J and 1/J of face set `set` (0 x, 1 y, 2 z faces)
+// at face index f, whose row index is jj: from the per-row tables when the
 // face metrics have the channel's form, else from the 3-D face arrays
-__device__ __forceinline__ void face_metrics(const Dev &d, int set, long long f, int jj, double mm[9], double &Jf) {
+__device__ __forceinline__ void face_metrics(const Dev &d, int set, long long f, int jj, double mm[9], double &Jf,
+                                             double &iJf) {
   if (d.face_tables) {
-    const double *t = d.ftab + ((long long)set * d.Y + jj) * 2;
+    const double *t = d.ftab + ((long long)set * d.Y + jj) * 4;
     mm[0] = 1; mm[1] = 0; mm[2] = 0; mm[3] = 0; mm[4] = t[0]; mm[5] = 0; mm[6] = 0; mm[7] = 0; mm[8] = 1;
     Jf = t[1];
+    iJf = t[2];
   } else {
 #pragma unroll
     for (int v = 0; v < 9; v++) mm[v] = d.mf[set][v][f];
     Jf = d.Jf[set][f];
+    iJf = nr_rcp(Jf);
+  }
+}
+
+// |n| and 1/|n| of the face normal of direction `set` (the metric vector of
+// that direction): from the per-row table on the channel grid (1 for the x
+// and z faces, |etdy| for the y faces), else formed from the metric terms
+__device__ __forceinline__ void face_norm(const Dev &d, int set, int jj, double mx, double my, double mz, double &sq,
+                                          double &insqr) {
+  if (d.face_tables) {
+    if (set == 1) {
+      sq = fabs(my);
+      insqr = d.ftab[((long long)set * d.Y + jj) * 4 + 3];
+    } else {
+      sq = 1.0;
+      insqr = 1.0;
+    }
+  } else {
+    sq = nr_sqrt(mx * mx + my * my + mz * mz);
+    insqr = nr_rcp(sq);
   }
 }
 
@@ -103,7 +164,7 @@ __device__ __forceinline__ void muscl_side(const Dev &d, const long long (&o)[N]
   double s = c[0] * d.iJ[o[0]];
 #pragma unroll
   for (int p = 1; p < N; p++) s += c[p] * d.iJ[o[p]];
-  const double t = 1. / s;
+  const double t = nr_rcp(s);
 #pragma unroll
   for (int v = 0; v < 5; v++) {
     const double *u = d.U_[v];
@@ -144,36 +205,38 @@ __device__ __forceinline__ void side2(const Dev &d, long long a, long long b, do
 // Preconditioned Roe flux through one face, Flux_X.cpp:229-350 (same
 // statements in Flux_Y.cpp:291-396 and Flux_Z.cpp:250-354; the pressure-jump
 // term uses the face's own unit normal).  L, R: MUSCL states; (mx,my,mz)
-// face metric; Jf face Jacobian.  Also returns Fav3 and iP+P_ for the wall
-// faces of Flux_Y.cpp:400-408.
+// face metric, sq its norm and insqr = 1/sq; iJf the reciprocal of the face
+// Jacobian.  Also returns Fav3 and iP+P_ for the wall faces of
+// Flux_Y.cpp:400-408.
 __device__ __forceinline__ void roe_face(const double L[5], const double R[5], double mx, double my,
-                                         double mz, double Jf, double e, double F[5], double &Fav3o,
-                                         double &ppo) {
+                                         double mz, double sq, double insqr, double iJf, double e, double F[5],
+                                         double &Fav3o, double &ppo) {
   // The reference's statements in its order; each group of divisions by one
-  // denominator is one reciprocal and products, and the divisions by the
-  // constant gamma - 1 are products with its reciprocal (results differ from
-  // the reference's in the last bits only).
+  // denominator is one reciprocal and products, the divisions by the
+  // constant gamma - 1 are products with its reciprocal, the Roe-averaged
+  // density sqrt(rho_L rho_R) is the product of the two square roots the
+  // averages use anyway, and the reciprocals and square roots are the
+  // Newton-refined ones (results differ from the reference's in the last
+  // bits only).
   constexpr double rkg = 1.0 / (KG - 1);
-  const double sq = sqrt(mx * mx + my * my + mz * mz);
-  const double insqr = 1.0 / sq;
   const double NX = mx * insqr, NY = my * insqr, NZ = mz * insqr;
-  const double _rho = L[0], irl = 1.0 / _rho;
+  const double _rho = L[0], irl = nr_rcp(_rho);
   const double _u = L[1] * irl, _v = L[2] * irl, _w = L[3] * irl;
   const double iU = mx * _u + my * _v + mz * _w;
   const double _VV = _u * _u + _v * _v + _w * _w;
   const double iP = (L[4] - 0.5 * _rho * _VV) * (KG - 1);
   const double iC = KG * iP * irl;
   const double _H = 0.5 * _VV + iC * rkg;
-  const double rho_ = R[0], irr = 1.0 / rho_;
+  const double rho_ = R[0], irr = nr_rcp(rho_);
   const double u_ = R[1] * irr, v_ = R[2] * irr, w_ = R[3] * irr;
   const double U_ = mx * u_ + my * v_ + mz * w_;
   const double VV_ = u_ * u_ + v_ * v_ + w_ * w_;
   const double P_ = (R[4] - 0.5 * rho_ * VV_) * (KG - 1);
   const double C_ = KG * P_ * irr;
   const double H_ = 0.5 * VV_ + C_ * rkg;
-  const double temp5 = sqrt(_rho), temp6 = sqrt(rho_);
-  const double i4 = 1.0 / (temp5 + temp6);
-  const double rho = sqrt(_rho * rho_);
+  const double temp5 = nr_sqrt(_rho), temp6 = nr_sqrt(rho_);
+  const double i4 = nr_rcp(temp5 + temp6);
+  const double rho = temp5 * temp6;
   const double u = (temp5 * _u + temp6 * u_) * i4;
   const double v = (temp5 * _v + temp6 * v_) * i4;
   const double w = (temp5 * _w + temp6 * w_) * i4;
@@ -181,7 +244,7 @@ __device__ __forceinline__ void roe_face(const double L[5], const double R[5], d
   const double VV = u * u + v * v + w * w;
   const double H = (temp5 * _H + temp6 * H_) * i4;
   const double C = (H - 0.5 * VV) * (KG - 1);
-  const double iCc = 1.0 / C;
+  const double iCc = nr_rcp(C);
   const double dU1 = rho_ - _rho;
   const double dU2 = rho_ * u_ - _rho * _u;
   const double dU3 = rho_ * v_ - _rho * _v;
@@ -191,12 +254,12 @@ __device__ __forceinline__ void roe_face(const double L[5], const double R[5], d
   const double beta = theda_p > e ? theda_p : e;   // max() macro semantics
   const double Un = U * insqr;
   const double temp = 0.5 * (1 + beta) * Un;
-  const double S = 0.5 * sqrt(4 * beta * C + Un * Un * (1 - beta) * (1 - beta));
-  const double iS = 1.0 / S;
+  const double S = 0.5 * nr_sqrt(4 * beta * C + Un * Un * (1 - beta) * (1 - beta));
+  const double iS = nr_rcp(S);
   const double U_p = 0.5 * (1 + theda_p) * Un;
-  const double C_p = 0.5 * sqrt(4 * C * theda_p + Un * Un * (1 - theda_p) * (1 - theda_p));
+  const double C_p = 0.5 * nr_sqrt(4 * C * theda_p + Un * Un * (1 - theda_p) * (1 - theda_p));
   const double dP = P_ - iP, dUn = (U_ - iU) * insqr;
-  const double temp1 = dP * iCc / (rho * beta);
+  const double temp1 = dP * iCc * nr_rcp(rho * beta);
   const double temp2 = U_p * iS * dUn;
   const double temp3 = 0.5 * (1 - beta) * Un * temp * iS;
   const double temp4 = 0.5 * (1 - theda_p) * Un * U_p * iS;
@@ -208,7 +271,7 @@ __device__ __forceinline__ void roe_face(const double L[5], const double R[5], d
   const double Fav3 = aU * dU3 + deltaU * rho * v + deltaP * NY;
   const double Fav4 = aU * dU4 + deltaU * rho * w + deltaP * NZ;
   const double Fav5 = aU * dU5 + deltaU * rho * H + deltaP * Un;
-  const double h = 0.5 / Jf;
+  const double h = 0.5 * iJf;
   F[0] = ((_rho * iU + rho_ * U_) - Fav1 * sq) * h;
   F[1] = ((_rho * _u * iU + rho_ * u_ * U_ + mx * (iP + P_)) - Fav2 * sq) * h;
   F[2] = ((_rho * _v * iU + rho_ * v_ * U_ + my * (iP + P_)) - Fav3 * sq) * h;
@@ -225,23 +288,31 @@ struct CPrim {
   T rho, u, v, w, VV, P, C, Tt, H, beta;
 };
 
+// reciprocal in the arithmetic type: the Newton-refined one in FP64
+template <typename T>
+__device__ __forceinline__ T recip(T a);
+template <>
+__device__ __forceinline__ double recip<double>(double a) { return nr_rcp(a); }
+template <>
+__device__ __forceinline__ float recip<float>(float a) { return 1.0f / a; }
+
 template <typename T>
 __device__ __forceinline__ CPrim<T> cprim(T q1, T q2, T q3, T q4, T q5, T J, T e) {
   CPrim<T> r;
   const T K = (T)KG;
   // divisions by one denominator as one reciprocal and products
-  const T iq1 = (T)1 / q1;
+  const T iq1 = recip<T>(q1);
   r.rho = q1 * J;
   r.u = q2 * iq1;
   r.v = q3 * iq1;
   r.w = q4 * iq1;
   r.VV = r.u * r.u + r.v * r.v + r.w * r.w;
   r.P = (q5 * J - (T)0.5 * r.rho * r.VV) * (K - 1);
-  const T irho = (T)1 / r.rho;
+  const T irho = recip<T>(r.rho);
   r.C = K * r.P * irho;
   r.Tt = r.P * irho;
-  r.H = (T)0.5 * r.VV + r.C / (K - 1);
-  const T th = r.VV / r.C;
+  r.H = (T)0.5 * r.VV + r.C * (T)(1.0 / (KG - 1));
+  const T th = r.VV * recip<T>(r.C);
   r.beta = th > e ? th : e;
   return r;
 }
@@ -486,28 +557,28 @@ __device__ __forceinline__ void make_record(double q1, double q2, double q3, dou
                                             const double mm[9], double e, double rdx, double rdy, double rdz,
                                             double dt, double r[REC_N]) {
   const double K = KG;
-  double rq1 = 1.0 / q1;
+  double rq1 = nr_rcp(q1);
   double rho = q1 * J;
   double u = q2 * rq1, v = q3 * rq1, w = q4 * rq1;
   double VV = u * u + v * v + w * w;
   double P = (q5 * J - 0.5 * rho * VV) * (K - 1);
-  double rrho = 1.0 / rho;
+  double rrho = nr_rcp(rho);
   double C = K * P * rrho;
   double Tt = P * rrho;
-  double th = VV / C;
+  double th = VV * nr_rcp(C);
   double beta = th > e ? th : e;
   double lam[3], U[3];
 #pragma unroll
   for (int dd = 0; dd < 3; dd++) {
     double mx = mm[3 * dd], my = mm[3 * dd + 1], mz = mm[3 * dd + 2];
     U[dd] = mx * u + my * v + mz * w;
-    double S = sqrt(U[dd] * U[dd] * (beta - 1) * (beta - 1) + 4 * beta * C * (mx * mx + my * my + mz * mz));
+    double S = nr_sqrt(U[dd] * U[dd] * (beta - 1) * (beta - 1) + 4 * beta * C * (mx * mx + my * my + mz * mz));
     lam[dd] = ((beta + 1) * fabs(U[dd]) + S) * 0.5;
   }
   double lambda = lam[0] * rdx + lam[1] * rdy + lam[2] * rdz;
   double ld = 2 * lambda * dt;
-  double a1 = 1.0 / (3 * beta + ld);
-  double a2 = 1.0 / (3 + ld);
+  double a1 = nr_rcp(3 * beta + ld);
+  double a2 = nr_rcp(3 + ld);
   r[R_BETA] = beta;
   r[R_H] = 0.5 * P * K * beta;
   r[R_HR] = 0.5 * rrho;

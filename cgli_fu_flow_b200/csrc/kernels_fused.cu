@@ -30,8 +30,12 @@ __device__ __forceinline__ void cell_metrics(const Dev &d, const SweepArgs &a, i
 // exchanges planes ie and 3 before its first pass, :942-976).  CH: the grid
 // is uniform in x and z (a.channel_metrics), J and etdy come from the per-row
 // tables instead of ten 3-D metric arrays.
+// (the mixed-precision channel instance is held at six CTAs per SM, the
+// occupancy of the other instances: uncapped it takes ten registers more and
+// drops to five)
 template <bool MIXED, bool CH>
-__global__ void __launch_bounds__(64, CGLI_RESIDUAL_MINBLOCKS) k_residual_fast(Dev d, SweepArgs a) {
+__global__ void __launch_bounds__(64, (MIXED && CH && CGLI_RESIDUAL_MINBLOCKS < 6) ? 6 : CGLI_RESIDUAL_MINBLOCKS)
+    k_residual_fast(Dev d, SweepArgs a) {
   int k = 2 + blockIdx.x * blockDim.x + threadIdx.x;
   int j = 2 + blockIdx.y;
   int i = 2 + blockIdx.z;
@@ -47,8 +51,8 @@ __global__ void __launch_bounds__(64, CGLI_RESIDUAL_MINBLOCKS) k_residual_fast(D
     // go to the per-(j,k) halo records
     double mm[9], r[REC_N];
     cell_metrics<CH>(d, a, j, c, mm);
-    make_record(d.U_[0][c], d.U_[1][c], d.U_[2][c], d.U_[3][c], d.U_[4][c], J, mm, d.e, 1.0 / d.dxi, 1.0 / d.det,
-                1.0 / d.dzt, deltaT, r);
+    make_record(d.U_[0][c], d.U_[1][c], d.U_[2][c], d.U_[3][c], d.U_[4][c], J, mm, d.e, d.rdxi, d.rdet, d.rdzt,
+                deltaT, r);
     const long long h = (long long)j * d.dj + k;
     if (halo_plane) {
       for (int v2 = 0; v2 < REC_N; v2++) {
@@ -79,8 +83,8 @@ __global__ void __launch_bounds__(64, CGLI_RESIDUAL_MINBLOCKS) k_residual_fast(D
   CPrim<double> q = cprim<double>(d.U_[0][c], d.U_[1][c], d.U_[2][c], d.U_[3][c], d.U_[4][c], J, d.e);
   double rho = q.rho, u = q.u, v = q.v, w = q.w, VV = q.VV, T = q.Tt, H = q.H, beta = q.beta;
   // Gamma^-1 of Dual_time_stepping.cpp:771-802; divisions by rho and by
-  // rho*gamma as reciprocals
-  const double irho = 1 / rho, itemp = 1 / (rho * KG);
+  // rho*gamma as one (Newton-refined) reciprocal and products
+  const double irho = nr_rcp(rho), itemp = irho * (1.0 / KG);
   double d11 = -(H * (KG - 1) + VV - KG * (T + VV)) * beta;
   double d12 = -(KG - 1) * u * beta, d13 = -(KG - 1) * v * beta, d14 = -(KG - 1) * w * beta;
   double d15 = (KG - 1) * beta;
@@ -97,7 +101,7 @@ __global__ void __launch_bounds__(64, CGLI_RESIDUAL_MINBLOCKS) k_residual_fast(D
   double Rk[5], sp[5];
   sponge_terms(d, i, c, sp);
   double f = d.buoyancy ? -(rho - 1.1842) * 9.81 : d.scal[0];
-  const double i2dt = 1 / (2 * deltaT), idx = 1 / d.dxi, idy = 1 / d.det, idz = 1 / d.dzt, iJ = 1 / J;
+  const double i2dt = nr_rcp(2 * deltaT), idx = d.rdxi, idy = d.rdet, idz = d.rdzt, iJ = nr_rcp(J);
   for (int n = 0; n < 5; n++) {
     double Rp = -(3 * d.U_[n][c] - 4 * d.U[n][c] + d.Uq[n][c]) * i2dt;
     double Rf = -((d.inF[0][n][fx1] - d.inF[0][n][fx0]) * idx + (d.inF[1][n][fy1] - d.inF[1][n][fx0]) * idy +

@@ -188,8 +188,11 @@ __global__ void k_fill_face_tables(Dev d) {
   if (j >= d.Y) return;
   for (int set = 0; set < 3; set++) {
     const long long r = ix(d, 2, j, 1);
-    d.ftab[((long long)set * d.Y + j) * 2] = d.mf[set][4][r];
-    d.ftab[((long long)set * d.Y + j) * 2 + 1] = d.Jf[set][r];
+    double *t = d.ftab + ((long long)set * d.Y + j) * 4;
+    t[0] = d.mf[set][4][r];
+    t[1] = d.Jf[set][r];
+    t[2] = 1.0 / t[1];
+    t[3] = 1.0 / fabs(t[0]);
   }
 }
 
@@ -235,9 +238,10 @@ __global__ void __launch_bounds__(64, CGLI_FLUX_MINBLOCKS) k_flux_x(Dev d) {
     side5L(d, c - 2 * di, di, L);
     side5R(d, c - di, di, R);
   }
-  double mm[9], Jf;
-  face_metrics(d, 0, f, j, mm, Jf);
-  roe_face(L, R, mm[0], mm[1], mm[2], Jf, d.e, F, fav3, pp);
+  double mm[9], Jf, iJf, sq, insqr;
+  face_metrics(d, 0, f, j, mm, Jf, iJf);
+  face_norm(d, 0, j, mm[0], mm[1], mm[2], sq, insqr);
+  roe_face(L, R, mm[0], mm[1], mm[2], sq, insqr, iJf, d.e, F, fav3, pp);
   for (int v = 0; v < 5; v++) d.inF[0][v][f] = F[v];
 }
 
@@ -269,17 +273,18 @@ __global__ void __launch_bounds__(64, CGLI_FLUX_MINBLOCKS) k_flux_y(Dev d) {
   long long f = ix(d, i, j, k);
   double L[5], R[5], F[5], fav3, pp;
   muscl_y(d, i + 1, j, k + 1, L, R);
-  double mm[9], Jf;
-  face_metrics(d, 1, f, j, mm, Jf);
+  double mm[9], Jf, iJf, sq, insqr;
+  face_metrics(d, 1, f, j, mm, Jf, iJf);
   const double ety = mm[4];
-  roe_face(L, R, mm[3], ety, mm[5], Jf, d.e, F, fav3, pp);
+  face_norm(d, 1, j, mm[3], ety, mm[5], sq, insqr);
+  roe_face(L, R, mm[3], ety, mm[5], sq, insqr, iJf, d.e, F, fav3, pp);
   if (j == 1 || j == jn) {
     F[0] = 0; F[1] = 0; F[3] = 0; F[4] = 0;
-    F[2] = 0.5 * (ety * pp - 1. * fav3) / Jf;
+    F[2] = 0.5 * (ety * pp - 1. * fav3) * iJf;
     if (d.curved_walls) {
       // a curved wall also carries the x and z pressure force
-      F[1] = 0.5 * (mm[3] * pp) / Jf;
-      F[3] = 0.5 * (mm[5] * pp) / Jf;
+      F[1] = 0.5 * (mm[3] * pp) * iJf;
+      F[3] = 0.5 * (mm[5] * pp) * iJf;
     }
   }
   for (int v = 0; v < 5; v++) d.inF[1][v][f] = F[v];
@@ -308,9 +313,10 @@ __global__ void __launch_bounds__(64, CGLI_FLUX_MINBLOCKS) k_flux_z(Dev d) {
   long long f = ix(d, i, j, k);
   double L[5], R[5], F[5], fav3, pp;
   muscl_z(d, i + 1, j + 1, k, L, R);
-  double mm[9], Jf;
-  face_metrics(d, 2, f, j, mm, Jf);
-  roe_face(L, R, mm[6], mm[7], mm[8], Jf, d.e, F, fav3, pp);
+  double mm[9], Jf, iJf, sq, insqr;
+  face_metrics(d, 2, f, j, mm, Jf, iJf);
+  face_norm(d, 2, j, mm[6], mm[7], mm[8], sq, insqr);
+  roe_face(L, R, mm[6], mm[7], mm[8], sq, insqr, iJf, d.e, F, fav3, pp);
   for (int v = 0; v < 5; v++) d.inF[2][v][f] = F[v];
 }
 
@@ -323,10 +329,11 @@ __global__ void k_vprim(Dev d) {
   int i = 2 + blockIdx.z;
   if (k > d.nz + 2) return;
   long long c = ix(d, i, j, k);
-  double rho = d.U_[0][c];
-  double U = d.U_[1][c] / rho, V = d.U_[2][c] / rho, W = d.U_[3][c] / rho;
+  // the divisions by rho, rho R and J as Newton-refined reciprocals
+  double rho = d.U_[0][c], irho = nr_rcp(rho);
+  double U = d.U_[1][c] * irho, V = d.U_[2][c] * irho, W = d.U_[3][c] * irho;
   double P = (d.U_[4][c] - 0.5 * rho * (U * U + V * V + W * W)) * (KG - 1) * d.J[c];
-  double T = P / (rho * RG) / d.J[c];
+  double T = P * (irho * (1.0 / RG)) * nr_rcp(d.J[c]);
   d.vprim[0][c] = U; d.vprim[1][c] = V; d.vprim[2][c] = W; d.vprim[3][c] = T;
 }
 
@@ -350,27 +357,27 @@ __global__ void __launch_bounds__(64, CGLI_VISCOUS_MINBLOCKS) k_viscous_faces(De
   VP o = vp(d, c);
   if (j <= jn && k <= kn) {
     double out[4];
-    double mm[9], Jf;
-    face_metrics(d, 0, f, j - 1, mm, Jf);
-    visc_face_x(d.dxi, d.det, d.dzt, d.mu, d.pr, o, vp(d, c - di), vp(d, c + dj), vp(d, c - di + dj), vp(d, c - dj), vp(d, c - di - dj),
-                vp(d, c + 1), vp(d, c - di + 1), vp(d, c - 1), vp(d, c - di - 1), mm, Jf, out);
+    double mm[9], Jf, iJf;
+    face_metrics(d, 0, f, j - 1, mm, Jf, iJf);
+    visc_face_x(d.rdxi, d.rdet, d.rdzt, d.mu, d.rpr, o, vp(d, c - di), vp(d, c + dj), vp(d, c - di + dj), vp(d, c - dj), vp(d, c - di - dj),
+                vp(d, c + 1), vp(d, c - di + 1), vp(d, c - 1), vp(d, c - di - 1), mm, iJf, out);
     for (int v = 0; v < 4; v++) d.vflux[0][v][c] = out[v];
   }
   if (i <= ie && k <= kn) {
     double out[4];
-    double mm[9], Jf;
-    face_metrics(d, 1, f, j - 1, mm, Jf);
-    visc_face_y(d.dxi, d.det, d.dzt, d.mu, d.pr, o, vp(d, c - dj), vp(d, c + di), vp(d, c + di - dj), vp(d, c - di), vp(d, c - di - dj),
-                vp(d, c + 1), vp(d, c - dj + 1), vp(d, c - 1), vp(d, c - dj - 1), mm, Jf, out);
+    double mm[9], Jf, iJf;
+    face_metrics(d, 1, f, j - 1, mm, Jf, iJf);
+    visc_face_y(d.rdxi, d.rdet, d.rdzt, d.mu, d.rpr, o, vp(d, c - dj), vp(d, c + di), vp(d, c + di - dj), vp(d, c - di), vp(d, c - di - dj),
+                vp(d, c + 1), vp(d, c - dj + 1), vp(d, c - 1), vp(d, c - dj - 1), mm, iJf, out);
     for (int v = 0; v < 4; v++) d.vflux[1][v][c] = out[v];
   }
   if (i <= ie && j <= jn) {
     double out[4];
-    double mm[9], Jf;
-    face_metrics(d, 2, f, j - 1, mm, Jf);
-    visc_face_z(d.dxi, d.det, d.dzt, d.mu, d.pr, o, vp(d, c - 1), vp(d, c + di), vp(d, c + di - 1), vp(d, c - di), vp(d, c - di - 1),
+    double mm[9], Jf, iJf;
+    face_metrics(d, 2, f, j - 1, mm, Jf, iJf);
+    visc_face_z(d.rdxi, d.rdet, d.rdzt, d.mu, d.rpr, o, vp(d, c - 1), vp(d, c + di), vp(d, c + di - 1), vp(d, c - di), vp(d, c - di - 1),
                 vp(d, c + dj), vp(d, c + dj - 1), vp(d, c - dj), vp(d, c - dj - 1), vp(d, c - di + dj),
-                mm, Jf, out);
+                mm, iJf, out);
     for (int v = 0; v < 4; v++) d.vflux[2][v][c] = out[v];
   }
 }
@@ -382,7 +389,7 @@ __global__ void k_viscous_div(Dev d) {
   int i = 3 + blockIdx.z;
   if (k > d.nz + 1) return;
   long long c = ix(d, i, j, k);
-  const double invXI = 1. / (d.dxi), invET = 1. / (d.det), invZT = 1. / (d.dzt);
+  const double invXI = d.rdxi, invET = d.rdet, invZT = d.rdzt;
   for (int v = 0; v < 4; v++)
     d.vF[v][c] = (d.vflux[0][v][c + d.di] - d.vflux[0][v][c]) * invXI +
                  (d.vflux[1][v][c + d.dj] - d.vflux[1][v][c]) * invET +

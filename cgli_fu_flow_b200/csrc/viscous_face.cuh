@@ -73,21 +73,21 @@ __device__ __forceinline__ MetricProducts metric_products(const double x[9]) {
 }
 
 // Sutherland's law as Viscous_terms.cpp:527 writes it, with (T/Tref)^1.5
-// evaluated as x*sqrt(x) (the same value to rounding, without pow)
+// evaluated as x*sqrt(x) (the same value to rounding, without pow) and the
+// Newton-refined square root and reciprocal
 __device__ __forceinline__ double sutherland_mu(double mu, double T) {
   const double x = T * (1.0 / 298.0592);
-  return mu * (x * sqrt(x)) * (298.0592 + 110.) / (T + 110.);
+  return mu * (x * nr_sqrt(x)) * (298.0592 + 110.) * nr_rcp(T + 110.);
 }
 
 // x face i-1/2, Viscous_terms.cpp:399-546
 template <typename P>
-__device__ __forceinline__ void visc_face_x(double dxi, double det, double dzt, double mu, double pr,
+__device__ __forceinline__ void visc_face_x(double rdxi, double rdet, double rdzt, double mu, double ipr,
                                             const P &o, const P &im, const P &jp, const P &iJ, const P &jm,
                                             const P &ijm, const P &kp, const P &iK, const P &km, const P &ikm,
-                                            const double mm[9], double Jf, double out[4]) {
-  const double invXI = 1. / (dxi), inv4ET = 1. / (4 * det), inv4ZT = 1. / (4 * dzt);
+                                            const double mm[9], double iJf, double out[4]) {
+  const double invXI = rdxi, inv4ET = 0.25 * rdet, inv4ZT = 0.25 * rdzt;
   const double CvK = CV * KG;
-  const double iJf = 1.0 / Jf, ipr = 1.0 / pr;
   double U = o.U, V = o.V, W = o.W, T = o.T;
   double du_dx = (U - im.U) * invXI, dv_dx = (V - im.V) * invXI, dw_dx = (W - im.W) * invXI;
   double du2_dx = (U * U - im.U * im.U) * invXI, dv2_dx = (V * V - im.V * im.V) * invXI,
@@ -127,13 +127,12 @@ __device__ __forceinline__ void visc_face_x(double dxi, double det, double dzt, 
 
 // y face j-1/2, Viscous_terms.cpp:549-700
 template <typename P>
-__device__ __forceinline__ void visc_face_y(double dxi, double det, double dzt, double mu, double pr,
+__device__ __forceinline__ void visc_face_y(double rdxi, double rdet, double rdzt, double mu, double ipr,
                                             const P &o, const P &jm, const P &ip, const P &jI, const P &im,
                                             const P &ijm, const P &kp, const P &jK, const P &km, const P &jkm,
-                                            const double mm[9], double Jf, double out[4]) {
-  const double inv4XI = 1. / (4 * dxi), invET = 1. / (det), inv4ZT = 1. / (4 * dzt);
+                                            const double mm[9], double iJf, double out[4]) {
+  const double inv4XI = 0.25 * rdxi, invET = rdet, inv4ZT = 0.25 * rdzt;
   const double CvK = CV * KG;
-  const double iJf = 1.0 / Jf, ipr = 1.0 / pr;
   double U = o.U, V = o.V, W = o.W, T = o.T;
   double du_dx = (ip.U + jI.U - im.U - ijm.U) * inv4XI, dv_dx = (ip.V + jI.V - im.V - ijm.V) * inv4XI,
          dw_dx = (ip.W + jI.W - im.W - ijm.W) * inv4XI;
@@ -174,13 +173,12 @@ __device__ __forceinline__ void visc_face_y(double dxi, double det, double dzt, 
 // z face k-1/2, Viscous_terms.cpp:714-861, with the typo of :744-746 that
 // pairs u at (i,j+1,k-1) with v, w at (i-1,j+1,k) (argument iJ)
 template <typename P>
-__device__ __forceinline__ void visc_face_z(double dxi, double det, double dzt, double mu, double pr,
+__device__ __forceinline__ void visc_face_z(double rdxi, double rdet, double rdzt, double mu, double ipr,
                                             const P &o, const P &km, const P &ip, const P &kI, const P &im,
                                             const P &ikm, const P &jp, const P &kJ, const P &jm, const P &jkm,
-                                            const P &iJ, const double mm[9], double Jf, double out[4]) {
-  const double inv4XI = 1. / (4 * dxi), inv4ET = 1. / (4 * det), invZT = 1. / (dzt);
+                                            const P &iJ, const double mm[9], double iJf, double out[4]) {
+  const double inv4XI = 0.25 * rdxi, inv4ET = 0.25 * rdet, invZT = rdzt;
   const double CvK = CV * KG;
-  const double iJf = 1.0 / Jf, ipr = 1.0 / pr;
   double U = o.U, V = o.V, W = o.W, T = o.T;
   double du_dx = (ip.U + kI.U - im.U - ikm.U) * inv4XI, dv_dx = (ip.V + kI.V - im.V - ikm.V) * inv4XI,
          dw_dx = (ip.W + kI.W - im.W - ikm.W) * inv4XI;
