@@ -73,9 +73,10 @@ constexpr int W_BYTES = 27 * 32 * ROW;                 // 55296: all taps of one
 constexpr int WG_COPY = 7 * 32 * ROW;                  // 14336: 7 y rows (the 4th dy shift)
 constexpr int WG_PLANE = 3 * WG_COPY;
 constexpr int G_TILE = 4 * 32 * ROW;                   // 8192: dZ of one output tile
-constexpr int CONV_SMEM = 1024 + 4 * FWD_PLANE + W_BYTES + 256;
+constexpr int CONV_SLOTS = 8;                          // TMEM accumulators of k_conv (32 columns each)
+constexpr int CONV_SMEM = 1024 + 4 * FWD_PLANE + W_BYTES + 512;
 constexpr int WGRAD_SMEM = 1024 + 4 * WG_PLANE + 2 * G_TILE + 256;
-constexpr uint32_t IDESC_FWD = tc::idesc_bf16(128, 32, false, false);
+
 constexpr uint32_t IDESC_WG = tc::idesc_bf16(128, 32, true, true);
 constexpr int SPIN = 1 << 22;
 
@@ -149,10 +150,12 @@ __global__ void __launch_bounds__(192, 1)
   const uint32_t A0 = base;
   const uint32_t W0 = base + 4 * FWD_PLANE;
   uint64_t *bars = reinterpret_cast<uint64_t *>(sb + 4 * FWD_PLANE + W_BYTES);
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 16);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 32);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
   auto bar = [&](int i) { return tc::smem_addr(bars + i); };
-  enum { FULL = 0, FREE = 4, ACCF = 8, ACCE = 10, WBAR = 12 };
+  constexpr int RS = CONV_SLOTS;
+  enum { FULL = 0, FREE = 4, ACCF = 8, ACCE = 8 + RS, WBAR = 8 + 2 * RS, NBAR = 9 + 2 * RS };
+  static_assert(NBAR <= 32, "barrier area");
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nyb = a.ny >> 2;
@@ -161,18 +164,25 @@ __global__ void __launch_bounds__(192, 1)
   const int n = min(a.xchunk, a.nx - xa);
 
   if (threadIdx.x == 0) {
-    for (int i = 0; i < 13; i++) tc::mbar_init(bar(i), (i == ACCE || i == ACCE + 1) ? 128 : 1);
+    for (int i = 0; i < NBAR; i++) tc::mbar_init(bar(i), (i >= ACCE && i < ACCE + RS) ? 128 : 1);
     *abort_flag = 0;
     tc::mbar_fence_init();
   }
   if (warp == 1) {
-    tc::tmem_alloc(tc::smem_addr(tmem_slot), 64);
+    tc::tmem_alloc(tc::smem_addr(tmem_slot), 32 * RS);
     tc::tmem_relinquish();
   }
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t tmem = *tmem_slot;
+  // every accumulator starts at zero (the MMAs only accumulate; the epilogue
+  // zeroes a slot again once it has read it)
+  if (warp >= 2)
+    for (int sl = 0; sl < RS; sl++) tc::tmem_zero_32x32(tmem + ((uint32_t)((warp & 3) * 32) << 16) + 32 * sl);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
   bool ok = true;
 
   if (warp == 0) {
@@ -198,33 +208,53 @@ __global__ void __launch_bounds__(192, 1)
     }
   } else if (warp == 1) {
     if (lane == 0) {
+      // Plane p (x = xa + p - 1) is the A operand of the taps dx = 0, 1, 2 of
+      // output tiles p, p - 1, p - 2.  For each (dy, dz, K half) one MMA
+      // multiplies it by the three dx blocks of weights side by side (N = 96)
+      // into the three tiles' accumulators, which sit in adjacent TMEM slots
+      // (tile q in slot q % RS at column 32 (RS - 1 - q % RS), so tile q - 1
+      // is 32 columns to the right of tile q); where the slots wrap, or only
+      // one or two of the tiles exist (the first and last planes), the block
+      // is split or narrowed.  A plane is read from shared memory once, by
+      // 18 MMAs, and its ring slot is free as soon as they complete.
       int last = -1;
+      const uint64_t adesc = tc::desc_sw64(A0, 16, 512), wdesc = tc::desc_sw64(W0, 16, 512);
       if (!one_wait(bar(WBAR), 0, a.spin, abort_flag)) ok = false;
-      for (int t = 0; t < n && ok; t++) {
-        const int b = t & 1;
-        if (t >= 2 && !one_wait(bar(ACCE + b), ((t >> 1) - 1) & 1, a.spin, abort_flag)) { ok = false; break; }
-        for (int q = 0; q < 3 && ok; q++)
-          if (!one_wait(bar(FULL + ((t + q) & 3)), ((t + q) >> 2) & 1, a.spin, abort_flag)) ok = false;
-        if (!ok) break;
-        tc::fence_after_sync();
-        const uint32_t d = tmem + b * 32;
-#pragma unroll 1
-        for (int tap = 0; tap < 27; tap++) {
-          const int dx = tap / 9, dy = (tap / 3) % 3, dz = tap % 3;
-          const uint32_t ab = A0 + ((t + dx) & 3) * FWD_PLANE + dz * FWD_COPY + dy * 32 * ROW;
-          const uint32_t wb = W0 + tap * 32 * ROW;
-#pragma unroll
-          for (int kk = 0; kk < 2; kk++)
-            tc::mma_f16(d, tc::desc_sw64(ab + kk * 32, 16, 512), tc::desc_sw64(wb + kk * 32, 16, 512), IDESC_FWD,
-                        (tap | kk) != 0);
+      for (int p = 0; p < n + 2 && ok; p++) {
+        const int lo = p > n - 1 ? p - (n - 1) : 0, hi = p < 2 ? p : 2;   // dx whose tile p - dx exists
+        // tile p (dx = 0) starts in slot p % RS, last used by tile p - RS
+        if (lo == 0 && p >= RS && !one_wait(bar(ACCE + p % RS), ((p / RS) - 1) & 1, a.spin, abort_flag)) {
+          ok = false;
+          break;
         }
-        tc::mma_commit(bar(ACCF + b));
-        tc::mma_commit(bar(FREE + (t & 3)));
-        last = t;
+        if (!one_wait(bar(FULL + (p & 3)), (p >> 2) & 1, a.spin, abort_flag)) { ok = false; break; }
+        tc::fence_after_sync();
+        const uint64_t ap = adesc + (uint64_t)((p & 3) * (FWD_PLANE >> 4));
+        for (int d0 = lo; d0 <= hi;) {
+          int d1 = d0;   // the segment d0..d1 of adjacent slots
+          while (d1 < hi && (p - d1) % RS != 0) d1++;
+          const uint32_t dcol = tmem + 32 * (RS - 1 - (p - d0) % RS);
+          const uint32_t idesc = d1 == d0 ? tc::idesc_bf16(128, 32, false, false)
+                                 : d1 == d0 + 1 ? tc::idesc_bf16(128, 64, false, false)
+                                                : tc::idesc_bf16(128, 96, false, false);
+          const uint64_t wp = wdesc + (uint64_t)((d0 * 32 * ROW) >> 4);
+#pragma unroll
+          for (int g = 0; g < 9; g++) {
+            const int dy = g / 3, dz = g % 3;
+            const uint64_t a_d = ap + (uint64_t)((dz * FWD_COPY + dy * 32 * ROW) >> 4);
+            const uint64_t w_d = wp + (uint64_t)((g * 96 * ROW) >> 4);
+#pragma unroll
+            for (int kk = 0; kk < 2; kk++) tc::mma_f16(dcol, a_d + 2 * kk, w_d + 2 * kk, idesc, 1u);
+          }
+          d0 = d1 + 1;
+        }
+        tc::mma_commit(bar(FREE + (p & 3)));
+        if (hi == 2) tc::mma_commit(bar(ACCF + (p - 2) % RS));   // tile p - 2 is complete
+        last = p;
       }
       if (!ok) *abort_flag = 1;
       // the MMAs issued complete before TMEM is released
-      if (last >= 0) tc::mbar_wait(bar(ACCF + (last & 1)), (last >> 1) & 1, a.spin);
+      if (last >= 0) tc::mbar_wait(bar(FREE + (last & 3)), (last >> 2) & 1, a.spin);
     }
   } else {
     // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31
@@ -236,13 +266,15 @@ __global__ void __launch_bounds__(192, 1)
       for (int c = 0; c < 32; c++) bias[c] = __ldg(a.bias + c);
     }
     for (int t = 0; t < n; t++) {
-      const int b = t & 1;
-      if (!warp_wait(bar(ACCF + b), (t >> 1) & 1, a.spin, abort_flag)) { ok = false; break; }
+      const int sl = t % RS;
+      if (!warp_wait(bar(ACCF + sl), (t / RS) & 1, a.spin, abort_flag)) { ok = false; break; }
       tc::fence_after_sync();
       float acc[32];
-      tc::tmem_ld_32x32(tmem + ((uint32_t)(ew * 32) << 16) + b * 32, acc);
+      const uint32_t ta = tmem + ((uint32_t)(ew * 32) << 16) + 32 * (RS - 1 - sl);
+      tc::tmem_ld_32x32(ta, acc);
+      tc::tmem_zero_32x32(ta);
       tc::fence_before_sync();
-      tc::mbar_arrive(bar(ACCE + b));
+      tc::mbar_arrive(bar(ACCE + sl));
       const int x = xa + t;
       const size_t pidx = ((size_t)(x + 1) * a.Yp + (y + 1)) * a.Zp + (z + 1);
       if (MODE == CONV_OUT) {
@@ -290,7 +322,7 @@ __global__ void __launch_bounds__(192, 1)
   __syncthreads();
   if (warp == 1) {
     tc::fence_after_sync();
-    tc::tmem_dealloc(tmem, 64);
+    tc::tmem_dealloc(tmem, 32 * RS);
   }
 }
 
@@ -361,21 +393,27 @@ __global__ void __launch_bounds__(192, 1)
   } else if (warp == 1) {
     if (lane == 0) {
       bool issued = false;
+      const uint64_t xdesc = tc::desc_sw64(X0, 32 * ROW, 512), gdesc = tc::desc_sw64(G0, 512, 512);
       for (int t = 0; t < n && ok; t++) {
         for (int q = 0; q < 3 && ok; q++)
           if (!one_wait(bar(FULL + ((t + q) & 3)), ((t + q) >> 2) & 1, a.spin, abort_flag)) ok = false;
         if (ok && !one_wait(bar(GFULL + (t & 1)), (t >> 1) & 1, a.spin, abort_flag)) ok = false;
         if (!ok) break;
         tc::fence_after_sync();
-#pragma unroll 1
+        // 72 MMAs fully unrolled on base descriptors plus compile-time offsets
+        // (as in k_conv)
+        const uint64_t xp[3] = {xdesc + (uint64_t)(((t + 0) & 3) * (WG_PLANE >> 4)),
+                                xdesc + (uint64_t)(((t + 1) & 3) * (WG_PLANE >> 4)),
+                                xdesc + (uint64_t)(((t + 2) & 3) * (WG_PLANE >> 4))};
+        const uint64_t g_d = gdesc + (uint64_t)((t & 1) * (G_TILE >> 4));
+#pragma unroll
         for (int g = 0; g < 9; g++) {
           const int dx = g / 3, dz = g % 3;
-          const uint32_t xb = X0 + ((t + dx) & 3) * WG_PLANE + dz * WG_COPY;
-          const uint32_t gb = G0 + (t & 1) * G_TILE;
+          const uint64_t x_d = xp[dx] + (uint64_t)((dz * WG_COPY) >> 4);
 #pragma unroll
           for (int kk = 0; kk < 8; kk++)
-            tc::mma_f16(tmem + g * 32, tc::desc_sw64(xb + kk * 1024, 32 * ROW, 512), tc::desc_sw64(gb + kk * 1024, 512, 512),
-                        IDESC_WG, (t > 0 || kk > 0) ? 1u : 0u);
+            tc::mma_f16(tmem + g * 32, x_d + (uint64_t)(kk * (1024 >> 4)), g_d + (uint64_t)(kk * (1024 >> 4)), IDESC_WG,
+                        (t > 0 || kk > 0) ? 1u : 0u);
         }
         tc::mma_commit(bar(FREE + (t & 3)));
         tc::mma_commit(bar(GFREE + (t & 1)));
@@ -661,13 +699,18 @@ __global__ void k_bias_total(const float *part, int nblk, float *db) {
 
 // BF16 copies of the float32 master weights: forward [27][cout][cin] and
 // input-gradient [27][cin][cout] with the taps reversed
+// BF16 weights of the forward (wf) and input-gradient (wt: transposed,
+// tap-reversed) convolutions, tap t = 9 dx + 3 dy + dz stored as block
+// 3 (3 dy + dz) + dx: the three dx taps of one (dy, dz) are 96 consecutive
+// rows (output channel, 32 input channels), the N = 96 B operand of k_conv
+__device__ __forceinline__ int wblock(int t) { return ((t / 3) % 3 * 3 + t % 3) * 3 + t / 9; }
 __global__ void k_prep_weights(const float *W, bf16 *wf, bf16 *wt) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= 27 * 1024) return;
   const int t = e / 1024, co = (e / 32) % 32, ci = e % 32;
   const bf16 h = __float2bfloat16_rn(W[e]);
-  wf[e] = h;
-  wt[(26 - t) * 1024 + ci * 32 + co] = h;
+  wf[wblock(t) * 1024 + co * 32 + ci] = h;
+  wt[wblock(26 - t) * 1024 + ci * 32 + co] = h;
 }
 
 // Adam (Kingma & Ba 2015), bias-corrected, float32

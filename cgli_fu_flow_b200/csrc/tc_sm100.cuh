@@ -211,6 +211,19 @@ __device__ __forceinline__ void tmem_ld_32x32(uint32_t taddr, float v[32]) {
   for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
 }
 
+// zeros into 32 lanes x 32 consecutive 32-bit columns (lane taddr.lane + t
+// from thread t), waited for before returning
+__device__ __forceinline__ void tmem_zero_32x32(uint32_t taddr) {
+  const uint32_t z = 0;
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
+      "{%1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, "
+      "%1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1};" ::"r"(taddr),
+      "r"(z)
+      : "memory");
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+
 // Shared-memory matrix descriptor (sm_100 layout): start address, leading
 // and stride byte offsets in 16-byte units, version 1, 64-byte swizzle.
 // K-major 64B-swizzled operand: rows of 64 bytes, 8-row groups 512 bytes
