@@ -344,7 +344,10 @@ __device__ __forceinline__ VP vp(const Dev &d, long long c) {
 
 // face viscous fluxes of cell (i,j,k): x face i-1/2 for j<=jn, k<=kn; y face
 // j-1/2 for i<=ie, k<=kn; z face k-1/2 for i<=ie, j<=jn (the faces the
-// divergence of Viscous_terms.cpp:875-904 reads)
+// divergence of Viscous_terms.cpp:875-904 reads).  CH: the face metrics have
+// the channel's form (d.face_tables), so the per-row tables give eta_y and
+// 1/J and the channel forms of the face fluxes apply.
+template <bool CH>
 __global__ void __launch_bounds__(64, CGLI_VISCOUS_MINBLOCKS) k_viscous_faces(Dev d) {
   int k = 2 + blockIdx.x * blockDim.x + threadIdx.x;
   int j = 2 + blockIdx.y;
@@ -357,27 +360,48 @@ __global__ void __launch_bounds__(64, CGLI_VISCOUS_MINBLOCKS) k_viscous_faces(De
   VP o = vp(d, c);
   if (j <= jn && k <= kn) {
     double out[4];
-    double mm[9], Jf, iJf;
-    face_metrics(d, 0, f, j - 1, mm, Jf, iJf);
-    visc_face_x(d.rdxi, d.rdet, d.rdzt, d.mu, d.rpr, o, vp(d, c - di), vp(d, c + dj), vp(d, c - di + dj), vp(d, c - dj), vp(d, c - di - dj),
-                vp(d, c + 1), vp(d, c - di + 1), vp(d, c - 1), vp(d, c - di - 1), mm, iJf, out);
+    if (CH) {
+      const double *t = d.ftab + (0LL * d.Y + (j - 1)) * 4;
+      visc_face_x_channel(d.rdxi, d.rdet, d.rdzt, d.mu, d.rpr, t[0], o, vp(d, c - di), vp(d, c + dj),
+                          vp(d, c - di + dj), vp(d, c - dj), vp(d, c - di - dj), vp(d, c + 1), vp(d, c - di + 1),
+                          vp(d, c - 1), vp(d, c - di - 1), t[2], out);
+    } else {
+      double mm[9], Jf, iJf;
+      face_metrics(d, 0, f, j - 1, mm, Jf, iJf);
+      visc_face_x(d.rdxi, d.rdet, d.rdzt, d.mu, d.rpr, o, vp(d, c - di), vp(d, c + dj), vp(d, c - di + dj), vp(d, c - dj),
+                  vp(d, c - di - dj), vp(d, c + 1), vp(d, c - di + 1), vp(d, c - 1), vp(d, c - di - 1), mm, iJf, out);
+    }
     for (int v = 0; v < 4; v++) d.vflux[0][v][c] = out[v];
   }
   if (i <= ie && k <= kn) {
     double out[4];
-    double mm[9], Jf, iJf;
-    face_metrics(d, 1, f, j - 1, mm, Jf, iJf);
-    visc_face_y(d.rdxi, d.rdet, d.rdzt, d.mu, d.rpr, o, vp(d, c - dj), vp(d, c + di), vp(d, c + di - dj), vp(d, c - di), vp(d, c - di - dj),
-                vp(d, c + 1), vp(d, c - dj + 1), vp(d, c - 1), vp(d, c - dj - 1), mm, iJf, out);
+    if (CH) {
+      const double *t = d.ftab + (1LL * d.Y + (j - 1)) * 4;
+      visc_face_y_channel(d.rdxi, d.rdet, d.rdzt, d.mu, d.rpr, t[0], o, vp(d, c - dj), vp(d, c + di),
+                          vp(d, c + di - dj), vp(d, c - di), vp(d, c - di - dj), vp(d, c + 1), vp(d, c - dj + 1),
+                          vp(d, c - 1), vp(d, c - dj - 1), t[2], out);
+    } else {
+      double mm[9], Jf, iJf;
+      face_metrics(d, 1, f, j - 1, mm, Jf, iJf);
+      visc_face_y(d.rdxi, d.rdet, d.rdzt, d.mu, d.rpr, o, vp(d, c - dj), vp(d, c + di), vp(d, c + di - dj), vp(d, c - di),
+                  vp(d, c - di - dj), vp(d, c + 1), vp(d, c - dj + 1), vp(d, c - 1), vp(d, c - dj - 1), mm, iJf, out);
+    }
     for (int v = 0; v < 4; v++) d.vflux[1][v][c] = out[v];
   }
   if (i <= ie && j <= jn) {
     double out[4];
-    double mm[9], Jf, iJf;
-    face_metrics(d, 2, f, j - 1, mm, Jf, iJf);
-    visc_face_z(d.rdxi, d.rdet, d.rdzt, d.mu, d.rpr, o, vp(d, c - 1), vp(d, c + di), vp(d, c + di - 1), vp(d, c - di), vp(d, c - di - 1),
-                vp(d, c + dj), vp(d, c + dj - 1), vp(d, c - dj), vp(d, c - dj - 1), vp(d, c - di + dj),
-                mm, iJf, out);
+    if (CH) {
+      const double *t = d.ftab + (2LL * d.Y + (j - 1)) * 4;
+      visc_face_z_channel(d.rdxi, d.rdet, d.rdzt, d.mu, d.rpr, t[0], o, vp(d, c - 1), vp(d, c + di),
+                          vp(d, c + di - 1), vp(d, c - di), vp(d, c - di - 1), vp(d, c + dj), vp(d, c + dj - 1),
+                          vp(d, c - dj), vp(d, c - dj - 1), t[2], out);
+    } else {
+      double mm[9], Jf, iJf;
+      face_metrics(d, 2, f, j - 1, mm, Jf, iJf);
+      visc_face_z(d.rdxi, d.rdet, d.rdzt, d.mu, d.rpr, o, vp(d, c - 1), vp(d, c + di), vp(d, c + di - 1), vp(d, c - di),
+                  vp(d, c - di - 1), vp(d, c + dj), vp(d, c + dj - 1), vp(d, c - dj), vp(d, c - dj - 1),
+                  vp(d, c - di + dj), mm, iJf, out);
+    }
     for (int v = 0; v < 4; v++) d.vflux[2][v][c] = out[v];
   }
 }
@@ -632,7 +656,8 @@ void launch_flux_z(const Dev &d, cudaStream_t s) {
 }
 void launch_viscous(const Dev &d, cudaStream_t s) {
   k_vprim<<<cellgrid(d.nz + 2, d.ny + 2, d.nx + 2, 64), 64, 0, s>>>(d);
-  k_viscous_faces<<<cellgrid(d.nz + 1, d.ny + 1, d.nx + 1, 64), 64, 0, s>>>(d);
+  if (d.face_tables) k_viscous_faces<true><<<cellgrid(d.nz + 1, d.ny + 1, d.nx + 1, 64), 64, 0, s>>>(d);
+  else k_viscous_faces<false><<<cellgrid(d.nz + 1, d.ny + 1, d.nx + 1, 64), 64, 0, s>>>(d);
   k_viscous_div<<<cellgrid(d.nz, d.ny, d.nx, 64), 64, 0, s>>>(d);
 }
 void launch_dts_residual(const Dev &d, cudaStream_t s) {

@@ -616,7 +616,7 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
 // tile-skewed layout), fully parallel rather than inside the wavefront's
 // chain of dependent steps, with per-block partial sums of the squared
 // increments (:1761-1776); one block per (j, i) row of k.  The divisions by
-// q1, rho, T and J are reciprocals (1/J from the table).
+// q1, rho, T and J are Newton-refined reciprocals (1/J from the table).
 template <typename T>
 __global__ void __launch_bounds__(128) k_update_skewed(Dev d, SweepArgs a) {
   // a wavefront pass that gave up left dQ incomplete: keep the state
@@ -627,16 +627,16 @@ __global__ void __launch_bounds__(128) k_update_skewed(Dev d, SweepArgs a) {
   for (int k = 2 + threadIdx.x; k <= d.nz + 1; k += blockDim.x) {
     const long long c = ix(d, i, j, k), slot = skew_slot<T>(d, i, j, k);
     const double J = d.J[c], iJ = d.iJ[c];
-    const double q1 = d.U_[0][c], iq1 = 1 / q1;
+    const double q1 = d.U_[0][c], iq1 = nr_rcp(q1);
     const double rhoold = q1 * J;
     const double Uold = d.U_[1][c] * iq1, Vold = d.U_[2][c] * iq1, Wold = d.U_[3][c] * iq1;
     const double VVold = Uold * Uold + Vold * Vold + Wold * Wold;
     const double Pold = (d.U_[4][c] * J - 0.5 * rhoold * VVold) * (KG - 1);
-    const double Told = Pold / rhoold;
+    const double Told = Pold * (iq1 * iJ);   // 1 / rho = 1 / (q1 J)
     const double P = Pold + (double)dq[0][slot] * J, U = Uold + (double)dq[1][slot] * J;
     const double V = Vold + (double)dq[2][slot] * J, W = Wold + (double)dq[3][slot] * J;
     const double Tn = Told + (double)dq[4][slot] * J;
-    const double rho = P / Tn, rJ = rho * iJ;
+    const double rho = P * nr_rcp(Tn), rJ = rho * iJ;
     d.U_[0][c] = rJ;
     d.U_[1][c] = rJ * U;
     d.U_[2][c] = rJ * V;

@@ -217,4 +217,87 @@ __device__ __forceinline__ void visc_face_z(double rdxi, double rdet, double rdz
                    q.f10 * Wz * dv_dy + CvK * q.f4 * dT_dy * ipr) * iJf;
 }
 
+// ----------------------------------------------------------------------------
+// The same three face fluxes on a face whose metrics have the channel's form
+// xi = (1,0,0), eta = (0,e,0), zeta = (0,0,1) (checked on the device over
+// every face before these are used).  Then a1..f10 are a1 = 4/3, a2 = a3 =
+// a4 = 1; b1 = b3 = b4 = e^2, b2 = 4/3 e^2; c1 = c2 = c4 = 1, c3 = 4/3;
+// d5 = e, d7 = -2/3 e; e6 = 1, e9 = -2/3; f8 = e, f10 = -2/3 e; and every
+// other product is exactly zero, so each flux keeps only its nonzero terms
+// (the reference's sums with the zero terms dropped: the same value to
+// rounding) and only the differences those terms use are formed.
+
+// x face i-1/2 (Viscous_terms.cpp:399-546 with the channel's metrics)
+template <typename P>
+__device__ __forceinline__ void visc_face_x_channel(double rdxi, double rdet, double rdzt, double mu, double ipr,
+                                                    double e, const P &o, const P &im, const P &jp, const P &iJ,
+                                                    const P &jm, const P &ijm, const P &kp, const P &iK, const P &km,
+                                                    const P &ikm, double iJf, double out[4]) {
+  const double invXI = rdxi, inv4ET = 0.25 * rdet, inv4ZT = 0.25 * rdzt;
+  const double CvK = CV * KG;
+  const double U = o.U, V = o.V, W = o.W, T = o.T;
+  const double du_dx = (U - im.U) * invXI, dv_dx = (V - im.V) * invXI, dw_dx = (W - im.W) * invXI;
+  const double du2_dx = (U * U - im.U * im.U) * invXI, dv2_dx = (V * V - im.V * im.V) * invXI,
+               dw2_dx = (W * W - im.W * im.W) * invXI;
+  const double dT_dx = (T - im.T) * invXI;
+  const double du_dy = (jp.U + iJ.U - jm.U - ijm.U) * inv4ET, dv_dy = (jp.V + iJ.V - jm.V - ijm.V) * inv4ET;
+  const double du_dz = (kp.U + iK.U - km.U - ikm.U) * inv4ZT, dw_dz = (kp.W + iK.W - km.W - ikm.W) * inv4ZT;
+  const double Ux = 0.5 * (U + im.U), Vx = 0.5 * (V + im.V), Wx = 0.5 * (W + im.W), Tx = 0.5 * (T + im.T);
+  const double m = sutherland_mu(mu, Tx) * iJf;
+  out[0] = m * ((4. / 3) * du_dx - (2. / 3) * e * dv_dy - (2. / 3) * dw_dz);
+  out[1] = m * (dv_dx + e * du_dy);
+  out[2] = m * (dw_dx + du_dz);
+  out[3] = m * ((2. / 3) * du2_dx + 0.5 * dv2_dx + 0.5 * dw2_dx + CvK * dT_dx * ipr + e * Vx * du_dy -
+                (2. / 3) * e * Ux * dv_dy + Wx * du_dz - (2. / 3) * Ux * dw_dz);
+}
+
+// y face j-1/2 (Viscous_terms.cpp:549-700 with the channel's metrics)
+template <typename P>
+__device__ __forceinline__ void visc_face_y_channel(double rdxi, double rdet, double rdzt, double mu, double ipr,
+                                                    double e, const P &o, const P &jm, const P &ip, const P &jI,
+                                                    const P &im, const P &ijm, const P &kp, const P &jK, const P &km,
+                                                    const P &jkm, double iJf, double out[4]) {
+  const double inv4XI = 0.25 * rdxi, invET = rdet, inv4ZT = 0.25 * rdzt;
+  const double CvK = CV * KG;
+  const double U = o.U, V = o.V, W = o.W, T = o.T;
+  const double du_dx = (ip.U + jI.U - im.U - ijm.U) * inv4XI, dv_dx = (ip.V + jI.V - im.V - ijm.V) * inv4XI;
+  const double du_dy = (U - jm.U) * invET, dv_dy = (V - jm.V) * invET, dw_dy = (W - jm.W) * invET;
+  const double du2_dy = (U * U - jm.U * jm.U) * invET, dv2_dy = (V * V - jm.V * jm.V) * invET,
+               dw2_dy = (W * W - jm.W * jm.W) * invET;
+  const double dT_dy = (T - jm.T) * invET;
+  const double dv_dz = (kp.V + jK.V - km.V - jkm.V) * inv4ZT, dw_dz = (kp.W + jK.W - km.W - jkm.W) * inv4ZT;
+  const double Uy = 0.5 * (U + jm.U), Vy = 0.5 * (V + jm.V), Wy = 0.5 * (W + jm.W), Ty = 0.5 * (T + jm.T);
+  const double m = sutherland_mu(mu, Ty) * iJf, e2 = e * e;
+  out[0] = m * (e * dv_dx + e2 * du_dy);
+  out[1] = m * (-(2. / 3) * e * du_dx + (4. / 3) * e2 * dv_dy - (2. / 3) * e * dw_dz);
+  out[2] = m * (e2 * dw_dy + e * dv_dz);
+  out[3] = m * (0.5 * e2 * du2_dy + (2. / 3) * e2 * dv2_dy + 0.5 * e2 * dw2_dy + CvK * e2 * dT_dy * ipr +
+                e * Uy * dv_dx - (2. / 3) * e * Vy * du_dx + e * Wy * dv_dz - (2. / 3) * e * Vy * dw_dz);
+}
+
+// z face k-1/2 (Viscous_terms.cpp:714-861 with the channel's metrics; the
+// typo of :744-746 only feeds terms whose products are zero here)
+template <typename P>
+__device__ __forceinline__ void visc_face_z_channel(double rdxi, double rdet, double rdzt, double mu, double ipr,
+                                                    double e, const P &o, const P &km, const P &ip, const P &kI,
+                                                    const P &im, const P &ikm, const P &jp, const P &kJ, const P &jm,
+                                                    const P &jkm, double iJf, double out[4]) {
+  const double inv4XI = 0.25 * rdxi, inv4ET = 0.25 * rdet, invZT = rdzt;
+  const double CvK = CV * KG;
+  const double U = o.U, V = o.V, W = o.W, T = o.T;
+  const double du_dx = (ip.U + kI.U - im.U - ikm.U) * inv4XI, dw_dx = (ip.W + kI.W - im.W - ikm.W) * inv4XI;
+  const double dv_dy = (jp.V + kJ.V - jm.V - jkm.V) * inv4ET, dw_dy = (jp.W + kJ.W - jm.W - jkm.W) * inv4ET;
+  const double du_dz = (U - km.U) * invZT, dv_dz = (V - km.V) * invZT, dw_dz = (W - km.W) * invZT;
+  const double du2_dz = (U * U - km.U * km.U) * invZT, dv2_dz = (V * V - km.V * km.V) * invZT,
+               dw2_dz = (W * W - km.W * km.W) * invZT;
+  const double dT_dz = (T - km.T) * invZT;
+  const double Uz = 0.5 * (U + km.U), Vz = 0.5 * (V + km.V), Wz = 0.5 * (W + km.W), Tz = 0.5 * (T + km.T);
+  const double m = sutherland_mu(mu, Tz) * iJf;
+  out[0] = m * (dw_dx + du_dz);
+  out[1] = m * (e * dw_dy + dv_dz);
+  out[2] = m * (-(2. / 3) * du_dx - (2. / 3) * e * dv_dy + (4. / 3) * dw_dz);
+  out[3] = m * (0.5 * du2_dz + 0.5 * dv2_dz + (2. / 3) * dw2_dz + CvK * dT_dz * ipr + Uz * dw_dx -
+                (2. / 3) * Wz * du_dx + e * Vz * dw_dy - (2. / 3) * e * Wz * dv_dy);
+}
+
 }  // namespace cgli
