@@ -56,7 +56,8 @@ struct cgli_ctx {
   bool have_metrics = false, have_state = false;
   double *h_norms = nullptr;   // pinned, 8 doubles
   double *d_out = nullptr;     // device scratch for norms / bulk flux
-  int update_blocks = 0;
+  int update_blocks = 0;         // partial sums of the per-row update kernels (routine path, DP-LUR)
+  int sweep_update_blocks = 0;   // partial sums of the update after the wavefront passes
   int sweep_tiles = 0;
   cgli::SweepArgs sw;
   bool metrics_checked = false;
@@ -320,7 +321,8 @@ int cgli_create(const cgli_params *p, cgli_ctx **out) {
   const int tile_i = mixed_passes ? cgli::SweepTile<float>::TI : cgli::SweepTile<double>::TI;
   const int tile_j = mixed_passes ? cgli::SweepTile<float>::TJ : cgli::SweepTile<double>::TJ;
   c->sweep_tiles = nti * ntj;
-  size_t nblk = (size_t)std::max(c->update_blocks, c->sweep_tiles);
+  c->sweep_update_blocks = cgli::sweep_update_blocks(d, mixed_passes);
+  size_t nblk = (size_t)std::max(std::max(c->update_blocks, c->sweep_tiles), c->sweep_update_blocks);
   if (rc == CGLI_OK) rc = alloc(c, 5 * sizeof(double) * nblk, (void **)&d.partial);
   {
     cgli::SweepArgs &a = c->sw;
@@ -768,7 +770,7 @@ int cgli_inner_iteration(cgli_ctx *c, double er[5]) {
     if (e != cudaSuccess) return fail(CGLI_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
   }
   CUDA_TRY(cudaGraphLaunch(c->iter_graph, c->stream));
-  rc = read_norms(c, er, c->update_blocks);   // synchronises the stream
+  rc = read_norms(c, er, dplur ? c->update_blocks : c->sweep_update_blocks);   // synchronises the stream
   if (rc == CGLI_OK && !dplur) {
     float ms = 0;
     if (cudaEventElapsedTime(&ms, c->sweep_ev[0], c->sweep_ev[1]) == cudaSuccess) {

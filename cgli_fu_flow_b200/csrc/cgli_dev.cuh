@@ -549,9 +549,27 @@ __device__ __forceinline__ void sweep_coef(T q1, T q2, T q3, T q4, T q5, T J, co
 // with U = mx u + my v + mz w the contravariant velocity, lam its spectral
 // radius (Dual_time_stepping.cpp:1040-1072 and :1384-1409), h = P K beta / 2,
 // hr = 1 / (2 rho), hbT = beta T (K-1) / 2, g = (K-1)(beta-1) / (2 rho K); the
-// own diagonal d11, d22, d51 of :887-895.
-constexpr int REC_N = 14;
-enum { R_BETA = 0, R_H, R_HR, R_HBT, R_G, R_UX, R_UY, R_UZ, R_LX, R_LY, R_LZ, R_D11, R_D22, R_D51 };
+// own diagonal d11, d22, d51 of :887-895.  The record keeps beta, h, hr, the
+// three U and lam, d11 and d22 (11 words); hbT = 2 h hr (K-1)/K,
+// g = (beta-1) hr (K-1)/K and d51 = -3 g d11 d22 / dt are formed from them
+// where they are used (a few products, off the wavefront's dependency
+// chain), so that a cell's record and MR are 16 words.
+constexpr int REC_N = 11;
+enum { R_BETA = 0, R_H, R_HR, R_UX, R_UY, R_UZ, R_LX, R_LY, R_LZ, R_D11, R_D22 };
+
+template <typename T>
+__device__ __forceinline__ T rec_hbt(const T r[REC_N]) {
+  return r[R_H] * r[R_HR] * (T)(2.0 * (KG - 1) / KG);
+}
+template <typename T>
+__device__ __forceinline__ T rec_g(const T r[REC_N]) {
+  return (r[R_BETA] - 1) * r[R_HR] * (T)((KG - 1) / KG);
+}
+// rdt = 1 / dt
+template <typename T>
+__device__ __forceinline__ T rec_d51(const T r[REC_N], T rdt) {
+  return (T)-3 * rec_g<T>(r) * r[R_D11] * r[R_D22] * rdt;
+}
 
 __device__ __forceinline__ void make_record(double q1, double q2, double q3, double q4, double q5, double J,
                                             const double mm[9], double e, double rdx, double rdy, double rdz,
@@ -564,7 +582,6 @@ __device__ __forceinline__ void make_record(double q1, double q2, double q3, dou
   double P = (q5 * J - 0.5 * rho * VV) * (K - 1);
   double rrho = nr_rcp(rho);
   double C = K * P * rrho;
-  double Tt = P * rrho;
   double th = VV * nr_rcp(C);
   double beta = th > e ? th : e;
   double lam[3], U[3];
@@ -582,13 +599,10 @@ __device__ __forceinline__ void make_record(double q1, double q2, double q3, dou
   r[R_BETA] = beta;
   r[R_H] = 0.5 * P * K * beta;
   r[R_HR] = 0.5 * rrho;
-  r[R_HBT] = 0.5 * beta * Tt * (K - 1);
-  r[R_G] = 0.5 * (K - 1) * (beta - 1) * rrho * (1.0 / KG);
   r[R_UX] = U[0]; r[R_UY] = U[1]; r[R_UZ] = U[2];
   r[R_LX] = lam[0]; r[R_LY] = lam[1]; r[R_LZ] = lam[2];
   r[R_D11] = 2 * dt * a1;
   r[R_D22] = 2 * dt * a2;
-  r[R_D51] = -(6 * (K - 1) * (beta - 1) * dt) * (a1 * a2) * rrho * (1.0 / KG);
 }
 
 // split Jacobian entries of one direction from a record
@@ -604,10 +618,11 @@ __device__ __forceinline__ Split<T> split_from_record(const T r[REC_N], int dir,
   a.p31 = r[R_HR] * my;
   a.p41 = r[R_HR] * mz;
   a.p22 = (T)0.5 * (U + lam);
-  a.p51 = r[R_G] * U;
-  a.p52 = r[R_HBT] * mx;
-  a.p53 = r[R_HBT] * my;
-  a.p54 = r[R_HBT] * mz;
+  const T hbt = rec_hbt<T>(r);
+  a.p51 = rec_g<T>(r) * U;
+  a.p52 = hbt * mx;
+  a.p53 = hbt * my;
+  a.p54 = hbt * mz;
   a.m11 = (T)0.5 * (beta * U - lam);
   a.m22 = (T)0.5 * (U - lam);
   return a;

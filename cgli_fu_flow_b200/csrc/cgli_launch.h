@@ -9,9 +9,18 @@
 
 namespace cgli {
 
-// words per slot of SweepArgs::cellrec: record, MR, pad
-constexpr int CR_N = REC_N + 5 + 1;
+// words per slot of SweepArgs::cellrec: record, MR (16 words: whole 16-byte
+// vectors in both precisions)
+constexpr int CR_N = REC_N + 5;
 constexpr int CR_MR = REC_N;
+static_assert(CR_N == 16, "record + MR fill 16 words");
+// position of 16-byte vector u (0..7 FP64, 0..3 FP32) within the slot whose
+// index in its step block is t: rotated by t so that the slots' vectors,
+// read one per lane, spread over the shared-memory banks
+template <typename T>
+__host__ __device__ __forceinline__ int rec_vec_pos(int u, int t) {
+  return sizeof(T) == 8 ? (u ^ (t & 7)) : (u ^ ((t >> 1) & 3));
+}
 
 // Wavefront geometry per arithmetic type of the passes: TI x TJ (i, j)
 // columns per CTA (one thread each, so TI * TJ <= 1024 and a multiple of
@@ -64,8 +73,8 @@ struct SweepArgs {
   // thread) = (tile * S + s) * TI*TJ + t, S = Nz + TI + TJ - 2
   double *dq[5];                  // dQ: forward result, then backward result (in place)
   // per slot, CR_N consecutive words: the split-Jacobian / diagonal record
-  // (REC_N), the residual MR (5) and one pad word, so that the residual
-  // writes and the sweep reads whole 16-byte vectors of one cell
+  // (REC_N) and the residual MR (5), so that the residual writes and the
+  // sweep reads whole 16-byte vectors of one cell
   double *cellrec;
   // the same in float for CGLI_MIXED
   float *dqf[5], *cellrecf;
@@ -116,6 +125,8 @@ int sweep_cluster_x(int nti, int ntj, bool mixed);
 void launch_sweeps(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed);
 // the update and norm partials after the last pass (k_update_skewed)
 void launch_sweep_update(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed);
+// partial sums (blocks) the update after the wavefront passes writes
+int sweep_update_blocks(const Dev &d, bool mixed);
 // everything of a fused inner iteration before the sweeps
 void launch_fused_residual(const Dev &d, const SweepArgs &a, cudaStream_t s, int precision);
 // one pass (forward / backward, final with the update) of the sweeps

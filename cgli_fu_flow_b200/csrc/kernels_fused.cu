@@ -46,6 +46,7 @@ __global__ void __launch_bounds__(64, (MIXED && CH && CGLI_RESIDUAL_MINBLOCKS < 
   const int ie = d.nx + 2;
   const bool halo_plane = (i == 2 || i == ie + 1);
   const long long slot = halo_plane ? 0 : skew_slot<typename std::conditional<MIXED, float, double>::type>(d, i, j, k);
+  double r8, r9, r10;   // record words stored together with MR
   {
     // the cell's sweep record; planes 2 and ie+1 (the periodic halo copies)
     // go to the per-(j,k) halo records
@@ -66,19 +67,23 @@ __global__ void __launch_bounds__(64, (MIXED && CH && CGLI_RESIDUAL_MINBLOCKS < 
       }
       return;
     }
-    // the record part of the cell's contiguous block (MR follows at the end)
+    // the record part of the cell's contiguous block; the vectors that the
+    // record's last words share with MR go out with MR below
+    // (vectors in the rotated order of rec_vec_pos: t = slot % 8, the
+    // slot's position in its step block, whose size is a multiple of 8)
+    const int t = (int)(slot & 7);
     if (MIXED) {
       float4 *o = reinterpret_cast<float4 *>(a.cellrecf + slot * CR_N);
-      o[0] = make_float4((float)r[0], (float)r[1], (float)r[2], (float)r[3]);
-      o[1] = make_float4((float)r[4], (float)r[5], (float)r[6], (float)r[7]);
-      o[2] = make_float4((float)r[8], (float)r[9], (float)r[10], (float)r[11]);
-      float2 *o2 = reinterpret_cast<float2 *>(a.cellrecf + slot * CR_N + 12);
-      o2[0] = make_float2((float)r[12], (float)r[13]);
+      o[rec_vec_pos<float>(0, t)] = make_float4((float)r[0], (float)r[1], (float)r[2], (float)r[3]);
+      o[rec_vec_pos<float>(1, t)] = make_float4((float)r[4], (float)r[5], (float)r[6], (float)r[7]);
     } else {
       double2 *o = reinterpret_cast<double2 *>(a.cellrec + slot * CR_N);
 #pragma unroll
-      for (int q = 0; q < 7; q++) o[q] = make_double2(r[2 * q], r[2 * q + 1]);
+      for (int q = 0; q < 5; q++) o[rec_vec_pos<double>(q, t)] = make_double2(r[2 * q], r[2 * q + 1]);
     }
+    r8 = r[8];
+    r9 = r[9];
+    r10 = r[10];
   }
   CPrim<double> q = cprim<double>(d.U_[0][c], d.U_[1][c], d.U_[2][c], d.U_[3][c], d.U_[4][c], J, d.e);
   double rho = q.rho, u = q.u, v = q.v, w = q.w, VV = q.VV, T = q.Tt, H = q.H, beta = q.beta;
@@ -118,17 +123,20 @@ __global__ void __launch_bounds__(64, (MIXED && CH && CGLI_RESIDUAL_MINBLOCKS < 
   MR[2] = (d31 * Rk[0] + d22 * Rk[2]);
   MR[3] = (d41 * Rk[0] + d22 * Rk[3]);
   MR[4] = (d51 * Rk[0] + d52 * Rk[1] + d53 * Rk[2] + d54 * Rk[3] + d55 * Rk[4]);
-  // MR after the record in the cell's contiguous block of CR_N words
+  // MR after the record in the cell's contiguous block of CR_N = 16 words
+  // (record words 0..10, MR 11..15)
+  const int t = (int)(slot & 7);
   if (MIXED) {
-    float2 *o2 = reinterpret_cast<float2 *>(a.cellrecf + slot * CR_N + CR_MR);
-    o2[0] = make_float2((float)MR[0], (float)MR[1]);
-    float4 *o = reinterpret_cast<float4 *>(a.cellrecf + slot * CR_N + 16);
-    o[0] = make_float4((float)MR[2], (float)MR[3], (float)MR[4], 0.f);
+    float4 *o = reinterpret_cast<float4 *>(a.cellrecf + slot * CR_N);
+    o[rec_vec_pos<float>(2, t)] = make_float4((float)r8, (float)r9, (float)r10, (float)MR[0]);
+    o[rec_vec_pos<float>(3, t)] = make_float4((float)MR[1], (float)MR[2], (float)MR[3], (float)MR[4]);
   } else {
-    double2 *o = reinterpret_cast<double2 *>(a.cellrec + slot * CR_N + CR_MR);
-    o[0] = make_double2(MR[0], MR[1]);
-    o[1] = make_double2(MR[2], MR[3]);
-    o[2] = make_double2(MR[4], 0.0);
+    double2 *o = reinterpret_cast<double2 *>(a.cellrec + slot * CR_N);
+    (void)r8;
+    (void)r9;
+    o[rec_vec_pos<double>(5, t)] = make_double2(r10, MR[0]);
+    o[rec_vec_pos<double>(6, t)] = make_double2(MR[1], MR[2]);
+    o[rec_vec_pos<double>(7, t)] = make_double2(MR[3], MR[4]);
   }
   // the lagged halos of the first sweep; an open slab's stay zero
   if (!d.x_open && (i == ie || i == 3)) {

@@ -189,29 +189,37 @@ __device__ __forceinline__ float4 ld_rec(const float4 *q) {
   return *q;
 #endif
 }
-__device__ __forceinline__ void load_cellrec(const double *p, double rec[REC_N], double *mr) {
+// The 16-byte vectors of a slot are stored in an order rotated by the
+// slot's position t in its step block (rec_vec_pos): a warp's vector loads
+// of its slots (one per lane, consecutive slots 128 B (FP64) or 64 B (FP32)
+// apart) then fall on distinct shared-memory banks in every phase of eight
+// lanes.
+__device__ __forceinline__ void load_cellrec(const double *p, int t, double rec[REC_N], double *mr) {
+  // words 0..10 the record, 11..15 MR
   const double2 *q = reinterpret_cast<const double2 *>(p);
 #pragma unroll
-  for (int t = 0; t < 7; t++) {
-    const double2 v = ld_rec(q + t);
-    rec[2 * t] = v.x;
-    rec[2 * t + 1] = v.y;
+  for (int u = 0; u < 5; u++) {
+    const double2 v = ld_rec(q + rec_vec_pos<double>(u, t));
+    rec[2 * u] = v.x;
+    rec[2 * u + 1] = v.y;
   }
+  const double2 a = ld_rec(q + rec_vec_pos<double>(5, t));
+  rec[10] = a.x;
   if (mr) {
-    const double2 a = ld_rec(q + 7), b = ld_rec(q + 8), c = ld_rec(q + 9);
-    mr[0] = a.x; mr[1] = a.y; mr[2] = b.x; mr[3] = b.y; mr[4] = c.x;
+    const double2 b = ld_rec(q + rec_vec_pos<double>(6, t)), c = ld_rec(q + rec_vec_pos<double>(7, t));
+    mr[0] = a.y; mr[1] = b.x; mr[2] = b.y; mr[3] = c.x; mr[4] = c.y;
   }
 }
-__device__ __forceinline__ void load_cellrec(const float *p, float rec[REC_N], float *mr) {
+__device__ __forceinline__ void load_cellrec(const float *p, int t, float rec[REC_N], float *mr) {
   const float4 *q = reinterpret_cast<const float4 *>(p);
-  const float4 a = ld_rec(q), b = ld_rec(q + 1), c = ld_rec(q + 2), e = ld_rec(q + 3);
+  const float4 a = ld_rec(q + rec_vec_pos<float>(0, t)), b = ld_rec(q + rec_vec_pos<float>(1, t)),
+               c = ld_rec(q + rec_vec_pos<float>(2, t));
   rec[0] = a.x; rec[1] = a.y; rec[2] = a.z; rec[3] = a.w;
   rec[4] = b.x; rec[5] = b.y; rec[6] = b.z; rec[7] = b.w;
-  rec[8] = c.x; rec[9] = c.y; rec[10] = c.z; rec[11] = c.w;
-  rec[12] = e.x; rec[13] = e.y;
+  rec[8] = c.x; rec[9] = c.y; rec[10] = c.z;
   if (mr) {
-    const float4 f = ld_rec(q + 4);
-    mr[0] = e.z; mr[1] = e.w; mr[2] = f.x; mr[3] = f.y; mr[4] = f.z;
+    const float4 e = ld_rec(q + rec_vec_pos<float>(3, t));
+    mr[0] = c.w; mr[1] = e.x; mr[2] = e.y; mr[3] = e.z; mr[4] = e.w;
   }
 }
 
@@ -247,7 +255,7 @@ template <typename T, int DIR, bool BACKWARD>
 __device__ __forceinline__ void channel_products(const T r[REC_N], T m, const T n[5], T o[5]) {
   constexpr int q = DIR + 1;
   const T U = r[R_UX + DIR], lam = r[R_LX + DIR], beta = r[R_BETA];
-  const T p1q = r[R_H] * m, pq1 = r[R_HR] * m, p5q = r[R_HBT] * m, p51 = r[R_G] * U;
+  const T p1q = r[R_H] * m, pq1 = r[R_HR] * m, p5q = rec_hbt<T>(r) * m, p51 = rec_g<T>(r) * U;
   if (!BACKWARD) {
     const T p11 = (T)0.5 * (beta * U + lam), p22 = (T)0.5 * (U + lam);
     o[0] = -p11 * n[0] - p1q * n[q];
@@ -372,7 +380,7 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
   // the lanes that wait on the pushes: the tile's receiving edge, all of them
   const bool wait_x = dsm_recv && (BACKWARD ? il == TI - 1 : il == 0);
   const int push_polls = a.spin_limit > (0x7fffffff - kCopyPolls) / 64 ? 0x7fffffff : 64 * a.spin_limit + kCopyPolls;
-  const T rdx = (T)(1.0 / d.dxi), rdy = (T)(1.0 / d.det), rdz = (T)(1.0 / d.dzt);
+  const T rdx = (T)d.rdxi, rdy = (T)d.rdet, rdz = (T)d.rdzt, rdt = (T)(1.0 / d.dt);
   T *xb = SweepPtrs<T>::xb(a), *yb = SweepPtrs<T>::yb(a);
   T *const *dq = SweepPtrs<T>::dq(a);
   T carry_z[5] = {0, 0, 0, 0, 0};
@@ -451,7 +459,7 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
     T rec[REC_N], mr[5];
     if (active) {
       const T *st = s_rec + (s % RING) * kStage;
-      load_cellrec(st + threadIdx.x * CR_N, rec, BACKWARD ? (T *)nullptr : mr);
+      load_cellrec(st + threadIdx.x * CR_N, (int)threadIdx.x, rec, BACKWARD ? (T *)nullptr : mr);
       if (DQB)
 #pragma unroll
         for (int v = 0; v < 5; v++) mr[v] = st[TI * TJ * CR_N + v * TI * TJ + threadIdx.x];
@@ -496,7 +504,7 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
       T L[5];
 #pragma unroll
       for (int v = 0; v < 5; v++) L[v] = tx[v] * rdx + ty[v] * rdy + (zedge ? (T)0 : carry_z[v]) * rdz;
-      const T d11 = rec[R_D11], d22 = rec[R_D22], d51 = rec[R_D51];
+      const T d11 = rec[R_D11], d22 = rec[R_D22], d51 = rec_d51<T>(rec, rdt);
       T n[5];
       if (!BACKWARD) {
         // Dual_time_stepping.cpp:1289-1293
@@ -615,17 +623,56 @@ __global__ void __launch_bounds__(TI *TJ, CGLI_SWEEP_MINBLOCKS) k_sweep(Dev d, S
 // primitive update of every interior cell from its final dQ (read from the
 // tile-skewed layout), fully parallel rather than inside the wavefront's
 // chain of dependent steps, with per-block partial sums of the squared
-// increments (:1761-1776); one block per (j, i) row of k.  The divisions by
-// q1, rho, T and J are Newton-refined reciprocals (1/J from the table).
+// increments (:1761-1776).  The divisions by q1, rho, T and J are
+// Newton-refined reciprocals (1/J from the table).
+//
+// A block owns one row il of one tile's TJ columns and UPD_KC consecutive k
+// of them.  In the tile-skewed layout those cells lie in UPD_KC + TJ - 1
+// consecutive steps, each holding the row's TJ slots side by side: the block
+// reads them whole (TJ consecutive words per step and variable) into shared
+// memory, then each warp updates 32 consecutive k of one column, so the
+// reads and writes of the state in the reference layout are coalesced too.
+constexpr int UPD_KC = 32;
 template <typename T>
-__global__ void __launch_bounds__(128) k_update_skewed(Dev d, SweepArgs a) {
+inline unsigned sweep_update_grid_x(const Dev &d) {
+  constexpr int TI = SweepTile<T>::TI, TJ = SweepTile<T>::TJ;
+  return (unsigned)(((d.nx + TI - 1) / TI) * ((d.ny + TJ - 1) / TJ) * TI);
+}
+template <typename T>
+inline unsigned sweep_update_grid_y(const Dev &d) { return (unsigned)((d.nz + UPD_KC - 1) / UPD_KC); }
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_update_skewed(Dev d, SweepArgs a) {
+  constexpr int TI = SweepTile<T>::TI, TJ = SweepTile<T>::TJ;
+  constexpr int NS = UPD_KC + TJ - 1;   // steps holding the block's cells
+  static_assert(256 % TJ == 0 && TJ % 8 == 0, "row staging");
+  __shared__ T sdq[5][NS][TJ + 1];       // (+1: the update reads a column down the steps)
   // a wavefront pass that gave up left dQ incomplete: keep the state
   if (*(volatile int *)d.status) return;
-  const int j = 2 + blockIdx.x, i = 3 + blockIdx.y;
+  const int ntj = (d.ny + TJ - 1) / TJ, S = d.nz + TI + TJ - 2;
+  const int tile = blockIdx.x / TI, il = blockIdx.x % TI;
+  const int ta = tile / ntj, tb = tile % ntj;
+  const int k0 = blockIdx.y * UPD_KC;    // first k of the block (0-based)
+  const int s0 = k0 + il;                // step of the cell (il, jl = 0, k0)
+  const long long base = (long long)tile * S * (TI * TJ) + il * TJ;
   T *const *dq = SweepPtrs<T>::dq(a);
+  for (int e = threadIdx.x; e < NS * TJ; e += blockDim.x) {
+    const int ls = e / TJ, jl = e % TJ, st = s0 + ls;
+    if (st < S) {
+      const long long g = base + (long long)st * (TI * TJ) + jl;
+#pragma unroll
+      for (int v = 0; v < 5; v++) sdq[v][ls][jl] = dq[v][g];
+    }
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int i = 3 + ta * TI + il;
   double acc[5] = {0, 0, 0, 0, 0};
-  for (int k = 2 + threadIdx.x; k <= d.nz + 1; k += blockDim.x) {
-    const long long c = ix(d, i, j, k), slot = skew_slot<T>(d, i, j, k);
+  for (int jl = warp; jl < TJ; jl += nw) {
+    const int j = 2 + tb * TJ + jl, kl = k0 + lane;
+    if (i > d.nx + 2 || j > d.ny + 1 || kl >= d.nz) continue;
+    const int ls = lane + jl;            // step kl + il + jl, relative to s0
+    const long long c = ix(d, i, j, 2 + kl);
     const double J = d.J[c], iJ = d.iJ[c];
     const double q1 = d.U_[0][c], iq1 = nr_rcp(q1);
     const double rhoold = q1 * J;
@@ -633,9 +680,9 @@ __global__ void __launch_bounds__(128) k_update_skewed(Dev d, SweepArgs a) {
     const double VVold = Uold * Uold + Vold * Vold + Wold * Wold;
     const double Pold = (d.U_[4][c] * J - 0.5 * rhoold * VVold) * (KG - 1);
     const double Told = Pold * (iq1 * iJ);   // 1 / rho = 1 / (q1 J)
-    const double P = Pold + (double)dq[0][slot] * J, U = Uold + (double)dq[1][slot] * J;
-    const double V = Vold + (double)dq[2][slot] * J, W = Wold + (double)dq[3][slot] * J;
-    const double Tn = Told + (double)dq[4][slot] * J;
+    const double P = Pold + (double)sdq[0][ls][jl] * J, U = Uold + (double)sdq[1][ls][jl] * J;
+    const double V = Vold + (double)sdq[2][ls][jl] * J, W = Wold + (double)sdq[3][ls][jl] * J;
+    const double Tn = Told + (double)sdq[4][ls][jl] * J;
     const double rho = P * nr_rcp(Tn), rJ = rho * iJ;
     d.U_[0][c] = rJ;
     d.U_[1][c] = rJ * U;
@@ -649,6 +696,15 @@ __global__ void __launch_bounds__(128) k_update_skewed(Dev d, SweepArgs a) {
     acc[4] += (Tn - Told) * (Tn - Told);
   }
   block_sum5(acc, d.partial + 5 * ((long long)blockIdx.y * gridDim.x + blockIdx.x));
+}
+
+template <typename T>
+static void launch_update_skewed(const Dev &d, const SweepArgs &a, cudaStream_t s) {
+  k_update_skewed<T><<<dim3(sweep_update_grid_x<T>(d), sweep_update_grid_y<T>(d)), 256, 0, s>>>(d, a);
+}
+int sweep_update_blocks(const Dev &d, bool mixed) {
+  return mixed ? (int)(sweep_update_grid_x<float>(d) * sweep_update_grid_y<float>(d))
+               : (int)(sweep_update_grid_x<double>(d) * sweep_update_grid_y<double>(d));
 }
 
 // dynamic shared memory of a wavefront pass: the ring of record stages
@@ -704,7 +760,7 @@ static void run_one_pass(const Dev &d, const SweepArgs &a, cudaStream_t s, bool 
     if (!backward) cudaLaunchKernelEx(&cfg, k_sweep<TI, TJ, Met, false, T, false>, d, a);
     else cudaLaunchKernelEx(&cfg, k_sweep<TI, TJ, Met, true, T, false>, d, a);
   }
-  if (final_pass) k_update_skewed<T><<<dim3(d.ny, d.nx), 128, 0, s>>>(d, a);
+  if (final_pass) launch_update_skewed<T>(d, a, s);
 }
 
 template <int TI, int TJ, class Met, typename T>
@@ -785,8 +841,8 @@ int sweep_cluster_x(int nti, int ntj, bool mixed) {
 }
 
 void launch_sweep_update(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed) {
-  if (mixed) k_update_skewed<float><<<dim3(d.ny, d.nx), 128, 0, s>>>(d, a);
-  else k_update_skewed<double><<<dim3(d.ny, d.nx), 128, 0, s>>>(d, a);
+  if (mixed) launch_update_skewed<float>(d, a, s);
+  else launch_update_skewed<double>(d, a, s);
 }
 
 void launch_sweeps(const Dev &d, const SweepArgs &a, cudaStream_t s, bool mixed) {
