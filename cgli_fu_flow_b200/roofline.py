@@ -21,12 +21,12 @@ SWEEP_BYTES_PER_CELL = {"fp64": 25 * 8, "mixed": 25 * 4}
 
 # DRAM bytes (read + write) per cell of one sweep pass from an ncu capture of
 # the current k_sweep (16 x 16-column FP64 tiles; dram__bytes_read.sum +
-# dram__bytes_write.sum, forward 243 B and backward 291 B per cell, averaged)
+# dram__bytes_write.sum, forward 202 B and backward 250 B per cell, averaged)
 # on the 160x128x128 channel; traffic grows with the cell count, so it is
-# scaled to the benchmark grid.  The passes read each cell's 20-word record
-# block (the backward pass also its forward result) and write 5 words.  See
+# scaled to the benchmark grid.  The passes read each cell's 16-word record +
+# MR slot (the backward pass also its forward result) and write 5 words.  See
 # profiles/k_sweep_channel_160x128x128.md.
-MEASURED_TRAFFIC_PER_CELL = {"fp64": (243.3 + 290.6) / 2, "mixed": None}
+MEASURED_TRAFFIC_PER_CELL = {"fp64": (202.2 + 250.2) / 2, "mixed": None}
 
 
 def hbm_peak() -> tuple[float, str]:
@@ -62,11 +62,12 @@ RESIDUAL_STAGES = ("halo_bc", "flux_x", "flux_y", "flux_z", "viscous", "residual
 
 # FP64 instructions per cell (thread level) of the residual side's kernels,
 # from ncu (sm__inst_executed_pipe_fp64.sum x 32 / cells) on the
-# 160x128x128 channel: flux 430 per face and direction, viscous faces 980,
-# residual assembly 315.  With the FP64 pipe's measured rate on this GPU
-# (a standalone FMA probe: 34 TFLOP/s = 17 T FP64 instructions/s) this is a
-# lower bound on the side's time that lies above its HBM bound.
-RESIDUAL_FP64_OPS_PER_CELL = 3 * 430 + 980 + 315
+# 160x128x128 channel: fluxes 294 / 297 / 377 per face (x / y / z), k_vprim
+# 27, viscous faces 279 (channel form), k_viscous_div 24, residual assembly
+# 260.  With the FP64 pipe's measured rate on this GPU (a standalone FMA
+# probe: 34 TFLOP/s = 17 T FP64 instructions/s) this is a lower bound on the
+# side's time.  See profiles/k_flux_k_viscous_k_residual_fast_channel_160x128x128.md.
+RESIDUAL_FP64_OPS_PER_CELL = 294 + 297 + 377 + 27 + 279 + 24 + 260
 FP64_INST_PER_S = 17.0e12
 
 
