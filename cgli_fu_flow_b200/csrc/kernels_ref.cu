@@ -347,8 +347,11 @@ __device__ __forceinline__ VP vp(const Dev &d, long long c) {
 // divergence of Viscous_terms.cpp:875-904 reads).  CH: the face metrics have
 // the channel's form (d.face_tables), so the per-row tables give eta_y and
 // 1/J and the channel forms of the face fluxes apply.
+// (the channel form fits 64 registers without spills: held at 16 CTAs per
+// SM, 32 warps to hide its stencil loads)
 template <bool CH>
-__global__ void __launch_bounds__(64, CGLI_VISCOUS_MINBLOCKS) k_viscous_faces(Dev d) {
+__global__ void __launch_bounds__(64, (CH && CGLI_VISCOUS_MINBLOCKS < 16) ? 16 : CGLI_VISCOUS_MINBLOCKS)
+    k_viscous_faces(Dev d) {
   int k = 2 + blockIdx.x * blockDim.x + threadIdx.x;
   int j = 2 + blockIdx.y;
   int i = 3 + blockIdx.z;
