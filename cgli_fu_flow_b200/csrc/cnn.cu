@@ -19,17 +19,24 @@
 //
 // Convolution = implicit GEMM on tcgen05.  One CTA owns a column of
 // 4 (y) x 32 (z) cells and marches over a chunk of x planes; an output tile
-// is the 128 cells of one x plane (M = 128), N = 32 output channels,
+// is the 128 cells of one x plane (M = 128), 32 output channels,
 // K = 27 taps x 32 input channels.  A TMA producer warp loads, per x plane,
 // three copies of the 6 (y) x 32 (z) x 32-channel halo box shifted by
-// dz = -1, 0, +1, 64-byte swizzled, into a 4-plane ring: the A operand of tap
-// (dx, dy, dz) is then the 128 consecutive rows starting at row 32 dy of
-// copy dz of plane x + dx, a shared-memory descriptor with no data movement.
-// All 27 taps of the weights stay resident in shared memory.  One thread
-// issues the 54 MMAs (K = 16 each) of a tile into one of two TMEM
-// accumulators; four epilogue warps read the other accumulator (tcgen05.ld),
-// add the bias and apply GELU (forward), or multiply by GELU'(z) of the layer
-// below (input gradient, same kernel with the transposed, flipped weights).
+// dz = -1, 0, +1, 64-byte swizzled, into a 4-plane ring: the rows of tap
+// (dy, dz) of a plane are then the 128 consecutive rows starting at row
+// 32 dy of copy dz, a shared-memory descriptor with no data movement.
+// Plane p is the A operand of the dx = 0, 1, 2 taps of output tiles p, p-1,
+// p-2, so one MMA per (dy, dz, K half) multiplies it by the three dx blocks
+// of weights side by side (N = 96; all 27 taps stay resident in shared
+// memory, stored (dy, dz)-major with the dx blocks adjacent) into the three
+// tiles' accumulators: a ring of eight 32-column TMEM slots in which tile
+// q - 1 sits 32 columns after tile q (the block is split where the ring
+// wraps, and narrowed where a tile does not exist).  Each plane is read by
+// its 18 MMAs once, and its ring slot is free as soon as they complete.
+// Four epilogue warps drain each finished tile (tcgen05.ld), zero its slot
+// for its next use, add the bias and apply GELU (forward), or multiply by
+// GELU'(z) of the layer below (input gradient, same kernel with the
+// transposed, flipped weights).
 //
 // Weight gradient = the same operand images read as MN-major matrices:
 // D[(dy, c_in)][c_out] = sum over cells of X(shifted by (dx, dy, dz))[c_in]
