@@ -7,7 +7,7 @@ REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if REPO not in sys.path:
     sys.path.insert(0, REPO)
 
-REFERENCE_DIR = os.environ.get("CGLI_REFERENCE_DIR", "/root/reference")
+from oracle.build_ref import REF_SRC as REFERENCE_DIR  # noqa: E402  (the reference tree the recipe reads)
 
 
 def pytest_configure(config):

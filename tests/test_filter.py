@@ -71,7 +71,7 @@ def test_filter_oracle_periodic_x_ends():
     assert np.array_equal(RY, R0[1], equal_nan=True) and np.array_equal(RZ, R0[2], equal_nan=True)
 
 
-REF = os.environ.get("CGLI_REFERENCE_DIR", "/root/reference")
+from oracle.build_ref import REF_SRC as REF  # noqa: E402  (the reference tree the recipe reads)
 
 
 @pytest.mark.skipif(not os.path.isdir(REF), reason="reference sources not present")
